@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Throughput of the B200 read-mapping path (reads/s) on the 4.6 Mbp / 1,000,000 x 150 bp
+workload, in batches of 262,144 reads per launch of the pipeline.
+
+One step maps the whole 1,000,000-read workload (4 batches). Two measurements:
+* value — inputs already resident in HBM, dnaln_gpu_map_batch_device, timed with CUDA
+  events on the launching stream;
+* e2e   — the reference-facing C call dnaln_gpu_map_batch on pinned HOST buffers, with the
+  host->device copy of the reads and the device->host copy of records and CIGARs inside
+  the timed region.
+
+`--impl reference` times the reference's own CPU mapper (Mapper::map, compiled from its
+sources into oracle/_ref) on the host cores with all threads, same workload and metric.
+
+Multi-GPU (`torchrun --nproc-per-node N bench.py --gpus N`): each rank maps its own
+1,000,000 reads against a replica of the index (weak scaling); no collective on the data
+path, timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "ecoli-4.6Mbp-1M-150bp"
+BATCH = 262_144
+METRIC = "reads/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--n-reads", type=int, default=None, help="override the workload's read count (testing)")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler(threading.Thread):
+    """Samples SM clock and clock-event reasons of one GPU through NVML (read-only)."""
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x2: "applications_clocks_setting"}
+
+    def __init__(self, device: int, period: float = 0.02):
+        super().__init__(daemon=True)
+        self.period, self.samples, self.reasons, self.stop_ev = period, [], set(), threading.Event()
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def run(self):
+        if not self.nv:
+            return
+        get_r = getattr(self.nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            self.nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop_ev.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = get_r(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def result(self):
+        self.stop_ev.set()
+        self.join(timeout=2)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def workload_config(n_reads: int, world: int) -> dict:
+    return {"workload": f"{WORKLOAD}: 4.6 Mbp i.i.d. genome (P(G)=P(C)=0.254), {n_reads:,} x 150 bp reads "
+                        "(1% substitution, 0.1% indel), k=15 w=10 bw=16 A2 B4 O4 E2, batches of 262,144",
+            "reads_per_step": n_reads, "batch": BATCH, "genome_bp": 4_600_000,
+            "l2": "no flush: each step streams 150 MB of reads (> 126 MB L2) plus ~1 GB of scratch",
+            "parallelism": f"dp{world} read shards, index replica per GPU"}
+
+
+def measured_peaks() -> tuple[float, str]:
+    try:
+        j = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def stage_bytes(stage: str, st: dict, reads_per_step: float, mean_len: float, bw: int = 16) -> float:
+    """Algorithmic HBM bytes of one step for each pipeline stage (definitions in DESIGN.md)."""
+    n = reads_per_step
+    mins = st.get("minimizers_per_read", 0.18 * mean_len) * n
+    anchors = st["anchors"]
+    W = 2 * bw + 1
+    if stage == "seed":      # ASCII in, codes out (both strands), minimizers + probe results out, one bucket per probe
+        return n * mean_len * (1 + 2) + mins * (16 + 8 + 16) + n * 12
+    if stage == "chain":     # minimizers + probe results in, occurrence positions in, candidates out
+        return mins * 24 + anchors * 4 + st["candidates"] * 28 + n * 4
+    if stage == "sw_tb":     # query + target window in, direction nibbles written once, result out
+        tasks = st["sw_tasks_tb"]
+        return tasks * (mean_len + (mean_len + 2 * bw) + mean_len * ((W + 7) // 8) * 4 + 32)
+    if stage == "sw_score":
+        tasks = st["sw_tasks_score"]
+        return tasks * (mean_len + (mean_len + 2 * bw) + 32)
+    return n * (40 + 16)     # post: records + CIGARs out
+
+
+def cpu_baseline(g, reads, params) -> dict:
+    """The reference's CPU mapper on this host (all hardware threads), on one batch."""
+    import oracle
+    sample = reads.slice(0, min(len(reads), BATCH))
+    threads = len(os.sched_getaffinity(0))
+    if oracle.REF_SO.exists():
+        ref = oracle.Reference()
+        rg = ref.genome(g)
+        ref.time_map(rg, sample.slice(0, min(len(sample), 20_000)), params, threads)  # warm-up
+        reps, dt = 0, 0.0
+        while dt < 5.0 and reps < 20:   # >= ~5 s wall (x threads of CPU work)
+            dt += ref.time_map(rg, sample, params, threads)
+            reps += 1
+        one = sample.slice(0, min(len(sample), 50_000))
+        dt1 = ref.time_map(rg, one, params, 1)
+        return {"value": reps * len(sample) / dt, "unit": METRIC, "cores": threads, "kind": "reference",
+                "sample": f"{reps} x {len(sample):,} reads of the workload (one batch), Mapper::map with "
+                          f"{threads} threads (one Mapper per thread over read shards)",
+                "single_thread_value": len(one) / dt1, "cpu": _cpu_model()}
+    port = oracle.Port()
+    pi = port.index(g)
+    one = sample.slice(0, min(len(sample), 20_000))
+    t0 = time.perf_counter()
+    port.map(pi, one, params)
+    dt = time.perf_counter() - t0
+    return {"value": len(one) / dt, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"{len(one):,} reads of the workload, scalar C port, 1 thread", "cpu": _cpu_model()}
+
+
+def _cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args) -> None:
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    import dnaln_b200 as D
+    from dnaln_b200 import synth
+    g, reads, _ = synth.workload(WORKLOAD, seed=args.seed, n_reads=args.n_reads)
+    p = D.default_map_params()
+    threads = len(os.sched_getaffinity(0))
+    if oracle.REF_SO.exists():
+        ref, kind = oracle.Reference(), "reference"
+        rg = ref.genome(g)
+        run = lambda s: ref.time_map(rg, s, p, threads)  # noqa: E731
+        cores = threads
+        sample = reads
+    else:  # the C port, single-threaded, on a bounded sample
+        port, kind = oracle.Port(), "port"
+        pi = port.index(g)
+        sample = reads.slice(0, min(len(reads), 50_000))
+
+        def run(s):
+            t0 = time.perf_counter()
+            port.map(pi, s, p)
+            return time.perf_counter() - t0
+        cores = 1
+    for _ in range(args.warmup):
+        run(sample)
+    dt = sum(run(sample) for _ in range(args.steps))
+    value = args.steps * len(sample) / dt
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
+            "config": workload_config(len(sample), 1), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
+                             "sample": f"{len(sample):,} reads per step, Mapper::map, {cores} threads",
+                             "cpu": _cpu_model()},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import dnaln_b200 as D
+    from dnaln_b200 import _native as N
+    from dnaln_b200 import synth
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    g, reads, _ = synth.workload(WORKLOAD, seed=args.seed + 7919 * rank, n_reads=args.n_reads)
+    n_reads = len(reads)
+    p = D.default_map_params()
+    ctx = D.Context(local)
+    iid = ctx.index_build(g)
+    L = N.lib()
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    spans = [(a, min(n_reads, a + BATCH)) for a in range(0, n_reads, BATCH)]
+    parts = [reads.slice(a, b) for a, b in spans]
+
+    # ---- device-resident inputs (value) --------------------------------------------
+    dev = []
+    for part in parts:
+        n = len(part)
+        lens = part.seq_len
+        cap = int(np.sum(2 * lens.astype(np.int64) + 3))
+        dev.append(dict(
+            n=n, cap=cap,
+            seq=torch.from_numpy(part.seq).cuda(),
+            off=torch.from_numpy(np.ascontiguousarray(part.seq_off[:-1])).cuda(),
+            len=torch.from_numpy(lens).cuda(),
+            hash=torch.from_numpy(part.name_hash().view(np.int32)).cuda(),
+            out=torch.empty(n * 40, dtype=torch.uint8, device="cuda"),
+            cig=torch.empty(cap, dtype=torch.int32, device="cuda")))
+    used = C.c_int64()
+
+    def step_device():
+        for d in dev:
+            rc = L.dnaln_gpu_map_batch_device(ctx.handle, iid, d["seq"].data_ptr(), d["off"].data_ptr(),
+                                              d["len"].data_ptr(), d["hash"].data_ptr(), d["n"], C.byref(p),
+                                              d["out"].data_ptr(), d["cig"].data_ptr(), d["cap"], C.byref(used))
+            if rc:
+                raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(max(args.warmup, 3)):
+        step_device()
+    barrier()
+    ctx.reset_stats()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_device()
+    e1.record(stream)
+    barrier()
+    clk = clocks.result()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    st = ctx.stats()
+    value = world * n_reads * args.steps / (ms / 1e3)
+
+    # ---- end to end through the host-buffer C call (e2e) ----------------------------
+    host = []
+    for part in parts:
+        n = len(part)
+        lens = part.seq_len
+        cap = int(np.sum(2 * lens.astype(np.int64) + 3))
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        host.append(dict(n=n, cap=cap, seq=pin(part.seq), off=pin(part.seq_off[:-1]), len=pin(lens),
+                         hash=pin(part.name_hash().view(np.int32)),
+                         out=torch.empty(n * 40, dtype=torch.uint8).pin_memory(),
+                         cig=torch.empty(cap, dtype=torch.int32).pin_memory(),
+                         h2d=int(part.seq.nbytes) + 16 * n))
+    e2e_used = []
+
+    def step_e2e():
+        e2e_used.clear()
+        for h in host:
+            rc = L.dnaln_gpu_map_batch(ctx.handle, iid, h["seq"].data_ptr(), h["off"].data_ptr(), h["len"].data_ptr(),
+                                       h["hash"].data_ptr(), h["n"], C.byref(p), h["out"].data_ptr(),
+                                       h["cig"].data_ptr(), h["cap"], C.byref(used))
+            if rc:
+                raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
+            e2e_used.append(used.value)
+
+    e2e_steps = args.e2e_steps or args.steps
+    for _ in range(2):
+        step_e2e()
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        step_e2e()
+    f1.record(stream)
+    barrier()
+    wall_e2e = time.perf_counter() - w0
+    ms_e2e = max_over_ranks(f0.elapsed_time(f1))
+    e2e_value = world * n_reads * e2e_steps / (ms_e2e / 1e3)
+    h2d = sum(h["h2d"] for h in host)
+    d2h = sum(40 * h["n"] for h in host) + 4 * sum(e2e_used)
+
+    # ---- roofline of the dominant stage ---------------------------------------------
+    stage_ms = {"seed": st["ms_seed"], "chain": st["ms_chain"], "sw_score": st["ms_sw_score"], "sw_tb": st["ms_sw_tb"],
+                "post": st["ms_post"]}
+    dom = max(stage_ms, key=stage_ms.get)
+    per_step = {k: v / args.steps for k, v in st.items() if isinstance(v, (int, float))}
+    mean_len = float(np.mean(reads.seq_len))
+    launches_per_step = len(parts)  # one launch of the dominant stage's kernel per batch
+    bytes_step = stage_bytes(dom, per_step, n_reads, mean_len)
+    avg_launch_ms = stage_ms[dom] / (args.steps * launches_per_step)
+    achieved = (bytes_step / launches_per_step) / (avg_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tf = ROOT / "profiles" / f"traffic_{dom}.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    cells = st["cells"]
+    sw_ms = st["ms_sw_score"] + st["ms_sw_tb"]
+
+    out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+           "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, no dataset)",
+           "config": workload_config(n_reads, world),
+           "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "ms_per_step": ms_e2e / e2e_steps, "wall_s": wall_e2e},
+           "gpu_launches": int(st["launches"]),
+           "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                        "algorithmic_bytes_per_launch": bytes_step / launches_per_step,
+                        "avg_launch_ms": avg_launch_ms},
+           "stages_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
+           "sw_gcups": cells / (sw_ms / 1e3) / 1e9 if sw_ms > 0 else None,
+           "sw_cells_per_step": cells / args.steps,
+           "mapped_frac": st["mapped"] / max(st["reads"], 1),
+           "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(g, reads, p)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

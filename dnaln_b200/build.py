@@ -1,0 +1,89 @@
+"""Build of the in-tree native library ``dnaln_b200/libdnaln_b200.so``.
+
+CUDA sources are compiled for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``);
+host C++ sources with g++. Objects go to ``dnaln_b200/_build/``; the shared library is
+linked with the static CUDA runtime, so loading it needs no GPU (CUDA calls then fail
+with DNALN_ERR_NO_DEVICE). Rebuilds only when a source or header is newer than the
+library. Run ``python -m dnaln_b200.build`` or call :func:`build`.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+BUILD = PKG / "_build"
+LIB = PKG / "libdnaln_b200.so"
+
+CUDA_SOURCES = ["csrc/sw.cu", "csrc/seed.cu", "csrc/map.cu", "csrc/capi.cu"]
+HOST_SOURCES = ["host/index_host.cpp", "host/sam.cpp", "host/synth.cpp"]
+HEADERS = ["csrc/common.cuh", "csrc/sw.cuh", "csrc/seed.cuh", "csrc/map.cuh", "host/index_host.hpp"]
+PUBLIC_HEADERS = ["dnaln_b200.h", "dnaln_synth.h"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found (CUDA toolkit required to build dnaln_b200)")
+
+
+def _includes() -> list[str]:
+    return [f"-I{ROOT / 'include'}", f"-I{PKG / 'csrc'}", f"-I{PKG / 'host'}"]
+
+
+def _newest_input() -> float:
+    files = [PKG / s for s in CUDA_SOURCES + HOST_SOURCES + HEADERS] + [ROOT / "include" / h for h in PUBLIC_HEADERS]
+    files.append(Path(__file__))
+    return max(f.stat().st_mtime for f in files)
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"build step failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+
+
+def _compile_cuda(src: str, nvcc: str, extra: list[str]) -> Path:
+    obj = BUILD / (Path(src).stem + ".cu.o")
+    cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC",
+           *_includes(), *extra, "-c", str(PKG / src), "-o", str(obj)]
+    _run(cmd)
+    return obj
+
+
+def _compile_host(src: str) -> Path:
+    obj = BUILD / (Path(src).stem + ".o")
+    cxx = os.environ.get("CXX", "g++")
+    _run([cxx, "-O3", "-std=c++17", "-fPIC", "-Wall", "-Wextra", *_includes(), "-c", str(PKG / src), "-o", str(obj)])
+    return obj
+
+
+def build(force: bool = False, verbose: bool = False, extra_nvcc: list[str] | None = None) -> Path:
+    """Compiles the CUDA and host sources and links ``libdnaln_b200.so``; returns its path."""
+    if not force and LIB.exists() and LIB.stat().st_mtime >= _newest_input():
+        return LIB
+    BUILD.mkdir(exist_ok=True)
+    nvcc = _nvcc()
+    extra = list(extra_nvcc or [])
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:
+        futs = [ex.submit(_compile_cuda, s, nvcc, extra) for s in CUDA_SOURCES]
+        futs += [ex.submit(_compile_host, s) for s in HOST_SOURCES]
+        objs = [f.result() for f in futs]
+    tmp = LIB.with_suffix(".so.tmp")
+    _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lpthread"])
+    os.replace(tmp, LIB)
+    if verbose:
+        print(f"built {LIB}", file=sys.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

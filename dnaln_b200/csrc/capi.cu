@@ -1,0 +1,930 @@
+// capi.cu — the C ABI (include/dnaln_b200.h): contexts, HBM-resident genome indexes, and
+// the orchestration of each batch through the kernels of seed.cu, sw.cu and map.cu.
+//
+// One batch (Mapper::map, src/mapper.cpp:75-223) runs as:
+//   lengths -> packed offsets (scan)                         [1 small host read-back]
+//   k_seed: encode both strands, sketch, probe, anchor counts
+//   anchor offsets (scan)                                    [1 small host read-back]
+//   k_chain_map: anchors, sort, chaining DP, chains, candidate loci
+//   score-only SW over every candidate of reads with >= 2 candidates
+//   k_choose: best / ties / second best, fnv1a tie-break, traceback tasks
+//   SW with traceback over each read's chosen candidate (chunked by scratch size)
+//   k_records: MAPQ, positions, soft clips; CIGAR offsets (scan)  [1 host read-back]
+//   k_cigar_gather: final CIGARs
+// Task counts produced on the device are consumed on the device (kernels read them), so
+// the host only waits where it must size a buffer.
+#include <cub/device/device_reduce.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "dnaln_b200.h"
+#include "index_host.hpp"
+#include "map.cuh"
+#include "seed.cuh"
+#include "sw.cuh"
+
+using namespace dnb;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct IndexRes {
+  DevBuf table, positions, genome, coff, clen;
+  uint64_t n_keys = 0, n_pos = 0, n_buckets = 0, n_bases = 0;
+  uint32_t max_count = 0;
+  int32_t n_contigs = 0, k = 0, w = 0;
+  DevIndex dev{};
+};
+
+enum Ev { kEvSeed0, kEvSeed1, kEvChain0, kEvChain1, kEvSc0, kEvSc1, kEvTb0, kEvTb1, kEvPost0, kEvPost1, kEvH2d0,
+          kEvH2d1, kEvD2h0, kEvD2h1, kNumEv };
+
+}  // namespace
+
+struct dnaln_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr, st = nullptr;
+  std::string err;
+  std::map<int32_t, IndexRes> idx;
+  int32_t next_id = 1;
+  std::map<std::string, DevBuf> bufs;
+  uint32_t* d_err = nullptr;   // kernel error flags
+  int* d_count = nullptr;      // [0] score tasks, [1] traceback tasks
+  int64_t* h_info = nullptr;   // pinned read-back slots
+  cudaEvent_t ev[kNumEv] = {};
+  dnaln_stats stats{};
+  size_t dir_cap_bytes = size_t(1) << 30;  // direction-bit scratch per traceback launch
+};
+
+namespace {
+
+int fail(dnaln_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    const cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) return fail(c, DNALN_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+// Grow-only device buffer; returns nullptr (and sets the context error) on failure.
+template <class T>
+T* dbuf(dnaln_ctx* c, const char* name, size_t count) {
+  DevBuf& b = c->bufs[name];
+  const size_t need = (count ? count : 1) * sizeof(T);
+  if (b.cap < need) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t cap = need + need / 4;
+    if (cudaMalloc(&b.p, cap) != cudaSuccess) {
+      cudaGetLastError();
+      cap = need;
+      if (cudaMalloc(&b.p, cap) != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        fail(c, DNALN_ERR_OOM, "out of device memory allocating %zu bytes for %s", need, name);
+        return nullptr;
+      }
+    }
+    b.cap = cap;
+  }
+  return static_cast<T*>(b.p);
+}
+
+#define DBUF(ptr, T, name, count)                         \
+  T* ptr = dbuf<T>(c, name, (count));                     \
+  if (!ptr) return DNALN_ERR_OOM;
+
+int set_device(dnaln_ctx* c) {
+  CK(cudaSetDevice(c->device));
+  return DNALN_OK;
+}
+
+int exclusive_scan(dnaln_ctx* c, const int64_t* in, int64_t* out, int64_t n) {
+  size_t tmp = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, c->st));
+  DBUF(t, uint8_t, "cub_tmp", tmp);
+  CK(cub::DeviceScan::ExclusiveSum(t, tmp, in, out, n, c->st));
+  return DNALN_OK;
+}
+
+double ev_ms(dnaln_ctx* c, int a, int b) {
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]) != cudaSuccess) {
+    cudaGetLastError();
+    return 0.0;
+  }
+  return ms;
+}
+
+bool score_params_ok(const dnaln_score_params& s, std::string& why) {
+  // src/cli.hpp:93-95 (bw in [1, 1000]; A >= 1, B >= 0, O >= 0, E >= 1)
+  if (s.bw < 1 || s.bw > 1000) return why = "--bw must be in [1, 1000]", false;
+  if (s.match < 1 || s.mismatch < 0 || s.gap_open < 0 || s.gap_ext < 1)
+    return why = "scores must satisfy A >= 1, B >= 0, O >= 0, E >= 1", false;
+  if (s.ambig < 0) return why = "ambiguous-base penalty must be >= 0", false;
+  return true;
+}
+
+// Gap cost of the chaining DP for dd in [0, band] (src/chain.cpp:36).
+std::vector<int32_t> chain_cost_lut(int k, int band) {
+  std::vector<int32_t> lut(static_cast<size_t>(band) + 1, 0);
+  for (int dd = 1; dd <= band; ++dd) {
+    const int lg = 63 - __builtin_clzll(static_cast<unsigned long long>(dd));
+    lut[static_cast<size_t>(dd)] = static_cast<int>(0.01 * k * static_cast<double>(dd) + 0.5 * lg);
+  }
+  return lut;
+}
+
+__global__ void k_len64(const int32_t* __restrict__ len, int64_t n, int64_t* __restrict__ out,
+                        unsigned long long* __restrict__ max_len) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const int32_t l = len[i];
+    out[i] = l < 0 ? 0 : l;
+    atomicMax(max_len, static_cast<unsigned long long>(l < 0 ? 0 : l));
+  } else if (i == n) {
+    out[n] = 0;
+  }
+}
+
+__global__ void k_cig_slots(const int64_t* __restrict__ pofs, int64_t n, int64_t* __restrict__ out) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = 2 * pofs[i] + i;
+}
+
+inline unsigned nblk(int64_t n, int t = 256) { return static_cast<unsigned>((n + t - 1) / t); }
+
+int check_device_errors(dnaln_ctx* c, uint32_t bits) {
+  if (bits == 0) return DNALN_OK;
+  return fail(c, DNALN_ERR_DEVICE, "kernel error flags 0x%x (traceback bounds %d, cigar overflow %d, chain scratch %d, "
+                                   "probe loop %d)",
+              bits, !!(bits & kErrTracebackBounds), !!(bits & kErrCigarOverflow), !!(bits & kErrChainScratch),
+              !!(bits & kErrProbeLoop));
+}
+
+// Launches traceback SW over tasks [0, n_max) (count read on the device from n_dev),
+// chunked so the direction-bit scratch stays within dir_cap_bytes.
+int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks, int n_max, const int* n_dev,
+                      const uint8_t* qbase, const uint8_t* tbase, const SwParams& sp, SwResult* res, int rows_max,
+                      uint32_t* cig, const int64_t* cig_off) {
+  if (n_max <= 0) return DNALN_OK;
+  const size_t dir_w = tb ? sw_dir_bytes_per_warp(sp.W, rows_max > 0 ? rows_max : 1) : 0;
+  const size_t band_w = sw_band_bytes_per_warp(sp.W, bytes_ok);
+  const size_t per_warp = dir_w + band_w;
+  int64_t chunk = n_max;
+  if (per_warp > 0) {
+    const int64_t warps = static_cast<int64_t>(c->dir_cap_bytes / per_warp);
+    chunk = (warps < 1 ? 1 : warps) * 32;
+    if (chunk > n_max) chunk = ((n_max + 31) / 32) * 32;
+  }
+  const int64_t chunk_warps = (chunk + 31) / 32;
+  uint32_t* dir = nullptr;
+  int* band = nullptr;
+  if (dir_w) {
+    dir = dbuf<uint32_t>(c, "sw_dir", static_cast<size_t>(chunk_warps) * dir_w / sizeof(uint32_t));
+    if (!dir) return DNALN_ERR_OOM;
+  }
+  if (band_w) {
+    band = dbuf<int>(c, "sw_band", static_cast<size_t>(chunk_warps) * band_w / sizeof(int));
+    if (!band) return DNALN_ERR_OOM;
+  }
+  for (int64_t b = 0; b < n_max; b += chunk) {
+    const int cnt = static_cast<int>(n_max - b < chunk ? n_max - b : chunk);
+    if (!launch_sw(c->st, tb, bytes_ok, tasks, static_cast<int>(b), cnt, n_max, n_dev, qbase, tbase, sp, res, dir,
+                   rows_max, cig, cig_off, band, c->d_err))
+      return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
+    ++c->stats.launches;
+  }
+  CK(cudaGetLastError());
+  return DNALN_OK;
+}
+
+int validate_map_params(dnaln_ctx* c, const dnaln_map_params* p, const IndexRes& ix) {
+  if (!p) return fail(c, DNALN_ERR_INVALID_ARG, "null map params");
+  std::string why;
+  if (!score_params_ok(p->sc, why)) return fail(c, DNALN_ERR_INVALID_ARG, "%s", why.c_str());
+  if (p->k != ix.k || p->w != ix.w)
+    return fail(c, DNALN_ERR_INVALID_ARG, "map k/w (%d/%d) differ from the index's (%d/%d)", p->k, p->w, ix.k, ix.w);
+  if (p->max_cand < 1 || p->max_cand > 1024) return fail(c, DNALN_ERR_INVALID_ARG, "max_cand must be in [1, 1024]");
+  if (p->ch.lookback < 0 || p->ch.band < 0 || p->ch.band > (1 << 20))
+    return fail(c, DNALN_ERR_INVALID_ARG, "chain lookback must be >= 0 and band in [0, 2^20]");
+  return DNALN_OK;
+}
+
+// The device pipeline. Inputs and d_out in device memory; CIGARs go to d_cigar
+// (capacity cigar_cap) or, when d_cigar is null, to an internal buffer returned via
+// *cigar_dev. *cigar_used = total ops.
+int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_off, const int32_t* d_seq_len,
+            const uint32_t* d_hash, int64_t n, const dnaln_map_params& p, dnaln_map_record* d_out, uint32_t* d_cigar,
+            int64_t cigar_cap, int64_t* cigar_used, uint32_t** cigar_dev) {
+  cudaStream_t st = c->st;
+  const int bw = p.sc.bw, W = 2 * bw + 1, MC = p.max_cand;
+  const int chain_band = p.ch.band < bw ? p.ch.band : bw;  // src/mapper.cpp:9
+  *cigar_used = 0;
+  if (n == 0) return DNALN_OK;
+
+  // packed offsets, total bases, longest read
+  DBUF(len64, int64_t, "len64", n + 1);
+  DBUF(pofs, int64_t, "pofs", n + 1);
+  DBUF(info, unsigned long long, "info", 4);
+  CK(cudaMemsetAsync(info, 0, 4 * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
+  CK(cudaMemsetAsync(c->d_count, 0, 2 * sizeof(int), st));
+  unsigned long long* ctr = info + 1;  // cells, mapped, candidates (map.cuh)
+  k_len64<<<nblk(n + 1), 256, 0, st>>>(d_seq_len, n, len64, info);
+  if (int e = exclusive_scan(c, len64, pofs, n + 1)) return e;
+  CK(cudaMemcpyAsync(c->h_info, pofs + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 1, info, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const int64_t B = c->h_info[0];
+  const int64_t max_len = c->h_info[1];
+  if (max_len > (1 << 28)) return fail(c, DNALN_ERR_INVALID_ARG, "read longer than 2^28 bases");
+
+  // pass 1: encode, sketch, probe
+  DBUF(codes, uint8_t, "codes", 2 * B);
+  MinBuf mb;
+  mb.hash = dbuf<uint64_t>(c, "m_hash", B);
+  mb.pos = dbuf<uint32_t>(c, "m_pos", B);
+  mb.hit_off = dbuf<uint32_t>(c, "m_off", B);
+  mb.hit_cnt = dbuf<uint32_t>(c, "m_cnt", B);
+  if (!mb.hash || !mb.pos || !mb.hit_off || !mb.hit_cnt) return DNALN_ERR_OOM;
+  DBUF(n_min, int32_t, "n_min", n);
+  DBUF(n_anchor, int64_t, "n_anchor", n + 1);
+  DBUF(anchor_off, int64_t, "anchor_off", n + 1);
+  CK(cudaMemsetAsync(n_anchor + n, 0, sizeof(int64_t), st));
+  SeedParams sp{p.k, p.w, p.max_occ};
+  CK(cudaEventRecord(c->ev[kEvSeed0], st));
+  launch_seed(st, d_seq, d_seq_off, d_seq_len, pofs, n, codes, ix.dev, sp, mb, n_min, n_anchor, c->d_err);
+  CK(cudaEventRecord(c->ev[kEvSeed1], st));
+  CK(cudaGetLastError());
+  if (int e = exclusive_scan(c, n_anchor, anchor_off, n + 1)) return e;
+  CK(cudaMemcpyAsync(c->h_info, anchor_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const int64_t A = c->h_info[0];
+
+  // pass 2: anchors, chains, candidates
+  AnchorScratch as;
+  as.keys = dbuf<uint64_t>(c, "a_keys", A);
+  as.f = dbuf<int32_t>(c, "a_f", A);
+  as.prev = dbuf<int32_t>(c, "a_prev", A);
+  as.ord = dbuf<uint64_t>(c, "a_ord", A);
+  as.used = dbuf<uint8_t>(c, "a_used", A);
+  as.ch_score = dbuf<int32_t>(c, "c_score", A);
+  as.ch_sn = dbuf<uint32_t>(c, "c_sn", A);
+  as.ch_dmin = dbuf<int64_t>(c, "c_dmin", A);
+  as.ch_dmax = dbuf<int64_t>(c, "c_dmax", A);
+  as.ch_rpos = dbuf<uint32_t>(c, "c_rpos", A);
+  if (!as.keys || !as.f || !as.prev || !as.ord || !as.used || !as.ch_score || !as.ch_sn || !as.ch_dmin ||
+      !as.ch_dmax || !as.ch_rpos)
+    return DNALN_ERR_OOM;
+  CandBuf cb;
+  cb.n_cand = dbuf<int32_t>(c, "cand_n", n);
+  cb.rev = dbuf<uint8_t>(c, "cand_rev", n * MC);
+  cb.contig = dbuf<int32_t>(c, "cand_contig", n * MC);
+  cb.diag = dbuf<int64_t>(c, "cand_diag", n * MC);
+  cb.wstart = dbuf<int64_t>(c, "cand_wstart", n * MC);
+  if (!cb.n_cand || !cb.rev || !cb.contig || !cb.diag || !cb.wstart) return DNALN_ERR_OOM;
+  const std::vector<int32_t> lut = chain_cost_lut(p.k, chain_band);
+  DBUF(d_lut, int32_t, "chain_lut", lut.size());
+  CK(cudaMemcpyAsync(d_lut, lut.data(), lut.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  ChainParamsDev cp{p.ch.max_gap, chain_band, p.ch.lookback, p.ch.min_score, p.ch.min_anchors, p.k, d_lut};
+  CandParams cand{MC, bw, p.pri_ratio};
+  CK(cudaEventRecord(c->ev[kEvChain0], st));
+  launch_chain_map(st, pofs, d_seq_len, n, n_min, anchor_off, mb, ix.dev, cp, cand, as, cb, c->d_err);
+  CK(cudaEventRecord(c->ev[kEvChain1], st));
+  CK(cudaGetLastError());
+
+  // score-only ranking of multi-candidate reads
+  const dnaln_score_params& sc = p.sc;
+  const SwParams swp = make_sw_params(sc);
+  const bool bytes_ok = sw_bytes_ok(sc);
+  MapConsts mc{MC, bw, W, p.min_aln_score, sc.match};
+  DBUF(sc_tasks, SwTask, "sc_tasks", n * MC);
+  DBUF(res_sc, SwResult, "res_sc", n * MC);
+  CK(cudaEventRecord(c->ev[kEvSc0], st));
+  launch_score_tasks(st, n, pofs, d_seq_len, cb, ix.dev, mc, sc_tasks, c->d_count, ctr);
+  if (int e = launch_sw_chunked(c, false, bytes_ok, sc_tasks, static_cast<int>(n * MC), c->d_count, codes,
+                                ix.dev.genome, swp, res_sc, static_cast<int>(max_len), nullptr, nullptr))
+    return e;
+  CK(cudaEventRecord(c->ev[kEvSc1], st));
+
+  // choose, then traceback on the chosen candidate
+  DBUF(chosen, int32_t, "chosen", n);
+  DBUF(s2, int32_t, "s2", n);
+  DBUF(tb_tasks, SwTask, "tb_tasks", n);
+  DBUF(res_tb, SwResult, "res_tb", n);
+  DBUF(cig_tb, uint32_t, "cig_tb", 2 * B + n);
+  DBUF(cig_slot, int64_t, "cig_slot", n);
+  CK(cudaEventRecord(c->ev[kEvTb0], st));
+  launch_choose(st, n, pofs, d_seq_len, cb, res_sc, d_hash, ix.dev, mc, chosen, s2, tb_tasks, c->d_count + 1, ctr);
+  k_cig_slots<<<nblk(n), 256, 0, st>>>(pofs, n, cig_slot);
+  if (int e = launch_sw_chunked(c, true, bytes_ok, tb_tasks, static_cast<int>(n), c->d_count + 1, codes,
+                                ix.dev.genome, swp, res_tb, static_cast<int>(max_len), cig_tb, cig_slot))
+    return e;
+  CK(cudaEventRecord(c->ev[kEvTb1], st));
+
+  // records, CIGAR offsets and compaction
+  DBUF(cig_cnt, int64_t, "cig_cnt", n + 1);
+  DBUF(cig_off, int64_t, "cig_off", n + 1);
+  CK(cudaEventRecord(c->ev[kEvPost0], st));
+  launch_records(st, n, d_seq_len, cb, chosen, s2, res_tb, ix.dev, mc, d_out, cig_cnt, ctr);
+  if (int e = exclusive_scan(c, cig_cnt, cig_off, n + 1)) return e;
+  CK(cudaMemcpyAsync(c->h_info, cig_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 1, c->d_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 2, c->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 3, ctr, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const int64_t total_ops = c->h_info[0];
+  const uint64_t n_cells = static_cast<uint64_t>(c->h_info[3]), n_mapped = static_cast<uint64_t>(c->h_info[4]),
+                 n_cands = static_cast<uint64_t>(c->h_info[5]);
+  int counts[2];
+  std::memcpy(counts, c->h_info + 1, sizeof counts);
+  uint32_t errbits;
+  std::memcpy(&errbits, c->h_info + 2, sizeof errbits);
+  if (int e = check_device_errors(c, errbits)) return e;
+  *cigar_used = total_ops;
+  if (!d_cigar) {
+    d_cigar = dbuf<uint32_t>(c, "cig_out", total_ops);
+    if (!d_cigar) return DNALN_ERR_OOM;
+    cigar_cap = total_ops;
+  }
+  if (cigar_dev) *cigar_dev = d_cigar;
+  if (total_ops > cigar_cap)
+    return fail(c, DNALN_ERR_CAPACITY, "CIGAR buffer holds %lld ops, batch needs %lld",
+                static_cast<long long>(cigar_cap), static_cast<long long>(total_ops));
+  launch_cigar_gather(st, n, pofs, d_seq_len, res_tb, cig_tb, cig_off, d_out, d_cigar);
+  CK(cudaEventRecord(c->ev[kEvPost1], st));
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+
+  dnaln_stats& s = c->stats;
+  s.reads += static_cast<uint64_t>(n);
+  s.anchors += static_cast<uint64_t>(A);
+  s.sw_tasks_score += static_cast<uint64_t>(counts[0]);
+  s.sw_tasks_tb += static_cast<uint64_t>(counts[1]);
+  s.cells += n_cells;
+  s.mapped += n_mapped;
+  s.candidates += n_cands;
+  s.launches += 8;  // k_len64, k_seed, k_chain_map, k_score_tasks, k_choose, k_cig_slots, k_records, k_cigar_gather
+  s.ms_seed += ev_ms(c, kEvSeed0, kEvSeed1);
+  s.ms_chain += ev_ms(c, kEvChain0, kEvChain1);
+  s.ms_sw_score += ev_ms(c, kEvSc0, kEvSc1);
+  s.ms_sw_tb += ev_ms(c, kEvTb0, kEvTb1);
+  s.ms_post += ev_ms(c, kEvPost0, kEvPost1);
+  s.ms_total += ev_ms(c, kEvSeed0, kEvPost1);
+  return DNALN_OK;
+}
+
+IndexRes* find_index(dnaln_ctx* c, int32_t id) {
+  auto it = c->idx.find(id);
+  if (it == c->idx.end()) {
+    fail(c, DNALN_ERR_NOT_FOUND, "unknown index id %d", id);
+    return nullptr;
+  }
+  return &it->second;
+}
+
+int dalloc(dnaln_ctx* c, DevBuf& b, size_t bytes) {
+  if (cudaMalloc(&b.p, bytes ? bytes : 1) != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    return fail(c, DNALN_ERR_OOM, "out of device memory allocating %zu bytes for the index", bytes);
+  }
+  b.cap = bytes;
+  return DNALN_OK;
+}
+
+void free_index(IndexRes& r) {
+  for (DevBuf* b : {&r.table, &r.positions, &r.genome, &r.coff, &r.clen})
+    if (b->p) cudaFree(b->p);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dnaln_gpu_version(void) { return "dnaln-b200 0.1.0 (sm_100a)"; }
+
+uint32_t dnaln_fnv1a(const char* s, int64_t n) {  // src/common.hpp:136-140
+  uint32_t h = 2166136261u;
+  for (int64_t i = 0; i < n; ++i) h = (h ^ static_cast<unsigned char>(s[i])) * 16777619u;
+  return h;
+}
+
+void dnaln_fnv1a_batch(const char* names, const int64_t* name_off, int64_t n, uint32_t* out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = dnaln_fnv1a(names + name_off[i], name_off[i + 1] - name_off[i]);
+}
+
+int dnaln_gpu_ctx_create(int device, dnaln_ctx** out) {
+  if (!out) return DNALN_ERR_INVALID_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return DNALN_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return DNALN_ERR_NO_DEVICE;
+  auto* c = new dnaln_ctx;
+  c->device = device;
+  int e = DNALN_OK;
+  auto bad = [&](cudaError_t x) {
+    if (x != cudaSuccess && e == DNALN_OK) e = fail(c, DNALN_ERR_CUDA, "%s", cudaGetErrorString(x));
+  };
+  bad(cudaSetDevice(device));
+  bad(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+  c->st = c->own;
+  for (auto& x : c->ev) bad(cudaEventCreate(&x));
+  bad(cudaMalloc(&c->d_err, sizeof(uint32_t)));
+  bad(cudaMalloc(&c->d_count, 4 * sizeof(int)));
+  bad(cudaHostAlloc(&c->h_info, 8 * sizeof(int64_t), cudaHostAllocDefault));
+  if (e != DNALN_OK) {
+    dnaln_gpu_ctx_destroy(c);
+    return e;
+  }
+  *out = c;
+  return DNALN_OK;
+}
+
+int dnaln_gpu_ctx_destroy(dnaln_ctx* c) {
+  if (!c) return DNALN_OK;
+  cudaSetDevice(c->device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (auto& kv : c->idx) free_index(kv.second);
+  for (auto& kv : c->bufs)
+    if (kv.second.p) cudaFree(kv.second.p);
+  for (auto& x : c->ev)
+    if (x) cudaEventDestroy(x);
+  if (c->d_err) cudaFree(c->d_err);
+  if (c->d_count) cudaFree(c->d_count);
+  if (c->h_info) cudaFreeHost(c->h_info);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return DNALN_OK;
+}
+
+const char* dnaln_gpu_last_error(const dnaln_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int dnaln_gpu_set_stream(dnaln_ctx* c, void* stream) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  c->st = stream ? static_cast<cudaStream_t>(stream) : c->own;
+  return DNALN_OK;
+}
+
+int dnaln_gpu_get_stats(const dnaln_ctx* c, dnaln_stats* out) {
+  if (!c || !out) return DNALN_ERR_INVALID_ARG;
+  *out = c->stats;
+  return DNALN_OK;
+}
+
+int dnaln_gpu_reset_stats(dnaln_ctx* c) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  c->stats = dnaln_stats{};
+  return DNALN_OK;
+}
+
+int dnaln_gpu_host_alloc(dnaln_ctx* c, size_t bytes, void** out) {
+  if (!c || !out) return DNALN_ERR_INVALID_ARG;
+  if (int e = set_device(c)) return e;
+  CK(cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault));
+  return DNALN_OK;
+}
+
+int dnaln_gpu_host_free(dnaln_ctx* c, void* p) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  if (p) CK(cudaFreeHost(p));
+  return DNALN_OK;
+}
+
+int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases, const uint64_t* contig_off,
+                          const uint32_t* contig_len, int32_t n_contigs, int32_t k, int32_t w, int32_t* index_id) {
+  if (!c || !genome || !contig_off || !contig_len || !index_id || n_contigs < 1)
+    return fail(c, DNALN_ERR_INVALID_ARG, "null argument or no contigs");
+  if (k < 4 || k > 28) return fail(c, DNALN_ERR_INVALID_ARG, "k must be in [4, 28] (got %d)", k);
+  if (w < 1 || w > 255) return fail(c, DNALN_ERR_INVALID_ARG, "w must be in [1, 255] (got %d)", w);
+  if (n_bases >= (1ULL << 31)) return fail(c, DNALN_ERR_INVALID_ARG, "reference is too large (limit: 2^31 bp)");
+  for (int32_t i = 0; i < n_contigs; ++i)
+    if (contig_off[i] + contig_len[i] > n_bases || (i > 0 && contig_off[i] < contig_off[i - 1]))
+      return fail(c, DNALN_ERR_INVALID_ARG, "contig %d is outside the genome or out of order", i);
+  if (int e = set_device(c)) return e;
+  HostIndex h;
+  build_index_host(genome, contig_off, contig_len, n_contigs, k, w, h);
+  IndexRes r;
+  r.n_keys = h.n_keys;
+  r.n_pos = h.pos.size();
+  r.n_buckets = h.keys.size();
+  r.n_bases = n_bases;
+  r.max_count = h.max_count;
+  r.n_contigs = n_contigs;
+  r.k = k;
+  r.w = w;
+  std::vector<ulonglong2> table(h.keys.size());
+  for (size_t i = 0; i < table.size(); ++i)
+    table[i] = make_ulonglong2(h.keys[i], static_cast<uint64_t>(h.offs[i]) | static_cast<uint64_t>(h.cnts[i]) << 32);
+  int e = DNALN_OK;
+  if ((e = dalloc(c, r.table, table.size() * sizeof(ulonglong2))) ||
+      (e = dalloc(c, r.positions, h.pos.size() * sizeof(uint32_t))) || (e = dalloc(c, r.genome, n_bases)) ||
+      (e = dalloc(c, r.coff, n_contigs * sizeof(uint64_t))) || (e = dalloc(c, r.clen, n_contigs * sizeof(uint32_t)))) {
+    free_index(r);
+    return e;
+  }
+  cudaError_t x = cudaSuccess;
+  auto up = [&](DevBuf& b, const void* src, size_t bytes) {
+    if (x == cudaSuccess && bytes) x = cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
+  };
+  up(r.table, table.data(), table.size() * sizeof(ulonglong2));
+  up(r.positions, h.pos.data(), h.pos.size() * sizeof(uint32_t));
+  up(r.genome, genome, n_bases);
+  up(r.coff, contig_off, n_contigs * sizeof(uint64_t));
+  up(r.clen, contig_len, n_contigs * sizeof(uint32_t));
+  if (x != cudaSuccess) {
+    free_index(r);
+    return fail(c, DNALN_ERR_CUDA, "index upload: %s", cudaGetErrorString(x));
+  }
+  r.dev.table = static_cast<const ulonglong2*>(r.table.p);
+  r.dev.positions = static_cast<const uint32_t*>(r.positions.p);
+  r.dev.genome = static_cast<const uint8_t*>(r.genome.p);
+  r.dev.contig_off = static_cast<const uint64_t*>(r.coff.p);
+  r.dev.contig_len = static_cast<const uint32_t*>(r.clen.p);
+  r.dev.mask = h.mask;
+  r.dev.n_contigs = n_contigs;
+  r.dev.k = k;
+  r.dev.w = w;
+  const int32_t id = c->next_id++;
+  c->idx[id] = r;
+  *index_id = id;
+  return DNALN_OK;
+}
+
+int dnaln_gpu_index_stats(const dnaln_ctx* cc, int32_t id, uint64_t out6[6]) {
+  auto* c = const_cast<dnaln_ctx*>(cc);
+  if (!c || !out6) return DNALN_ERR_INVALID_ARG;
+  IndexRes* r = find_index(c, id);
+  if (!r) return DNALN_ERR_NOT_FOUND;
+  out6[0] = r->n_keys;
+  out6[1] = r->n_pos;
+  out6[2] = r->max_count;
+  out6[3] = r->n_buckets * 16 + r->n_pos * 4;  // src/index.hpp:46
+  out6[4] = r->n_buckets;
+  out6[5] = r->table.cap + r->positions.cap + r->genome.cap + r->coff.cap + r->clen.cap;
+  return DNALN_OK;
+}
+
+int dnaln_gpu_index_export(dnaln_ctx* c, int32_t id, uint64_t* keys, uint32_t* offsets, uint32_t* counts,
+                           uint32_t* positions) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  if (int e = set_device(c)) return e;
+  IndexRes* r = find_index(c, id);
+  if (!r) return DNALN_ERR_NOT_FOUND;
+  std::vector<ulonglong2> t(r->n_buckets);
+  CK(cudaMemcpy(t.data(), r->table.p, t.size() * sizeof(ulonglong2), cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < t.size(); ++i) {
+    if (keys) keys[i] = t[i].x;
+    if (offsets) offsets[i] = static_cast<uint32_t>(t[i].y);
+    if (counts) counts[i] = static_cast<uint32_t>(t[i].y >> 32);
+  }
+  if (positions && r->n_pos)
+    CK(cudaMemcpy(positions, r->positions.p, r->n_pos * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  return DNALN_OK;
+}
+
+int dnaln_gpu_index_free(dnaln_ctx* c, int32_t id) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  if (int e = set_device(c)) return e;
+  IndexRes* r = find_index(c, id);
+  if (!r) return DNALN_ERR_NOT_FOUND;
+  cudaStreamSynchronize(c->st);
+  free_index(*r);
+  c->idx.erase(id);
+  return DNALN_OK;
+}
+
+int dnaln_gpu_sketch(dnaln_ctx* c, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,
+                     const uint32_t* pos_offset, int64_t n, int32_t k, int32_t w, uint64_t* out_hash,
+                     uint32_t* out_pos, uint32_t* out_strand, int32_t* out_count) {
+  if (!c || n < 0 || (n > 0 && (!codes || !seq_off || !seq_len || !out_hash || !out_pos || !out_strand || !out_count)))
+    return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
+  if (k < 1 || k > 31) return fail(c, DNALN_ERR_INVALID_ARG, "k must be in [1, 31] (got %d)", k);
+  if (w < 1 || w > 255) return fail(c, DNALN_ERR_INVALID_ARG, "w must be in [1, 255] (got %d)", w);
+  if (n == 0) return DNALN_OK;
+  if (int e = set_device(c)) return e;
+  int64_t ext = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (seq_len[i] < 0 || seq_off[i] < 0) return fail(c, DNALN_ERR_INVALID_ARG, "negative offset or length");
+    ext = std::max<int64_t>(ext, seq_off[i] + seq_len[i]);
+  }
+  cudaStream_t st = c->st;
+  DBUF(d_codes, uint8_t, "sk_codes", ext);
+  DBUF(d_off, int64_t, "sk_off", n);
+  DBUF(d_len, int32_t, "sk_len", n);
+  DBUF(d_po, uint32_t, "sk_po", n);
+  DBUF(d_h, uint64_t, "sk_h", ext);
+  DBUF(d_p, uint32_t, "sk_p", ext);
+  DBUF(d_s, uint32_t, "sk_s", ext);
+  DBUF(d_cnt, int32_t, "sk_cnt", n);
+  CK(cudaMemcpyAsync(d_codes, codes, ext, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_off, seq_off, n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_len, seq_len, n * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  if (pos_offset) CK(cudaMemcpyAsync(d_po, pos_offset, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  launch_sketch_codes(st, d_codes, d_off, d_len, pos_offset ? d_po : nullptr, n, k, w, d_h, d_p, d_s, d_cnt);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out_hash, d_h, ext * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out_pos, d_p, ext * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out_strand, d_s, ext * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out_count, d_cnt, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return DNALN_OK;
+}
+
+int dnaln_gpu_lookup(dnaln_ctx* c, int32_t id, const uint64_t* hashes, int64_t n, uint32_t* out_offset,
+                     uint32_t* out_count) {
+  if (!c || n < 0 || (n > 0 && (!hashes || !out_offset || !out_count)))
+    return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
+  if (int e = set_device(c)) return e;
+  IndexRes* r = find_index(c, id);
+  if (!r) return DNALN_ERR_NOT_FOUND;
+  if (n == 0) return DNALN_OK;
+  cudaStream_t st = c->st;
+  DBUF(d_h, uint64_t, "lk_h", n);
+  DBUF(d_o, uint32_t, "lk_o", n);
+  DBUF(d_c, uint32_t, "lk_c", n);
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
+  CK(cudaMemcpyAsync(d_h, hashes, n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  launch_lookup(st, r->dev, d_h, n, d_o, d_c, c->d_err);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out_offset, d_o, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out_count, d_c, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  uint32_t bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->d_err, sizeof bits, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return check_device_errors(c, bits);
+}
+
+int dnaln_gpu_chain(dnaln_ctx* c, uint32_t* rpos, int32_t* qpos, uint32_t* strand, const int64_t* set_off,
+                    int64_t n_sets, int32_t k, const dnaln_chain_params* p, int32_t* out_score, uint32_t* out_strand,
+                    int32_t* out_n, int64_t* out_dmin, int64_t* out_dmax, uint32_t* out_rpos, int32_t* out_count) {
+  if (!c || !p || !set_off || n_sets < 0 || !out_count) return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
+  if (p->lookback < 0 || p->band < 0 || p->band > (1 << 20))
+    return fail(c, DNALN_ERR_INVALID_ARG, "chain lookback must be >= 0 and band in [0, 2^20]");
+  if (n_sets == 0) return DNALN_OK;
+  if (int e = set_device(c)) return e;
+  const int64_t total = set_off[n_sets] - set_off[0];
+  if (set_off[0] != 0 || total < 0) return fail(c, DNALN_ERR_INVALID_ARG, "set_off must start at 0 and increase");
+  std::vector<uint64_t> keys(static_cast<size_t>(total));
+  for (int64_t i = 0; i < total; ++i) {
+    if (strand[i] > 1 || rpos[i] >= (1u << 31) || qpos[i] < -(1 << 30) || qpos[i] >= (1 << 30))
+      return fail(c, DNALN_ERR_INVALID_ARG, "anchor %lld out of range (strand 0/1, rpos < 2^31, |qpos| < 2^30)",
+                  static_cast<long long>(i));
+    keys[static_cast<size_t>(i)] = anchor_key(strand[i], rpos[i], qpos[i]);
+  }
+  cudaStream_t st = c->st;
+  AnchorScratch as;
+  as.keys = dbuf<uint64_t>(c, "a_keys", total);
+  as.f = dbuf<int32_t>(c, "a_f", total);
+  as.prev = dbuf<int32_t>(c, "a_prev", total);
+  as.ord = dbuf<uint64_t>(c, "a_ord", total);
+  as.used = dbuf<uint8_t>(c, "a_used", total);
+  as.ch_score = dbuf<int32_t>(c, "c_score", total);
+  as.ch_sn = dbuf<uint32_t>(c, "c_sn", total);
+  as.ch_dmin = dbuf<int64_t>(c, "c_dmin", total);
+  as.ch_dmax = dbuf<int64_t>(c, "c_dmax", total);
+  as.ch_rpos = dbuf<uint32_t>(c, "c_rpos", total);
+  if (!as.keys || !as.f || !as.prev || !as.ord || !as.used || !as.ch_score || !as.ch_sn || !as.ch_dmin ||
+      !as.ch_dmax || !as.ch_rpos)
+    return DNALN_ERR_OOM;
+  DBUF(d_set, int64_t, "ch_set", n_sets + 1);
+  DBUF(d_cnt, int32_t, "ch_cnt", n_sets);
+  const std::vector<int32_t> lut = chain_cost_lut(k, p->band);
+  DBUF(d_lut, int32_t, "chain_lut", lut.size());
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
+  CK(cudaMemcpyAsync(as.keys, keys.data(), total * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_set, set_off, (n_sets + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_lut, lut.data(), lut.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  ChainParamsDev cp{p->max_gap, p->band, p->lookback, p->min_score, p->min_anchors, k, d_lut};
+  launch_chain_sets(st, d_set, n_sets, cp, as, d_cnt, c->d_err);
+  CK(cudaGetLastError());
+  std::vector<uint64_t> ord(static_cast<size_t>(total));
+  std::vector<int32_t> score(static_cast<size_t>(total));
+  std::vector<uint32_t> sn(static_cast<size_t>(total)), crp(static_cast<size_t>(total));
+  std::vector<int64_t> dmin(static_cast<size_t>(total)), dmax(static_cast<size_t>(total));
+  CK(cudaMemcpyAsync(keys.data(), as.keys, total * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(ord.data(), as.ord, total * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(score.data(), as.ch_score, total * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(sn.data(), as.ch_sn, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(crp.data(), as.ch_rpos, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(dmin.data(), as.ch_dmin, total * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(dmax.data(), as.ch_dmax, total * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out_count, d_cnt, n_sets * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  uint32_t bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->d_err, sizeof bits, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (int e = check_device_errors(c, bits)) return e;
+  for (int64_t i = 0; i < total; ++i) {
+    rpos[i] = key_rpos(keys[static_cast<size_t>(i)]);
+    qpos[i] = key_qpos(keys[static_cast<size_t>(i)]);
+    strand[i] = key_strand(keys[static_cast<size_t>(i)]);
+  }
+  for (int64_t s = 0; s < n_sets; ++s) {
+    const int64_t a0 = set_off[s];
+    for (int32_t j = 0; j < out_count[s]; ++j) {
+      const size_t src = static_cast<size_t>(a0 + static_cast<int64_t>(ord[static_cast<size_t>(a0 + j)] & 0xffffffffu));
+      const size_t dst = static_cast<size_t>(a0 + j);
+      out_score[dst] = score[src];
+      out_strand[dst] = sn[src] & 1u;
+      out_n[dst] = static_cast<int32_t>(sn[src] >> 1);
+      out_dmin[dst] = dmin[src];
+      out_dmax[dst] = dmax[src];
+      out_rpos[dst] = crp[src];
+    }
+  }
+  return DNALN_OK;
+}
+
+int dnaln_gpu_align(dnaln_ctx* c, const uint8_t* q, const int64_t* q_off, const int32_t* q_len, const uint8_t* t,
+                    const int64_t* t_off, const int32_t* t_len, int64_t n, int32_t traceback,
+                    const dnaln_score_params* sp, dnaln_align_result* out, uint32_t* cigar, int64_t cigar_cap,
+                    int64_t* cigar_used) {
+  if (!c || !sp || n < 0 || (n > 0 && (!q || !q_off || !q_len || !t || !t_off || !t_len || !out)))
+    return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
+  if (sp->bw < 0 || sp->bw > 1000 || sp->gap_ext < 0 || sp->gap_open < 0 || sp->mismatch < 0 || sp->ambig < 0)
+    return fail(c, DNALN_ERR_INVALID_ARG, "invalid score parameters");
+  if (cigar_used) *cigar_used = 0;
+  if (n == 0) return DNALN_OK;
+  if (n > (int64_t(1) << 31) - 64) return fail(c, DNALN_ERR_INVALID_ARG, "too many tasks in one call");
+  if (int e = set_device(c)) return e;
+  const int W = 2 * sp->bw + 1;
+  int64_t qext = 0, text = 0, cig_total = 0;
+  int rows_max = 0;
+  std::vector<SwTask> tasks(static_cast<size_t>(n));
+  std::vector<int64_t> slot_off(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    if (q_len[i] < 0 || t_len[i] < 0 || q_off[i] < 0 || t_off[i] < 0)
+      return fail(c, DNALN_ERR_INVALID_ARG, "negative offset or length in task %lld", static_cast<long long>(i));
+    qext = std::max<int64_t>(qext, q_off[i] + q_len[i]);
+    const int64_t tmax = static_cast<int64_t>(q_len[i]) + W - 1;
+    const int64_t tl = t_len[i] < tmax ? t_len[i] : tmax;
+    text = std::max<int64_t>(text, t_off[i] + tl);
+    SwTask& tk = tasks[static_cast<size_t>(i)];
+    tk.q_off = q_off[i];
+    tk.qlen = q_len[i];
+    tk.t_start = t_off[i];
+    tk.t_lo = t_off[i];
+    tk.t_hi = t_off[i] + tl;
+    tk.slot = static_cast<int32_t>(i);
+    slot_off[static_cast<size_t>(i)] = cig_total;
+    cig_total += 2 * static_cast<int64_t>(q_len[i]) + 1;
+    rows_max = std::max(rows_max, q_len[i]);
+  }
+  cudaStream_t st = c->st;
+  const bool tb = traceback != 0;
+  DBUF(d_q, uint8_t, "al_q", qext);
+  DBUF(d_t, uint8_t, "al_t", text);
+  DBUF(d_tasks, SwTask, "al_tasks", n);
+  DBUF(d_res, SwResult, "al_res", n);
+  CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
+  if (qext) CK(cudaMemcpyAsync(d_q, q, qext, cudaMemcpyHostToDevice, st));
+  if (text) CK(cudaMemcpyAsync(d_t, t, text, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_tasks, tasks.data(), n * sizeof(SwTask), cudaMemcpyHostToDevice, st));
+  const SwParams swp = make_sw_params(*sp);
+  uint32_t* d_cig = nullptr;
+  int64_t* d_slot = nullptr;
+  if (tb) {
+    d_cig = dbuf<uint32_t>(c, "al_cig", cig_total);
+    d_slot = dbuf<int64_t>(c, "al_slot", n);
+    if (!d_cig || !d_slot) return DNALN_ERR_OOM;
+    CK(cudaMemcpyAsync(d_slot, slot_off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  }
+  CK(cudaEventRecord(c->ev[tb ? kEvTb0 : kEvSc0], st));
+  if (int e = launch_sw_chunked(c, tb, sw_bytes_ok(*sp), d_tasks, static_cast<int>(n), nullptr, d_q, d_t, swp, d_res,
+                                rows_max, d_cig, d_slot))
+    return e;
+  CK(cudaEventRecord(c->ev[tb ? kEvTb1 : kEvSc1], st));
+  int64_t total = 0;
+  if (!tb) {
+    std::vector<SwResult> res(static_cast<size_t>(n));
+    CK(cudaMemcpyAsync(res.data(), d_res, n * sizeof(SwResult), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int64_t i = 0; i < n; ++i) {
+      dnaln_align_result& o = out[i];
+      std::memset(&o, 0, sizeof o);
+      o.score = res[static_cast<size_t>(i)].score;
+    }
+  } else {
+    DBUF(d_cnt, int64_t, "al_cnt", n + 1);
+    DBUF(d_doff, int64_t, "al_doff", n + 1);
+    DBUF(d_out, dnaln_align_result, "al_out", n);
+    launch_align_counts(st, n, d_res, d_cnt);
+    if (int e = exclusive_scan(c, d_cnt, d_doff, n + 1)) return e;
+    CK(cudaMemcpyAsync(c->h_info, d_doff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    total = c->h_info[0];
+    DBUF(d_final, uint32_t, "al_final", total);
+    launch_align_gather(st, n, d_res, d_cig, d_slot, d_doff, d_out, d_final);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, d_out, n * sizeof(dnaln_align_result), cudaMemcpyDeviceToHost, st));
+    if (cigar && total <= cigar_cap && total > 0)
+      CK(cudaMemcpyAsync(cigar, d_final, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  uint32_t bits = 0;
+  CK(cudaMemcpy(&bits, c->d_err, sizeof bits, cudaMemcpyDeviceToHost));
+  if (int e = check_device_errors(c, bits)) return e;
+  if (cigar_used) *cigar_used = total;
+  c->stats.cells += 0;
+  for (int64_t i = 0; i < n; ++i) c->stats.cells += static_cast<uint64_t>(q_len[i]) * W;
+  if (tb) {
+    c->stats.sw_tasks_tb += static_cast<uint64_t>(n);
+    c->stats.ms_sw_tb += ev_ms(c, kEvTb0, kEvTb1);
+  } else {
+    c->stats.sw_tasks_score += static_cast<uint64_t>(n);
+    c->stats.ms_sw_score += ev_ms(c, kEvSc0, kEvSc1);
+  }
+  if (tb && total > cigar_cap)
+    return fail(c, DNALN_ERR_CAPACITY, "CIGAR buffer holds %lld ops, tasks need %lld",
+                static_cast<long long>(cigar_cap), static_cast<long long>(total));
+  return DNALN_OK;
+}
+
+int dnaln_gpu_map_batch_device(dnaln_ctx* c, int32_t id, const char* d_seq, const int64_t* d_seq_off,
+                               const int32_t* d_seq_len, const uint32_t* d_name_hash, int64_t n,
+                               const dnaln_map_params* p, dnaln_map_record* d_out, uint32_t* d_cigar,
+                               int64_t cigar_cap, int64_t* cigar_used) {
+  if (!c || n < 0 || !cigar_used || (n > 0 && (!d_seq || !d_seq_off || !d_seq_len || !d_name_hash || !d_out)))
+    return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
+  if (int e = set_device(c)) return e;
+  IndexRes* r = find_index(c, id);
+  if (!r) return DNALN_ERR_NOT_FOUND;
+  if (int e = validate_map_params(c, p, *r)) return e;
+  if (!d_cigar) return fail(c, DNALN_ERR_INVALID_ARG, "null CIGAR buffer");
+  const int e = run_map(c, *r, d_seq, d_seq_off, d_seq_len, d_name_hash, n, *p, d_out, d_cigar, cigar_cap,
+                        cigar_used, nullptr);
+  if (e == DNALN_OK) c->stats.cells += 0;
+  return e;
+}
+
+int dnaln_gpu_map_batch(dnaln_ctx* c, int32_t id, const char* seq, const int64_t* seq_off, const int32_t* seq_len,
+                        const uint32_t* name_hash, int64_t n, const dnaln_map_params* p, dnaln_map_record* out,
+                        uint32_t* cigar, int64_t cigar_cap, int64_t* cigar_used) {
+  if (!c || n < 0 || !cigar_used || (n > 0 && (!seq || !seq_off || !seq_len || !name_hash || !out)))
+    return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
+  if (int e = set_device(c)) return e;
+  IndexRes* r = find_index(c, id);
+  if (!r) return DNALN_ERR_NOT_FOUND;
+  if (int e = validate_map_params(c, p, *r)) return e;
+  *cigar_used = 0;
+  if (n == 0) return DNALN_OK;
+  int64_t ext = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (seq_len[i] < 0 || seq_off[i] < 0) return fail(c, DNALN_ERR_INVALID_ARG, "negative offset or length");
+    ext = std::max<int64_t>(ext, seq_off[i] + seq_len[i]);
+  }
+  cudaStream_t st = c->st;
+  DBUF(d_seq, char, "in_seq", ext);
+  DBUF(d_off, int64_t, "in_off", n);
+  DBUF(d_len, int32_t, "in_len", n);
+  DBUF(d_hash, uint32_t, "in_hash", n);
+  DBUF(d_out, dnaln_map_record, "out_rec", n);
+  CK(cudaEventRecord(c->ev[kEvH2d0], st));
+  CK(cudaMemcpyAsync(d_seq, seq, ext, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_off, seq_off, n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_len, seq_len, n * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_hash, name_hash, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  CK(cudaEventRecord(c->ev[kEvH2d1], st));
+  uint32_t* d_cig = nullptr;
+  int e = run_map(c, *r, d_seq, d_off, d_len, d_hash, n, *p, d_out, nullptr, 0, cigar_used, &d_cig);
+  if (e != DNALN_OK) return e;
+  if (*cigar_used > cigar_cap || (*cigar_used > 0 && !cigar))
+    return fail(c, DNALN_ERR_CAPACITY, "CIGAR buffer holds %lld ops, batch needs %lld",
+                static_cast<long long>(cigar_cap), static_cast<long long>(*cigar_used));
+  CK(cudaEventRecord(c->ev[kEvD2h0], st));
+  CK(cudaMemcpyAsync(out, d_out, n * sizeof(dnaln_map_record), cudaMemcpyDeviceToHost, st));
+  if (*cigar_used > 0)
+    CK(cudaMemcpyAsync(cigar, d_cig, *cigar_used * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(c->ev[kEvD2h1], st));
+  CK(cudaStreamSynchronize(st));
+  c->stats.ms_h2d += ev_ms(c, kEvH2d0, kEvH2d1);
+  c->stats.ms_d2h += ev_ms(c, kEvD2h0, kEvD2h1);
+  return DNALN_OK;
+}
+
+}  // extern "C"

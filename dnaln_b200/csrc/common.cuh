@@ -1,0 +1,100 @@
+// common.cuh — shared device-side definitions of the B200 mapping path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dnaln_b200.h"
+
+namespace dnb {
+
+constexpr uint64_t kInvalidHash = ~0ULL;  // palindromic k-mer / empty bucket (src/minimizer.cpp:7, src/index.hpp:53)
+constexpr int kWarp = 32;
+
+// Device error flags (bitwise OR into ErrorFlags::bits); any set bit fails the call with
+// DNALN_ERR_DEVICE. None of them can occur for well-formed input: they guard index
+// arithmetic so that a broken invariant is reported instead of reading out of bounds.
+enum : uint32_t {
+  kErrTracebackBounds = 1u << 0,
+  kErrCigarOverflow = 1u << 1,
+  kErrChainScratch = 1u << 2,
+  kErrProbeLoop = 1u << 3,
+};
+
+// Thomas Wang's 64-bit mix restricted to `mask` bits, step for step as the index keys are
+// defined (src/minimizer.hpp:21-31).
+__host__ __device__ __forceinline__ uint64_t hash64(uint64_t key, uint64_t mask) {
+  key = (~key + (key << 21)) & mask;
+  key = key ^ key >> 24;
+  key = ((key + (key << 3)) + (key << 8)) & mask;
+  key = key ^ key >> 14;
+  key = ((key + (key << 2)) + (key << 4)) & mask;
+  key = key ^ key >> 28;
+  key = (key + (key << 31)) & mask;
+  return key;
+}
+
+// ASCII -> base code, A/a 0, C/c 1, G/g 2, T/t/U/u 3, else 4 (src/common.hpp:23-31).
+__host__ __device__ __forceinline__ uint8_t nt4(uint8_t c) {
+  const uint8_t u = c & 0xDF;  // fold case
+  return u == 'A' ? 0 : u == 'C' ? 1 : u == 'G' ? 2 : (u == 'T' || u == 'U') ? 3 : 4;
+}
+
+// One band-SW task, in either addressing mode:
+//   query  = qbase[q_off .. q_off + qlen)
+//   target column j = tbase[t_start + j] when t_lo <= t_start + j < t_hi, else N.
+// GpuAligner tasks use a flat target buffer (t_lo = t_start, t_hi = t_start + tlen);
+// mapping tasks index the resident genome with the candidate contig's bounds, which
+// is the N-padded window of src/mapper.cpp:100-121 without a copy.
+struct SwTask {
+  int64_t q_off;
+  int64_t t_start, t_lo, t_hi;
+  int32_t qlen;
+  int32_t slot;  // result / CIGAR slot
+};
+
+struct SwResult {
+  int32_t score, qb, qe, tb, te, nm;
+  int32_t n_ops;  // CIGAR ops written (traceback order, i.e. reversed)
+  int32_t pad_;
+};
+
+struct SwParams {
+  int32_t match, mismatch, oe, ge, ambig, bw, W;
+  uint32_t prof_n;  // 4 bytes of -ambig (table entries 4..7 of the byte-permute profile)
+};
+
+__host__ __device__ __forceinline__ int sub_score(const SwParams& p, int a, int b) {
+  return (a > 3 || b > 3) ? -p.ambig : (a == b ? p.match : -p.mismatch);  // src/align.hpp:39
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ long long warp_max_ll(long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const long long x = __shfl_xor_sync(0xffffffffu, v, o);
+    v = x > v ? x : v;
+  }
+  return v;
+}
+
+// Exclusive prefix sum across the warp; *total receives the warp-wide sum.
+__device__ __forceinline__ int warp_exclusive_scan(int v, int* total) {
+  const int lane = threadIdx.x & 31;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  *total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+}  // namespace dnb

@@ -1,0 +1,502 @@
+// seed.cu — minimizer sketching, index probing, anchor generation, colinear chaining and
+// candidate selection, one warp per read (sm_100a).
+//
+// Sketch (src/minimizer.cpp:5-68). The reference streams a van Herk/Gil-Werman window
+// minimum; here the 32 lanes of a warp take 32 consecutive k-mer starts at a time. Each
+// lane builds its k-mer's forward and reverse-complement 2-bit words, its canonical hash
+// (palindromes get the never-selected hash ~0) and parks it in a per-warp ring in shared
+// memory; a ballot gives every lane the last k-mer start hit by an N, so "the window of w
+// k-mers ending here lies in one N-free run" is a compare. A full window's minimum is its
+// leftmost smallest hash (strict '<' scan over the ring). The reference emits the window
+// minimum unless its position equals the last emitted one; because window minima move
+// monotonically, that is the local rule "emit unless the previous window is full, has a
+// valid minimum and picked the same position", evaluated with one shuffle. Emitted
+// minimizers are compacted in order with a ballot.
+//
+// Probe (src/index.hpp:24-38, src/mapper.cpp:24-30): one lane per minimizer walks the
+// open-addressing table with 16-byte vector loads; hits with count 0 or above max_occ
+// are dropped.
+//
+// Chaining (src/chain.cpp:12-69). Anchors (src/mapper.cpp:32-40) are packed into one
+// 64-bit key (strand, rpos, qpos) so the reference's sort is a warp bitonic sort of
+// integers. The DP scans predecessors nearest-first with a `break` on strand change or
+// dr > max_gap; because anchors are sorted by (strand, rpos), the scanned predecessors
+// form one contiguous range, so the lanes test up to 32 predecessors each round
+// independently and a warp max over (score << 32 | j) picks the best with ties to the
+// nearest j, as the reference's strict '>' does. The FP64 gap cost comes from a
+// host-computed table (exactly the reference's expression). Chains are extracted from end
+// points in (f desc, index asc) order — another bitonic sort of packed keys — walked by
+// one lane, and ordered by score with ties in extraction order (the reference's
+// stable_sort). Candidate loci follow src/mapper.cpp:40-62.
+#include "common.cuh"
+#include "seed.cuh"
+
+namespace dnb {
+
+namespace {
+
+constexpr int kSeedWarps = 8;
+constexpr int kRing = 512;  // >= 32 + max w (255)
+constexpr int kChainWarps = 4;
+constexpr int kSmCap = 128;  // anchors per read held in shared memory
+
+struct SketchSmem {
+  uint64_t hash[kRing];
+  uint8_t strand[kRing];
+};
+
+// Sketches one sequence with the whole warp. code_at(i) returns the base code (0..4) at
+// i; emit(rank, hash, pos, strand) is called by the emitting lanes, ranks in order.
+// Returns the number of minimizers (same in all lanes).
+template <class CodeAt, class Emit>
+__device__ int warp_sketch(CodeAt code_at, int len, int k, int w, SketchSmem& sm, Emit emit) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t mask = (1ULL << (2 * k)) - 1;
+  const int nk = len - k + 1;  // k-mer starts
+  int count = 0, carry_bad = -1, p_arg = -1;
+  for (int base = 0; base < nk; base += 32) {
+    const int s = base + lane;
+    bool kv = false;
+    uint64_t h = kInvalidHash;
+    uint32_t st = 0;
+    if (s < nk) {
+      uint64_t fwd = 0, rev = 0;
+      bool hasn = false;
+      for (int m = 0; m < k; ++m) {
+        const uint32_t c = code_at(s + m);
+        hasn |= c > 3;
+        fwd = (fwd << 2) | (c & 3u);
+        rev |= static_cast<uint64_t>(3u - (c & 3u)) << (2 * m);
+      }
+      kv = !hasn;
+      if (kv) {
+        st = rev < fwd;
+        h = fwd != rev ? hash64(st ? rev : fwd, mask) : kInvalidHash;
+      }
+    }
+    __syncwarp();
+    sm.hash[s & (kRing - 1)] = h;
+    sm.strand[s & (kRing - 1)] = static_cast<uint8_t>(st);
+    const unsigned bad = __ballot_sync(0xffffffffu, s < nk && !kv);
+    const unsigned upto = bad & (0xffffffffu >> (31 - lane));
+    const int lastbad = upto ? base + 31 - __clz(upto) : carry_bad;
+    carry_bad = bad ? base + 31 - __clz(bad) : carry_bad;
+    __syncwarp();
+    int arg = -1;
+    uint64_t mh = kInvalidHash;
+    if (s < nk && s >= w - 1 && lastbad < s - w + 1) {  // full window of w k-mers
+      int b = s - w + 1;
+      uint64_t bh = sm.hash[b & (kRing - 1)];
+      for (int j = b + 1; j <= s; ++j) {
+        const uint64_t x = sm.hash[j & (kRing - 1)];
+        if (x < bh) {
+          bh = x;
+          b = j;
+        }
+      }
+      mh = bh;
+      arg = bh != kInvalidHash ? b : -1;
+    }
+    const int up = __shfl_up_sync(0xffffffffu, arg, 1);
+    const int prev_arg = lane == 0 ? p_arg : up;
+    const bool em = arg >= 0 && arg != prev_arg;
+    const unsigned ball = __ballot_sync(0xffffffffu, em);
+    if (em) emit(count + __popc(ball & ((1u << lane) - 1u)), mh, arg, sm.strand[arg & (kRing - 1)]);
+    count += __popc(ball);
+    p_arg = __shfl_sync(0xffffffffu, arg, 31);
+  }
+  return count;
+}
+
+__device__ __forceinline__ void probe(const DevIndex& ix, uint64_t h, uint32_t& off, uint32_t& cnt,
+                                      uint32_t* err) {
+  uint64_t i = h & ix.mask;
+  off = 0;
+  cnt = 0;
+  for (uint64_t it = 0; it <= ix.mask; ++it) {  // load <= 0.5: an empty bucket always ends the walk
+    const ulonglong2 b = __ldg(ix.table + i);
+    if (b.x == h) {
+      off = static_cast<uint32_t>(b.y);
+      cnt = static_cast<uint32_t>(b.y >> 32);
+      return;
+    }
+    if (b.x == kInvalidHash) return;
+    i = (i + 1) & ix.mask;
+  }
+  atomicOr(err, kErrProbeLoop);
+}
+
+__device__ __forceinline__ int contig_of(const DevIndex& ix, uint64_t gpos) {  // src/reference.cpp:25-32
+  int64_t lo = 0, hi = ix.n_contigs;
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) / 2;
+    if (ix.contig_off[mid] <= gpos) lo = mid;
+    else hi = mid;
+  }
+  return static_cast<int>(lo);
+}
+
+// Ascending sort of a[0, n) by the warp: bitonic network in its all-ascending form (the
+// first comparator of each merge pairs mirrored indices), so indices >= n act as +inf
+// padding and their comparators are skipped.
+__device__ void warp_sort_u64(uint64_t* a, int n) {
+  if (n <= 1) return;
+  const int lane = threadIdx.x & 31;
+  int lgN = 0;
+  while ((1 << lgN) < n) ++lgN;
+  const int halfN = 1 << (lgN - 1);
+  for (int lgs = 1; lgs <= lgN; ++lgs) {
+    const int lgh = lgs - 1, size = 1 << lgs;
+    for (int idx = lane; idx < halfN; idx += 32) {
+      const int blk = idx >> lgh, off = idx & ((1 << lgh) - 1);
+      const int i = blk * size + off, j = blk * size + size - 1 - off;
+      if (j < n) {
+        const uint64_t x = a[i], y = a[j];
+        if (y < x) {
+          a[i] = y;
+          a[j] = x;
+        }
+      }
+    }
+    __syncwarp();
+    for (int lgt = lgh - 1; lgt >= 0; --lgt) {
+      const int stride = 1 << lgt;
+      for (int idx = lane; idx < halfN; idx += 32) {
+        const int blk = idx >> lgt, off = idx & (stride - 1);
+        const int i = blk * 2 * stride + off, j = i + stride;
+        if (j < n) {
+          const uint64_t x = a[i], y = a[j];
+          if (y < x) {
+            a[i] = y;
+            a[j] = x;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t desc32(int32_t x) { return 0x7FFFFFFFu - static_cast<uint32_t>(x); }
+
+struct ChainArrays {
+  uint64_t* keys;
+  int32_t* f;
+  int32_t* prev;
+  uint64_t* ord;
+  uint8_t* used;
+};
+
+// Sorts the n anchor keys, runs the DP, extracts chains into as.ch_*[c0 + j] and leaves
+// their final order in ord[0, m) (low 32 bits = j). Returns m in every lane.
+__device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const AnchorScratch& as, int64_t c0) {
+  const int lane = threadIdx.x & 31;
+  warp_sort_u64(a.keys, n);
+  // DP (src/chain.cpp:22-45)
+  for (int i = 0; i < n; ++i) {
+    const uint64_t ki = a.keys[i];
+    const uint32_t si = key_strand(ki);
+    const int64_t ri = key_rpos(ki), qi = key_qpos(ki);
+    long long best = LLONG_MIN;
+    for (int r0 = 0; r0 < cp.lookback; r0 += 32) {
+      const int t = r0 + lane, j = i - 1 - t;
+      bool stop = true;
+      if (t < cp.lookback && j >= 0) {
+        const uint64_t kj = a.keys[j];
+        const int64_t dr = ri - key_rpos(kj);
+        if (key_strand(kj) == si && dr <= cp.max_gap) {
+          stop = false;
+          const int64_t dq = qi - key_qpos(kj);
+          if (dr > 0 && dq > 0) {
+            const int64_t dd = dr > dq ? dr - dq : dq - dr;
+            if (dd <= cp.band) {
+              int64_t g = dq < dr ? dq : dr;
+              if (g > cp.k) g = cp.k;
+              const int sc = a.f[j] + static_cast<int>(g) - cp.cost[dd];
+              const long long key = static_cast<long long>(sc) * 4294967296LL + j;
+              best = key > best ? key : best;
+            }
+          }
+        }
+      }
+      if (__all_sync(0xffffffffu, stop)) break;  // every later predecessor is out of range too
+    }
+    best = warp_max_ll(best);
+    if (lane == 0) {
+      const int sc = best == LLONG_MIN ? 0 : static_cast<int>(best >> 32);
+      if (best != LLONG_MIN && sc > cp.k) {
+        a.f[i] = sc;
+        a.prev[i] = static_cast<int>(best & 0xffffffffLL);
+      } else {
+        a.f[i] = cp.k;
+        a.prev[i] = -1;
+      }
+    }
+    __syncwarp();
+  }
+  // extraction order: f descending, index ascending (src/chain.cpp:49-50)
+  for (int i = lane; i < n; i += 32) {
+    a.ord[i] = static_cast<uint64_t>(desc32(a.f[i])) << 32 | static_cast<uint32_t>(i);
+    a.used[i] = 0;
+  }
+  __syncwarp();
+  warp_sort_u64(a.ord, n);
+  int m = 0;
+  if (lane == 0) {  // walk (src/chain.cpp:52-67)
+    for (int e = 0; e < n; ++e) {
+      const int end = static_cast<int>(a.ord[e] & 0xffffffffu);
+      if (a.used[end]) continue;
+      int i = end, cnt = 0;
+      int64_t dmin = LLONG_MAX, dmax = LLONG_MIN;
+      while (i >= 0 && !a.used[i]) {
+        a.used[i] = 1;
+        ++cnt;
+        const uint64_t ki = a.keys[i];
+        const int64_t d = static_cast<int64_t>(key_rpos(ki)) - key_qpos(ki);
+        dmin = d < dmin ? d : dmin;
+        dmax = d > dmax ? d : dmax;
+        i = a.prev[i];
+      }
+      const int score = a.f[end] - (i >= 0 ? a.f[i] : 0);
+      if (score < cp.min_score || cnt < cp.min_anchors) continue;
+      const uint64_t ke = a.keys[end];
+      as.ch_score[c0 + m] = score;
+      as.ch_sn[c0 + m] = key_strand(ke) | static_cast<uint32_t>(cnt) << 1;
+      as.ch_dmin[c0 + m] = dmin;
+      as.ch_dmax[c0 + m] = dmax;
+      as.ch_rpos[c0 + m] = key_rpos(ke);
+      ++m;
+    }
+  }
+  m = __shfl_sync(0xffffffffu, m, 0);
+  __syncwarp();
+  // final order: score descending, extraction order ascending (stable_sort, src/chain.cpp:68)
+  for (int j = lane; j < m; j += 32)
+    a.ord[j] = static_cast<uint64_t>(desc32(as.ch_score[c0 + j])) << 32 | static_cast<uint32_t>(j);
+  __syncwarp();
+  warp_sort_u64(a.ord, m);
+  return m;
+}
+
+struct ChainSmem {
+  uint64_t keys[kSmCap];
+  uint64_t ord[kSmCap];
+  int32_t f[kSmCap];
+  int32_t prev[kSmCap];
+  uint8_t used[kSmCap];
+};
+
+__global__ void __launch_bounds__(kSeedWarps * 32)
+    k_seed(const char* __restrict__ seq, const int64_t* __restrict__ seq_off, const int32_t* __restrict__ seq_len,
+           const int64_t* __restrict__ pofs, int64_t n, uint8_t* __restrict__ codes, DevIndex ix, SeedParams sp,
+           MinBuf mb, int32_t* __restrict__ n_min, int64_t* __restrict__ n_anchor, uint32_t* __restrict__ err) {
+  __shared__ SketchSmem sm[kSeedWarps];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * kSeedWarps + wib;
+  if (r >= n) return;
+  const int64_t so = pofs[r];  // packed offset of this read's codes and minimizer slots
+  const int len = seq_len[r];
+  const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + seq_off[r];
+  uint8_t* fw = codes + 2 * so;
+  uint8_t* rc = fw + len;
+  for (int i = lane; i < len; i += 32) {  // src/mapper.cpp:88-99
+    const uint8_t c = nt4(s[i]);
+    fw[i] = c;
+    rc[len - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
+  }
+  const int cnt = warp_sketch([&](int i) { return static_cast<uint32_t>(nt4(s[i])); }, len, sp.k, sp.w, sm[wib],
+                              [&](int rank, uint64_t h, int pos, uint32_t st) {
+                                mb.hash[so + rank] = h;
+                                mb.pos[so + rank] = static_cast<uint32_t>(pos) | st << 31;
+                              });
+  __syncwarp();
+  long long anchors = 0;
+  for (int j = lane; j < cnt; j += 32) {
+    uint32_t off, c;
+    probe(ix, mb.hash[so + j], off, c, err);
+    if (c > sp.max_occ) c = 0;
+    mb.hit_off[so + j] = off;
+    mb.hit_cnt[so + j] = c;
+    anchors += c;
+  }
+  anchors = warp_sum(anchors);
+  if (lane == 0) {
+    n_min[r] = cnt;
+    n_anchor[r] = anchors;
+  }
+}
+
+__global__ void __launch_bounds__(kChainWarps * 32)
+    k_chain_map(const int64_t* __restrict__ pofs, const int32_t* __restrict__ seq_len, int64_t n,
+                const int32_t* __restrict__ n_min, const int64_t* __restrict__ anchor_off, MinBuf mb, DevIndex ix,
+                ChainParamsDev cp, CandParams cand, AnchorScratch as, CandBuf cb, uint32_t* __restrict__ err) {
+  __shared__ ChainSmem sm[kChainWarps];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * kChainWarps + wib;
+  if (r >= n) return;
+  const int64_t a0 = anchor_off[r];
+  const int64_t na64 = anchor_off[r + 1] - a0;
+  if (na64 > 0x3FFFFFFF) {
+    if (lane == 0) {
+      atomicOr(err, kErrChainScratch);
+      cb.n_cand[r] = 0;
+    }
+    return;
+  }
+  const int na = static_cast<int>(na64);
+  const bool small = na <= kSmCap;
+  ChainArrays a;
+  a.keys = small ? sm[wib].keys : as.keys + a0;
+  a.ord = small ? sm[wib].ord : as.ord + a0;
+  a.f = small ? sm[wib].f : as.f + a0;
+  a.prev = small ? sm[wib].prev : as.prev + a0;
+  a.used = small ? sm[wib].used : as.used + a0;
+  const int64_t so = pofs[r];
+  const int len = seq_len[r], nm = n_min[r], k = cp.k;
+  // anchors in minimizer order x occurrence order (src/mapper.cpp:32-40)
+  int w_off = 0;
+  for (int base = 0; base < nm; base += 32) {
+    const int j = base + lane;
+    const int c = j < nm ? static_cast<int>(mb.hit_cnt[so + j]) : 0;
+    int total;
+    const int ex = warp_exclusive_scan(c, &total);
+    if (c) {
+      const uint32_t off = mb.hit_off[so + j], mp = mb.pos[so + j];
+      const int32_t pos = static_cast<int32_t>(mp & 0x7FFFFFFFu);
+      const uint32_t mst = mp >> 31;
+      for (int t = 0; t < c; ++t) {
+        const uint32_t v = __ldg(ix.positions + off + t);
+        const uint32_t rev = (v & 1u) ^ mst;
+        const int32_t qpos = rev ? len - pos - k : pos;
+        a.keys[w_off + ex + t] = anchor_key(rev, v >> 1, qpos);
+      }
+    }
+    w_off += total;
+  }
+  __syncwarp();
+  const int m = chain_core(a, na, cp, as, a0);
+  // candidate loci (src/mapper.cpp:40-62)
+  if (lane == 0) {
+    int nd = 0;
+    const int64_t cbase = r * cand.max_cand;
+    if (m > 0) {
+      const double min_score = static_cast<double>(as.ch_score[a0 + (a.ord[0] & 0xffffffffu)]) * cand.pri_ratio;
+      for (int c = 0; c < m; ++c) {
+        const int64_t ci = a0 + (a.ord[c] & 0xffffffffu);
+        if (static_cast<double>(as.ch_score[ci]) < min_score || nd >= cand.max_cand) break;
+        const int64_t dmin = as.ch_dmin[ci], dmax = as.ch_dmax[ci];
+        const int64_t diag = dmin + (dmax - dmin) / 2;
+        const uint8_t strand = static_cast<uint8_t>(as.ch_sn[ci] & 1u);
+        bool dup = false;
+        for (int x = 0; x < nd && !dup; ++x) {
+          const int64_t dd = cb.diag[cbase + x] - diag;
+          dup = cb.rev[cbase + x] == strand && (dd < 0 ? -dd : dd) <= cand.bw;
+        }
+        if (dup) continue;
+        cb.rev[cbase + nd] = strand;
+        cb.contig[cbase + nd] = contig_of(ix, as.ch_rpos[ci]);
+        cb.diag[cbase + nd] = diag;
+        cb.wstart[cbase + nd] = diag - cand.bw;
+        ++nd;
+      }
+    }
+    cb.n_cand[r] = nd;
+  }
+}
+
+__global__ void __launch_bounds__(kSeedWarps * 32)
+    k_sketch_codes(const uint8_t* __restrict__ codes, const int64_t* __restrict__ seq_off,
+                   const int32_t* __restrict__ seq_len, const uint32_t* __restrict__ pos_offset, int64_t n, int k,
+                   int w, uint64_t* __restrict__ out_hash, uint32_t* __restrict__ out_pos,
+                   uint32_t* __restrict__ out_strand, int32_t* __restrict__ out_count) {
+  __shared__ SketchSmem sm[kSeedWarps];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * kSeedWarps + wib;
+  if (r >= n) return;
+  const int64_t so = seq_off[r];
+  const uint8_t* s = codes + so;
+  const uint32_t po = pos_offset ? pos_offset[r] : 0u;
+  const int cnt = warp_sketch([&](int i) { return static_cast<uint32_t>(s[i]); }, seq_len[r], k, w, sm[wib],
+                              [&](int rank, uint64_t h, int pos, uint32_t st) {
+                                out_hash[so + rank] = h;
+                                out_pos[so + rank] = static_cast<uint32_t>(pos) + po;
+                                out_strand[so + rank] = st;
+                              });
+  if (lane == 0) out_count[r] = cnt;
+}
+
+__global__ void k_lookup(DevIndex ix, const uint64_t* __restrict__ hashes, int64_t n, uint32_t* __restrict__ out_off,
+                         uint32_t* __restrict__ out_cnt, uint32_t* __restrict__ err) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t off, c;
+  probe(ix, hashes[i], off, c, err);
+  out_off[i] = off;
+  out_cnt[i] = c;
+}
+
+__global__ void __launch_bounds__(kChainWarps * 32)
+    k_chain_sets(const int64_t* __restrict__ set_off, int64_t n_sets, ChainParamsDev cp, AnchorScratch as,
+                 int32_t* __restrict__ out_count, uint32_t* __restrict__ err) {
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * kChainWarps + wib;
+  if (s >= n_sets) return;
+  const int64_t a0 = set_off[s];
+  const int64_t na64 = set_off[s + 1] - a0;
+  if (na64 > 0x3FFFFFFF) {
+    if (lane == 0) {
+      atomicOr(err, kErrChainScratch);
+      out_count[s] = 0;
+    }
+    return;
+  }
+  ChainArrays a{as.keys + a0, as.f + a0, as.prev + a0, as.ord + a0, as.used + a0};
+  const int m = chain_core(a, static_cast<int>(na64), cp, as, a0);
+  if (lane == 0) out_count[s] = m;
+}
+
+}  // namespace
+
+void launch_seed(cudaStream_t st, const char* seq, const int64_t* seq_off, const int32_t* seq_len,
+                 const int64_t* pofs, int64_t n, uint8_t* codes, const DevIndex& ix, const SeedParams& sp, MinBuf mb,
+                 int32_t* n_min, int64_t* n_anchor, uint32_t* err) {
+  if (n <= 0) return;
+  const int64_t blocks = (n + kSeedWarps - 1) / kSeedWarps;
+  k_seed<<<static_cast<unsigned>(blocks), kSeedWarps * 32, 0, st>>>(seq, seq_off, seq_len, pofs, n, codes, ix, sp, mb,
+                                                                   n_min, n_anchor, err);
+}
+
+void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* n_min,
+                      const int64_t* anchor_off, MinBuf mb, const DevIndex& ix, const ChainParamsDev& cp,
+                      const CandParams& cand, AnchorScratch as, CandBuf cb, uint32_t* err) {
+  if (n <= 0) return;
+  const int64_t blocks = (n + kChainWarps - 1) / kChainWarps;
+  k_chain_map<<<static_cast<unsigned>(blocks), kChainWarps * 32, 0, st>>>(pofs, seq_len, n, n_min, anchor_off, mb, ix,
+                                                                         cp, cand, as, cb, err);
+}
+
+void launch_sketch_codes(cudaStream_t st, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,
+                         const uint32_t* pos_offset, int64_t n, int32_t k, int32_t w, uint64_t* out_hash,
+                         uint32_t* out_pos, uint32_t* out_strand, int32_t* out_count) {
+  if (n <= 0) return;
+  const int64_t blocks = (n + kSeedWarps - 1) / kSeedWarps;
+  k_sketch_codes<<<static_cast<unsigned>(blocks), kSeedWarps * 32, 0, st>>>(codes, seq_off, seq_len, pos_offset, n, k,
+                                                                           w, out_hash, out_pos, out_strand,
+                                                                           out_count);
+}
+
+void launch_lookup(cudaStream_t st, const DevIndex& ix, const uint64_t* hashes, int64_t n, uint32_t* out_off,
+                   uint32_t* out_cnt, uint32_t* err) {
+  if (n <= 0) return;
+  const int64_t blocks = (n + 255) / 256;
+  k_lookup<<<static_cast<unsigned>(blocks), 256, 0, st>>>(ix, hashes, n, out_off, out_cnt, err);
+}
+
+void launch_chain_sets(cudaStream_t st, const int64_t* set_off, int64_t n_sets, const ChainParamsDev& cp,
+                       AnchorScratch as, int32_t* out_count, uint32_t* err) {
+  if (n_sets <= 0) return;
+  const int64_t blocks = (n_sets + kChainWarps - 1) / kChainWarps;
+  k_chain_sets<<<static_cast<unsigned>(blocks), kChainWarps * 32, 0, st>>>(set_off, n_sets, cp, as, out_count, err);
+}
+
+}  // namespace dnb

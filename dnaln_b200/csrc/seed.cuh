@@ -1,0 +1,103 @@
+// seed.cuh — launch interface of the seeding and chaining kernels (seed.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace dnb {
+
+// Resident minimizer index: the reference's table of 16-byte buckets {key, offset,
+// count} with linear probing from key & mask (src/index.hpp:3-9,49-56), the position
+// array (pos << 1 | strand), the genome (1 code per byte) and its contig table.
+struct DevIndex {
+  const ulonglong2* table;  // .x = key, .y = offset | (uint64)count << 32
+  const uint32_t* positions;
+  const uint8_t* genome;
+  const uint64_t* contig_off;
+  const uint32_t* contig_len;
+  uint64_t mask;
+  int32_t n_contigs, k, w;
+};
+
+struct SeedParams {
+  int32_t k, w;
+  uint32_t max_occ;
+};
+
+struct ChainParamsDev {
+  int32_t max_gap, band, lookback, min_score, min_anchors, k;
+  const int32_t* cost;  // cost[dd] for dd in [0, band]: int(0.01*k*dd + 0.5*ilog2(dd)), host-computed
+};
+
+struct CandParams {
+  int32_t max_cand, bw;
+  double pri_ratio;
+};
+
+// Minimizers of one read: slot j of read r is at index seq_off[r] + j.
+struct MinBuf {
+  uint64_t* hash;
+  uint32_t* pos;     // position | strand << 31
+  uint32_t* hit_off; // offset into the position array (valid when hit_cnt > 0)
+  uint32_t* hit_cnt; // occurrences kept (0 when absent or above max_occ)
+};
+
+struct AnchorScratch {  // per anchor of reads too large for the shared-memory path
+  uint64_t* keys;
+  int32_t* f;
+  int32_t* prev;
+  uint64_t* ord;
+  uint8_t* used;
+  int32_t* ch_score;
+  uint32_t* ch_sn;   // strand | n_anchors << 1
+  int64_t* ch_dmin;
+  int64_t* ch_dmax;
+  uint32_t* ch_rpos;
+};
+
+struct CandBuf {
+  int32_t* n_cand;
+  uint8_t* rev;
+  int32_t* contig;
+  int64_t* diag;
+  int64_t* wstart;
+};
+
+// Pass 1 of a read batch: encode the ASCII read seq[seq_off[r], + seq_len[r]) to codes
+// (forward at 2*pofs[r], reverse complement right after it; pofs = exclusive prefix of
+// the lengths), sketch, probe (minimizer slots at pofs[r]); writes n_min[r] and
+// n_anchor[r].
+void launch_seed(cudaStream_t st, const char* seq, const int64_t* seq_off, const int32_t* seq_len,
+                 const int64_t* pofs, int64_t n, uint8_t* codes, const DevIndex& ix, const SeedParams& sp, MinBuf mb,
+                 int32_t* n_min, int64_t* n_anchor, uint32_t* err);
+
+// Pass 2: anchors, chaining, candidates. anchor_off = exclusive prefix of n_anchor (n+1).
+void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* n_min,
+                      const int64_t* anchor_off, MinBuf mb, const DevIndex& ix, const ChainParamsDev& cp,
+                      const CandParams& cand, AnchorScratch as, CandBuf cb, uint32_t* err);
+
+// Stage entry points: sketch of code sequences, lookups, chaining of given anchor sets.
+void launch_sketch_codes(cudaStream_t st, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,
+                         const uint32_t* pos_offset, int64_t n, int32_t k, int32_t w, uint64_t* out_hash,
+                         uint32_t* out_pos, uint32_t* out_strand, int32_t* out_count);
+void launch_lookup(cudaStream_t st, const DevIndex& ix, const uint64_t* hashes, int64_t n, uint32_t* out_off,
+                   uint32_t* out_cnt, uint32_t* err);
+// Anchors of set s are [set_off[s], set_off[s+1]) of keys (see anchor_key); sorted in
+// place. Chains of set s go to the ch_* arrays of `as` at set_off[s] + j, count to out_count.
+void launch_chain_sets(cudaStream_t st, const int64_t* set_off, int64_t n_sets, const ChainParamsDev& cp,
+                       AnchorScratch as, int32_t* out_count, uint32_t* err);
+
+// Sort key of an anchor: strand, then rpos, then qpos (src/chain.cpp:16-20); qpos is
+// biased by 2^30 so that it sorts as a signed value.
+__host__ __device__ __forceinline__ uint64_t anchor_key(uint32_t strand, uint32_t rpos, int32_t qpos) {
+  return (static_cast<uint64_t>(strand & 1u) << 62) | (static_cast<uint64_t>(rpos & 0x7FFFFFFFu) << 31) |
+         static_cast<uint64_t>(static_cast<uint32_t>(qpos + (1 << 30)) & 0x7FFFFFFFu);
+}
+__host__ __device__ __forceinline__ uint32_t key_strand(uint64_t k) { return static_cast<uint32_t>(k >> 62); }
+__host__ __device__ __forceinline__ uint32_t key_rpos(uint64_t k) {
+  return static_cast<uint32_t>((k >> 31) & 0x7FFFFFFFu);
+}
+__host__ __device__ __forceinline__ int32_t key_qpos(uint64_t k) {
+  return static_cast<int32_t>(k & 0x7FFFFFFFu) - (1 << 30);
+}
+
+}  // namespace dnb

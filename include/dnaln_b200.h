@@ -1,0 +1,192 @@
+/* dnaln_b200.h — C ABI of the B200 (sm_100a) read-mapping path.
+ *
+ * Drop-in boundary for dnaln's hot path: minimizer sketching -> minimizer-index probe ->
+ * colinear chaining -> banded Smith-Waterman with traceback. Host code (dnaln's C++
+ * mapper, or the C++ mirror in dnaln_b200/host/dnaln_gpu.hpp) calls these functions; all
+ * arguments are plain pointers and sizes, host memory unless a name says `device`.
+ *
+ * Every function returns DNALN_OK (0) or a DNALN_ERR_* code; dnaln_gpu_last_error()
+ * gives the message of the last failure on a context. The reference reports errors by
+ * die() -> exit(1) (src/common.cpp:55-64); the C++ mirror turns a non-zero status into
+ * the same message and exit code.
+ *
+ * Threading: a context serves one host thread at a time (the reference's Mapper and
+ * Aligner are not thread-safe either, src/mapper.hpp:78-93). Use one context per thread.
+ *
+ * Citations (file:line) are to the dnaln sources each entry point replaces. */
+#ifndef DNALN_B200_H
+#define DNALN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DNALN_OK 0
+#define DNALN_ERR_INVALID_ARG 1  /* bad parameter (same checks as src/cli.hpp:93-95, src/index.cpp:11-12) */
+#define DNALN_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define DNALN_ERR_OOM 3          /* device or pinned memory exhausted / over the context's budget */
+#define DNALN_ERR_CAPACITY 4     /* a caller-sized output is too small; the needed size is returned */
+#define DNALN_ERR_NO_DEVICE 5    /* no usable CUDA device */
+#define DNALN_ERR_DEVICE 6       /* a kernel reported an internal inconsistency (error flag) */
+#define DNALN_ERR_NOT_FOUND 7    /* unknown index id */
+
+typedef struct dnaln_ctx dnaln_ctx;
+
+/* Scoring of the banded SW: match, mismatch, gap open/extension (a gap of length L
+ * costs gap_open + L*gap_ext), score of any pair involving N, band half-width.
+ * Mirrors ScoreParams (src/align.hpp:34-40). */
+typedef struct {
+  int32_t match, mismatch, gap_open, gap_ext, ambig, bw;
+} dnaln_score_params;
+
+/* Mirrors ChainParams (src/chain.hpp:30-36). */
+typedef struct {
+  int32_t max_gap, band, lookback, min_score, min_anchors;
+} dnaln_chain_params;
+
+/* Mirrors MapParams (src/mapper.hpp:25-35) minus the CPU-only simd/prefetch switches. */
+typedef struct {
+  int32_t k, w;
+  uint32_t max_occ;
+  int32_t max_cand;
+  double pri_ratio;
+  int32_t min_aln_score;
+  dnaln_score_params sc;
+  dnaln_chain_params ch;
+} dnaln_map_params;
+
+/* Mirrors AlignResult (src/align.hpp:49-60); its CIGAR (M/I/D ops, BAM encoding
+ * (len << 4) | op) is cigar[cigar_off .. cigar_off + cigar_len) of the call's buffer. */
+typedef struct {
+  int32_t score, qb, qe, tb, te, nm;
+  int64_t cigar_off;
+  int32_t cigar_len;
+  int32_t pad_;
+} dnaln_align_result;
+
+/* Mirrors MapRecord (src/mapper.hpp:37-44). contig = -1 for an unmapped read; pos is the
+ * 0-based leftmost aligned position within the contig; the CIGAR (soft clips included)
+ * is cigar[cigar_off .. cigar_off + cigar_len). */
+typedef struct {
+  int64_t pos;
+  int64_t cigar_off;
+  int32_t contig, score, nm, n_cand;
+  int32_t cigar_len;
+  uint8_t rev, mapq, pad_[2];
+} dnaln_map_record;
+
+/* Per-context counters of the last map/align call and running totals, the device
+ * counterpart of MapStats (src/mapper.hpp:46-49). Times are CUDA-event milliseconds
+ * measured on the context's stream around each stage. */
+typedef struct {
+  uint64_t reads, mapped, anchors, candidates, cells, sw_tasks_score, sw_tasks_tb, minimizers;
+  double ms_seed;     /* encode + sketch + probe */
+  double ms_chain;    /* anchors + chaining + candidates */
+  double ms_sw_score; /* score-only SW ranking pass */
+  double ms_sw_tb;    /* SW with traceback */
+  double ms_post;     /* choose, MAPQ, records, CIGAR compaction */
+  double ms_h2d, ms_d2h, ms_total;
+  uint64_t launches;  /* kernels of this library launched (library scans excluded) */
+} dnaln_stats;
+
+/* ---- context ---------------------------------------------------------------------- */
+const char* dnaln_gpu_version(void);
+int dnaln_gpu_ctx_create(int device, dnaln_ctx** out);
+int dnaln_gpu_ctx_destroy(dnaln_ctx* ctx);
+const char* dnaln_gpu_last_error(const dnaln_ctx* ctx);
+/* Launch on `stream` (a cudaStream_t) instead of the context's own stream; NULL restores it. */
+int dnaln_gpu_set_stream(dnaln_ctx* ctx, void* stream);
+int dnaln_gpu_get_stats(const dnaln_ctx* ctx, dnaln_stats* out);
+int dnaln_gpu_reset_stats(dnaln_ctx* ctx);
+/* Page-locked host buffers for fast transfers (pass to the *_batch calls). */
+int dnaln_gpu_host_alloc(dnaln_ctx* ctx, size_t bytes, void** out);
+int dnaln_gpu_host_free(dnaln_ctx* ctx, void* p);
+
+/* ---- genome + minimizer index: MinimizerIndex::build (src/index.cpp:10-45) ----------
+ * genome: one base code (A0 C1 G2 T3 N4) per byte, contigs concatenated; contig c is
+ * [contig_off[c], contig_off[c] + contig_len[c]). The index (hash table of 16-byte
+ * buckets + position array, the reference's layout, src/index.hpp:3-9,49-56) and the
+ * genome stay resident in HBM until dnaln_gpu_index_free. Requires k in [4, 28], w in
+ * [1, 255] and fewer than 2^31 bases (src/index.cpp:11-12, src/reference.cpp:21). */
+int dnaln_gpu_index_build(dnaln_ctx* ctx, const uint8_t* genome, uint64_t n_bases, const uint64_t* contig_off,
+                          const uint32_t* contig_len, int32_t n_contigs, int32_t k, int32_t w, int32_t* index_id);
+/* n_keys, n_positions, max_count, memory_bytes (src/index.hpp:43-46), n_buckets, device bytes */
+int dnaln_gpu_index_stats(const dnaln_ctx* ctx, int32_t index_id, uint64_t out6[6]);
+/* Copies the resident table (n_buckets keys/offsets/counts) and position array to the host. */
+int dnaln_gpu_index_export(dnaln_ctx* ctx, int32_t index_id, uint64_t* keys, uint32_t* offsets, uint32_t* counts,
+                           uint32_t* positions);
+int dnaln_gpu_index_free(dnaln_ctx* ctx, int32_t index_id);
+
+/* ---- per-stage entry points (batched forms of the reference's per-read calls) ------- */
+
+/* sketch (src/minimizer.hpp:34) over n sequences of base codes: sequence s is
+ * codes[seq_off[s] .. + seq_len[s]) and its positions are reported + pos_offset[s]
+ * (pos_offset may be NULL = 0). Its minimizers go to out_*[seq_off[s] + j], j <
+ * out_count[s] (a sequence never has more minimizers than bases). */
+int dnaln_gpu_sketch(dnaln_ctx* ctx, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,
+                     const uint32_t* pos_offset, int64_t n, int32_t k, int32_t w, uint64_t* out_hash,
+                     uint32_t* out_pos, uint32_t* out_strand, int32_t* out_count);
+
+/* MinimizerIndex::lookup (src/index.hpp:24-38) for n hashes: out_count[i] occurrences at
+ * positions[out_offset[i] ..] of the resident index (count 0 = absent). */
+int dnaln_gpu_lookup(dnaln_ctx* ctx, int32_t index_id, const uint64_t* hashes, int64_t n, uint32_t* out_offset,
+                     uint32_t* out_count);
+
+/* Chainer::run (src/chain.hpp:41) over n_sets anchor sets: set s is anchors
+ * [set_off[s], set_off[s+1]) of the rpos/qpos/strand columns, which are sorted in place
+ * per set as the reference does. Chains of set s go to out_*[set_off[s] + j],
+ * j < out_count[s], in the reference's order (score descending, stable). */
+int dnaln_gpu_chain(dnaln_ctx* ctx, uint32_t* rpos, int32_t* qpos, uint32_t* strand, const int64_t* set_off,
+                    int64_t n_sets, int32_t k, const dnaln_chain_params* p, int32_t* out_score,
+                    uint32_t* out_strand, int32_t* out_n, int64_t* out_dmin, int64_t* out_dmax, uint32_t* out_rpos,
+                    int32_t* out_count);
+
+/* Aligner::align (src/align.hpp:62-68): task i aligns query q[q_off[i] .. + q_len[i])
+ * against target t[t_off[i] .. + t_len[i]) (N-padded to q_len + 2bw, as
+ * src/align.cpp:36-39). With traceback = 0 only score is set. CIGARs go to `cigar`
+ * (capacity cigar_cap ops; DNALN_ERR_CAPACITY with *cigar_used = needed if short;
+ * sum of 2*q_len+1 always suffices). */
+int dnaln_gpu_align(dnaln_ctx* ctx, const uint8_t* q, const int64_t* q_off, const int32_t* q_len, const uint8_t* t,
+                    const int64_t* t_off, const int32_t* t_len, int64_t n, int32_t traceback,
+                    const dnaln_score_params* sp, dnaln_align_result* out, uint32_t* cigar, int64_t cigar_cap,
+                    int64_t* cigar_used);
+
+/* ---- whole batch: Mapper::map (src/mapper.cpp:75-223) --------------------------------
+ * n reads, ASCII, read r = seq[seq_off[r] .. + seq_len[r]); name_hash[r] = FNV-1a of the
+ * read name (src/common.hpp:136-140, dnaln_fnv1a below), the tie-break between equal
+ * best candidates. Records go to out[r]; CIGARs to `cigar` (capacity cigar_cap ops,
+ * DNALN_ERR_CAPACITY with *cigar_used = needed if short; sum of 2*len+3 suffices). */
+int dnaln_gpu_map_batch(dnaln_ctx* ctx, int32_t index_id, const char* seq, const int64_t* seq_off,
+                        const int32_t* seq_len, const uint32_t* name_hash, int64_t n, const dnaln_map_params* p,
+                        dnaln_map_record* out, uint32_t* cigar, int64_t cigar_cap, int64_t* cigar_used);
+
+/* Same pipeline with every buffer already in device memory (no host transfers); the
+ * CIGAR count is returned through the host pointer cigar_used. */
+int dnaln_gpu_map_batch_device(dnaln_ctx* ctx, int32_t index_id, const char* d_seq, const int64_t* d_seq_off,
+                               const int32_t* d_seq_len, const uint32_t* d_name_hash, int64_t n,
+                               const dnaln_map_params* p, dnaln_map_record* d_out, uint32_t* d_cigar,
+                               int64_t cigar_cap, int64_t* cigar_used);
+
+/* FNV-1a of a read name (src/common.hpp:136-140), and of n names concatenated in
+ * names[name_off[i] .. name_off[i+1]) into out[i]. */
+uint32_t dnaln_fnv1a(const char* s, int64_t n);
+void dnaln_fnv1a_batch(const char* names, const int64_t* name_off, int64_t n, uint32_t* out);
+
+/* ---- host-side helpers of the mapping path ------------------------------------------ */
+
+/* Mapper::append_sam (src/mapper.cpp:231-270) for n records into out (capacity cap
+ * bytes); *used = bytes written (or needed, with DNALN_ERR_CAPACITY). Names and
+ * qualities are concatenated with offsets name_off/qual_off (n+1 entries; qual may be
+ * NULL for '*'); contig names likewise with cname_off. */
+int dnaln_sam_format(const char* seq, const int64_t* seq_off, const int32_t* seq_len, const char* names,
+                     const int64_t* name_off, const char* qual, const int64_t* qual_off,
+                     const dnaln_map_record* rec, const uint32_t* cigar, int64_t n, const char* cnames,
+                     const int64_t* cname_off, char* out, int64_t cap, int64_t* used);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
