@@ -99,6 +99,7 @@ SIGNATURES = {
     "dnaln_gpu_chain": (C.c_int, [P, P, P, P, P, i64, i32, C.POINTER(ChainParams), P, P, P, P, P, P, P]),
     "dnaln_gpu_align": (C.c_int, [P, P, P, P, P, P, P, i64, i32, C.POINTER(ScoreParams), P, P, i64,
                                   C.POINTER(i64)]),
+    "dnaln_gpu_align_noalloc": (C.c_int, [P, P, P, P, P, P, i64, i32, i32, C.POINTER(ScoreParams), P, P, i64, P]),
     "dnaln_gpu_map_batch": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64, C.POINTER(i64)]),
     "dnaln_gpu_map_batch_device": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64,
                                              C.POINTER(i64)]),

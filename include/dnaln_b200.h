@@ -154,6 +154,25 @@ int dnaln_gpu_align(dnaln_ctx* ctx, const uint8_t* q, const int64_t* q_off, cons
                     const dnaln_score_params* sp, dnaln_align_result* out, uint32_t* cigar, int64_t cigar_cap,
                     int64_t* cigar_used);
 
+/* Banded SW for callers that cannot allocate device memory (no counterpart in the
+ * reference): a host framework that owns every device allocation, or a serving loop that
+ * may not allocate per request. Same results as dnaln_gpu_align, but every buffer is the
+ * caller's DEVICE memory and the call allocates nothing: its scratch is one fixed 64 MiB
+ * static device array in the library, held by each GPU that loads it until exit.
+ * Task i aligns d_q[d_q_off[i] ..+ d_q_len[i]) against d_t[d_t_off[i] ..+ d_t_len[i]);
+ * every d_q_len[i] must be <= max_qlen. Its result goes to d_out[i] and, with traceback,
+ * its CIGAR to d_cigar[i * cigar_stride ..] (cigar_stride >= 2*max_qlen+1; cigar_off =
+ * i * cigar_stride). Launches go to `stream` (a cudaStream_t, NULL = default stream) and
+ * the call returns after they finish. Returns DNALN_ERR_INVALID_ARG when one warp of
+ * tasks of max_qlen rows at this band width does not fit the 64 MiB, DNALN_ERR_DEVICE
+ * when a query exceeds max_qlen. The first call on each device looks up the array's
+ * address (cudaGetSymbolAddress) and should come before any stream capture. All calls
+ * share the array: calls that overlap on the GPU race, so serialize them. */
+int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_off, const int32_t* d_q_len, const uint8_t* d_t,
+                            const int64_t* d_t_off, const int32_t* d_t_len, int64_t n, int32_t max_qlen,
+                            int32_t traceback, const dnaln_score_params* sp, dnaln_align_result* d_out,
+                            uint32_t* d_cigar, int64_t cigar_stride, void* stream);
+
 /* ---- whole batch: Mapper::map (src/mapper.cpp:75-223) --------------------------------
  * n reads, ASCII, read r = seq[seq_off[r] .. + seq_len[r]); name_hash[r] = FNV-1a of the
  * read name (src/common.hpp:136-140, dnaln_fnv1a below), the tie-break between equal
