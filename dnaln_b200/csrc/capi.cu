@@ -159,13 +159,15 @@ std::vector<int32_t> chain_cost_lut(int k, int band) {
 __global__ void k_len64(const int32_t* __restrict__ len, int64_t n, int64_t* __restrict__ out,
                         unsigned long long* __restrict__ max_len) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  int32_t l = 0;
   if (i < n) {
-    const int32_t l = len[i];
-    out[i] = l < 0 ? 0 : l;
-    atomicMax(max_len, static_cast<unsigned long long>(l < 0 ? 0 : l));
+    l = len[i] < 0 ? 0 : len[i];
+    out[i] = l;
   } else if (i == n) {
     out[n] = 0;
   }
+  l = __reduce_max_sync(0xffffffffu, l);  // one atomic per warp instead of one per read
+  if ((threadIdx.x & 31) == 0 && l > 0) atomicMax(max_len, static_cast<unsigned long long>(l));
 }
 
 __global__ void k_cig_slots(const int64_t* __restrict__ pofs, int64_t n, int64_t* __restrict__ out) {

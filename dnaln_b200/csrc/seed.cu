@@ -197,10 +197,14 @@ __device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const 
     const uint64_t ki = a.keys[i];
     const uint32_t si = key_strand(ki);
     const int64_t ri = key_rpos(ki), qi = key_qpos(ki);
-    long long best = LLONG_MIN;
+    // Per round of 32 predecessors one redux over score * 32 + (31 - lane): the largest
+    // score, ties to the smallest lane = the nearest j; earlier (nearer) rounds win ties
+    // across rounds through the strict '>' below — the reference's scan order.
+    int best_sc = 0, best_j = -1;
     for (int r0 = 0; r0 < cp.lookback; r0 += 32) {
       const int t = r0 + lane, j = i - 1 - t;
       bool stop = true;
+      int key = INT_MIN;
       if (t < cp.lookback && j >= 0) {
         const uint64_t kj = a.keys[j];
         const int64_t dr = ri - key_rpos(kj);
@@ -213,20 +217,22 @@ __device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const 
               int64_t g = dq < dr ? dq : dr;
               if (g > cp.k) g = cp.k;
               const int sc = a.f[j] + static_cast<int>(g) - cp.cost[dd];
-              const long long key = static_cast<long long>(sc) * 4294967296LL + j;
-              best = key > best ? key : best;
+              key = sc * 32 + (31 - lane);
             }
           }
         }
       }
+      const int m = __reduce_max_sync(0xffffffffu, key);
+      if (m != INT_MIN && (best_j < 0 || (m >> 5) > best_sc)) {
+        best_sc = m >> 5;
+        best_j = i - 1 - (r0 + 31 - (m & 31));
+      }
       if (__all_sync(0xffffffffu, stop)) break;  // every later predecessor is out of range too
     }
-    best = warp_max_ll(best);
     if (lane == 0) {
-      const int sc = best == LLONG_MIN ? 0 : static_cast<int>(best >> 32);
-      if (best != LLONG_MIN && sc > cp.k) {
-        a.f[i] = sc;
-        a.prev[i] = static_cast<int>(best & 0xffffffffLL);
+      if (best_j >= 0 && best_sc > cp.k) {
+        a.f[i] = best_sc;
+        a.prev[i] = best_j;
       } else {
         a.f[i] = cp.k;
         a.prev[i] = -1;
@@ -276,6 +282,132 @@ __device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const 
   __syncwarp();
   warp_sort_u64(a.ord, m);
   return m;
+}
+
+// Ascending bitonic sort of one 64-bit key per lane across the warp (lane order).
+__device__ __forceinline__ uint64_t warp_bitonic_u64(uint64_t v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const uint64_t o = __shfl_xor_sync(0xffffffffu, v, j);
+      const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+      v = keep_min ? (o < v ? o : v) : (o > v ? o : v);
+    }
+  }
+  return v;
+}
+
+// Chaining and candidate selection of a read with n <= 32 anchors, entirely in registers:
+// lane j holds anchor j (after the sort), its f and prev; every sequential step of the
+// reference (DP rows, the walk, the candidate loop) runs as a warp-uniform loop whose
+// operands come from shuffles, and the DP's predecessor max is one redux per row.
+// Same results as chain_core + the candidate loop of k_chain_map.
+__device__ void chain_map_small(uint64_t key, int n, const ChainParamsDev& cp, const CandParams& cand,
+                                const DevIndex& ix, const CandBuf& cb, int64_t r) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  key = warp_bitonic_u64(key);  // lanes >= n hold ~0 and sort last
+  const uint32_t st = key_strand(key);
+  const int32_t rp = static_cast<int32_t>(key_rpos(key)), qp = key_qpos(key);
+  // DP (src/chain.cpp:22-45); row i's best predecessor: max over lanes j < i of
+  // score * 32 + j, i.e. ties to the nearest j
+  int f = cp.k, prev = -1;
+  for (int i = 1; i < n; ++i) {
+    const uint32_t si = __shfl_sync(FULL, st, i);
+    const int32_t ri = __shfl_sync(FULL, rp, i), qi = __shfl_sync(FULL, qp, i);
+    int kv = INT_MIN;
+    if (lane < i && lane >= i - cp.lookback && st == si) {
+      const int64_t dr = static_cast<int64_t>(ri) - rp;
+      const int64_t dq = static_cast<int64_t>(qi) - qp;
+      if (dr <= cp.max_gap && dr > 0 && dq > 0) {
+        const int64_t dd = dr > dq ? dr - dq : dq - dr;
+        if (dd <= cp.band) {
+          int64_t g = dq < dr ? dq : dr;
+          if (g > cp.k) g = cp.k;
+          kv = (f + static_cast<int>(g) - cp.cost[dd]) * 32 + lane;
+        }
+      }
+    }
+    const int m = __reduce_max_sync(FULL, kv);
+    if (lane == i && m != INT_MIN && (m >> 5) > cp.k) {
+      f = m >> 5;
+      prev = m & 31;
+    }
+  }
+  // extraction order: f descending, index ascending (src/chain.cpp:49-50)
+  const uint64_t ok = lane < n ? (static_cast<uint64_t>(desc32(f)) << 32 | static_cast<uint32_t>(lane)) : ~0ULL;
+  const int end_of = static_cast<int>(warp_bitonic_u64(ok) & 0xffffffffu);
+  const int64_t dg = static_cast<int64_t>(rp) - qp;
+  // walk (src/chain.cpp:52-67); chain m is kept in the registers of lane m
+  uint32_t used = 0;
+  int m = 0, c_score = 0;
+  uint32_t c_strand = 0, c_rpos = 0;
+  int64_t c_dmin = 0, c_dmax = 0;
+  for (int e = 0; e < n; ++e) {
+    const int end = __shfl_sync(FULL, end_of, e);
+    if ((used >> end) & 1u) continue;
+    int i = end, cnt = 0;
+    int64_t dmin = LLONG_MAX, dmax = LLONG_MIN;
+    while (i >= 0 && !((used >> i) & 1u)) {
+      used |= 1u << i;
+      ++cnt;
+      const int64_t d = __shfl_sync(FULL, dg, i);
+      dmin = d < dmin ? d : dmin;
+      dmax = d > dmax ? d : dmax;
+      i = __shfl_sync(FULL, prev, i);
+    }
+    const int f_end = __shfl_sync(FULL, f, end);
+    const int f_stop = __shfl_sync(FULL, f, i >= 0 ? i : 0);
+    const uint32_t s_end = __shfl_sync(FULL, st, end);
+    const int32_t r_end = __shfl_sync(FULL, rp, end);
+    const int score = f_end - (i >= 0 ? f_stop : 0);
+    if (score < cp.min_score || cnt < cp.min_anchors) continue;
+    if (lane == m) {
+      c_score = score;
+      c_strand = s_end;
+      c_rpos = static_cast<uint32_t>(r_end);
+      c_dmin = dmin;
+      c_dmax = dmax;
+    }
+    ++m;
+  }
+  // chains by score descending, ties in extraction order (stable_sort, src/chain.cpp:68)
+  const uint64_t sk = lane < m ? (static_cast<uint64_t>(desc32(c_score)) << 32 | static_cast<uint32_t>(lane)) : ~0ULL;
+  const int chain_at = static_cast<int>(warp_bitonic_u64(sk) & 0xffffffffu);
+  // candidate loci (src/mapper.cpp:40-62); accepted candidate x is kept by lane x
+  int nd = 0;
+  int64_t my_diag = 0;
+  uint32_t my_rev = 0;
+  const int64_t cbase = r * cand.max_cand;
+  if (m > 0) {
+    const double min_score =
+        static_cast<double>(__shfl_sync(FULL, c_score, __shfl_sync(FULL, chain_at, 0))) * cand.pri_ratio;
+    for (int c = 0; c < m; ++c) {
+      const int ci = __shfl_sync(FULL, chain_at, c);
+      const int sc = __shfl_sync(FULL, c_score, ci);
+      if (static_cast<double>(sc) < min_score || nd >= cand.max_cand) break;
+      const int64_t dmin = __shfl_sync(FULL, c_dmin, ci), dmax = __shfl_sync(FULL, c_dmax, ci);
+      const int64_t diag = dmin + (dmax - dmin) / 2;
+      const uint32_t strand = __shfl_sync(FULL, c_strand, ci);
+      const uint32_t rpos = __shfl_sync(FULL, c_rpos, ci);
+      const int64_t dd = my_diag - diag;
+      if (__any_sync(FULL, lane < nd && my_rev == strand && (dd < 0 ? -dd : dd) <= cand.bw)) continue;
+      if (lane == nd) {
+        my_diag = diag;
+        my_rev = strand;
+      }
+      if (lane == 0) {
+        cb.rev[cbase + nd] = static_cast<uint8_t>(strand);
+        cb.contig[cbase + nd] = contig_of(ix, rpos);
+        cb.diag[cbase + nd] = diag;
+        cb.wstart[cbase + nd] = diag - cand.bw;
+      }
+      ++nd;
+    }
+  }
+  if (lane == 0) cb.n_cand[r] = nd;
 }
 
 struct ChainSmem {
@@ -374,6 +506,10 @@ __global__ void __launch_bounds__(kChainWarps * 32)
     w_off += total;
   }
   __syncwarp();
+  if (na <= 32) {  // the common case: everything in registers
+    chain_map_small(lane < na ? a.keys[lane] : ~0ULL, na, cp, cand, ix, cb, r);
+    return;
+  }
   const int m = chain_core(a, na, cp, as, a0);
   // candidate loci (src/mapper.cpp:40-62)
   if (lane == 0) {
