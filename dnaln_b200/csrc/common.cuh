@@ -34,10 +34,13 @@ __host__ __device__ __forceinline__ uint64_t hash64(uint64_t key, uint64_t mask)
   return key;
 }
 
-// ASCII -> base code, A/a 0, C/c 1, G/g 2, T/t/U/u 3, else 4 (src/common.hpp:23-31).
-__host__ __device__ __forceinline__ uint8_t nt4(uint8_t c) {
-  const uint8_t u = c & 0xDF;  // fold case
-  return u == 'A' ? 0 : u == 'C' ? 1 : u == 'G' ? 2 : (u == 'T' || u == 'U') ? 3 : 4;
+// ASCII -> base code, A/a 0, C/c 1, G/g 2, T/t/U/u 3, else 4 (src/common.hpp:23-31),
+// branch-free: (c & 0xDF) - 'A' indexes a bit set of {A, C, G, T, U}; for those letters
+// ((c >> 1) ^ (c >> 2)) & 3 is 0, 1, 2, 3, 3. Checked against the table for all 256 bytes.
+__host__ __device__ __forceinline__ uint32_t nt4(uint32_t c) {
+  const uint32_t u = (c & 0xDFu) - 0x41u;
+  const bool ok = u < 21u && ((0x180045u >> u) & 1u);
+  return ok ? (((c >> 1) ^ (c >> 2)) & 3u) : 4u;
 }
 
 // One band-SW task, in either addressing mode:

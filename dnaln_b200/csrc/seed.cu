@@ -108,6 +108,117 @@ __device__ int warp_sketch(CodeAt code_at, int len, int k, int w, SketchSmem& sm
   return count;
 }
 
+// 16-bit x -> its bits at the even positions of a 32-bit word.
+__device__ __forceinline__ uint32_t spread16(uint32_t x) {
+  x = (x | (x << 8)) & 0x00FF00FFu;
+  x = (x | (x << 4)) & 0x0F0F0F0Fu;
+  x = (x | (x << 2)) & 0x33333333u;
+  x = (x | (x << 1)) & 0x55555555u;
+  return x;
+}
+
+// hash64 for 2k <= 32: every step is either reduced mod 2^32 and then masked to 2k bits,
+// or a right shift of a value below 2^2k, so 32-bit arithmetic gives the same bits.
+__device__ __forceinline__ uint32_t hash32(uint32_t key, uint32_t mask) {
+  key = (~key + (key << 21)) & mask;
+  key = key ^ key >> 24;
+  key = ((key + (key << 3)) + (key << 8)) & mask;
+  key = key ^ key >> 14;
+  key = ((key + (key << 2)) + (key << 4)) & mask;
+  key = key ^ key >> 28;
+  key = (key + (key << 31)) & mask;
+  return key;
+}
+
+// Value of `cur` held d lanes to the left (0 <= d <= 31); lanes left of d read `prv`, the
+// previous chunk's value.
+__device__ __forceinline__ uint64_t from_left(uint64_t cur, uint64_t prv, int d) {
+  const int lane = threadIdx.x & 31;
+  const int src = (lane - d) & 31;
+  const uint64_t a = __shfl_sync(0xffffffffu, cur, src);
+  const uint64_t b = __shfl_sync(0xffffffffu, prv, src);
+  return lane >= d ? a : b;
+}
+
+__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return b < a ? b : a; }
+
+// warp_sketch for k <= 15 and w <= 32 (the defaults are 15 and 10), same output. Per
+// chunk of 32 k-mer starts each lane loads one base code; three ballots give the 64
+// positions the chunk's k-mers cover as bit planes (low bit, high bit, N), from which a
+// lane assembles its k-mer directly: spreading the k low/high bits into alternate bit
+// positions gives the reverse-complement word, and a bit reversal the forward word. The
+// hash runs in 32 bits. Each lane packs (hash, position, strand) into one 64-bit key, so
+// the leftmost minimum of a window is the minimum key; windows of w keys are minima of
+// power-of-two windows (doubling with shuffles), previous-chunk values kept in registers.
+template <class CodeAt, class Emit>
+__device__ int warp_sketch_fast(CodeAt code_at, int len, int k, int w, Emit emit) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const uint32_t kmask = (1u << k) - 1u, mask2k = (1u << (2 * k)) - 1u;
+  const int nk = len - k + 1;
+  uint64_t P[6], prvP[6];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) prvP[j] = ~0ULL;
+  int count = 0, carry_bad = -1, p_arg = -1;
+  uint32_t c_lo = lane < len ? code_at(lane) : 4u;
+  uint32_t c_hi = 32 + lane < len ? code_at(32 + lane) : 4u;
+  for (int base = 0; base < nk; base += 32) {
+    if (base > 0) {
+      c_lo = c_hi;
+      c_hi = base + 32 + lane < len ? code_at(base + 32 + lane) : 4u;
+    }
+    const uint64_t plo = static_cast<uint64_t>(__ballot_sync(FULL, c_lo & 1u)) |
+                         static_cast<uint64_t>(__ballot_sync(FULL, c_hi & 1u)) << 32;
+    const uint64_t phi = static_cast<uint64_t>(__ballot_sync(FULL, (c_lo >> 1) & 1u)) |
+                         static_cast<uint64_t>(__ballot_sync(FULL, (c_hi >> 1) & 1u)) << 32;
+    const uint64_t pn = static_cast<uint64_t>(__ballot_sync(FULL, c_lo > 3u)) |
+                        static_cast<uint64_t>(__ballot_sync(FULL, c_hi > 3u)) << 32;
+    const int s = base + lane;
+    const bool kv = s < nk && ((static_cast<uint32_t>(pn >> lane) & kmask) == 0u);
+    uint64_t key = ~0ULL;
+    if (kv) {
+      const uint32_t L = static_cast<uint32_t>(plo >> lane) & kmask, H = static_cast<uint32_t>(phi >> lane) & kmask;
+      const uint32_t sl = spread16(L), sh = spread16(H);
+      const uint32_t rev = (sl | sh << 1) ^ mask2k;       // base m at bits 2m, complemented
+      const uint32_t fwd = __brev(sh | sl << 1) >> (32 - 2 * k);  // base m at bits 2(k-1-m)
+      const uint32_t st = rev < fwd;
+      const uint32_t h = fwd != rev ? hash32(st ? rev : fwd, mask2k) : 0xFFFFFFFFu;
+      key = static_cast<uint64_t>(h) << 32 | static_cast<uint32_t>(s) << 1 | st;
+    }
+    const unsigned bad = __ballot_sync(FULL, s < nk && !kv);
+    const unsigned upto = bad & (0xffffffffu >> (31 - lane));
+    const int lastbad = upto ? base + 31 - __clz(upto) : carry_bad;
+    carry_bad = bad ? base + 31 - __clz(bad) : carry_bad;
+    // minima of windows of 2^j keys ending at s
+    P[0] = key;
+#pragma unroll
+    for (int j = 0; j < 5; ++j)
+      if ((2 << j) <= w) P[j + 1] = umin64(P[j], from_left(P[j], prvP[j], 1 << j));
+    uint64_t m = ~0ULL;
+    int off = 0;
+#pragma unroll
+    for (int j = 5; j >= 0; --j)
+      if (w & (1 << j)) {
+        m = umin64(m, from_left(P[j], prvP[j], off));
+        off += 1 << j;
+      }
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+      if ((1 << j) <= w) prvP[j] = P[j];
+    int arg = -1;
+    if (s < nk && s >= w - 1 && lastbad < s - w + 1 && static_cast<uint32_t>(m >> 32) != 0xFFFFFFFFu)
+      arg = static_cast<int>(static_cast<uint32_t>(m) >> 1);
+    const int up = __shfl_up_sync(FULL, arg, 1);
+    const int prev_arg = lane == 0 ? p_arg : up;
+    const bool em = arg >= 0 && arg != prev_arg;
+    const unsigned ball = __ballot_sync(FULL, em);
+    if (em) emit(count + __popc(ball & ((1u << lane) - 1u)), m >> 32, arg, static_cast<uint32_t>(m) & 1u);
+    count += __popc(ball);
+    p_arg = __shfl_sync(FULL, arg, 31);
+  }
+  return count;
+}
+
 __device__ __forceinline__ void probe(const DevIndex& ix, uint64_t h, uint32_t& off, uint32_t& cnt,
                                       uint32_t* err) {
   uint64_t i = h & ix.mask;
@@ -436,11 +547,13 @@ __global__ void __launch_bounds__(kSeedWarps * 32)
     fw[i] = c;
     rc[len - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
   }
-  const int cnt = warp_sketch([&](int i) { return static_cast<uint32_t>(nt4(s[i])); }, len, sp.k, sp.w, sm[wib],
-                              [&](int rank, uint64_t h, int pos, uint32_t st) {
-                                mb.hash[so + rank] = h;
-                                mb.pos[so + rank] = static_cast<uint32_t>(pos) | st << 31;
-                              });
+  const auto code_at = [&](int i) { return nt4(s[i]); };
+  const auto emit = [&](int rank, uint64_t h, int pos, uint32_t st) {
+    mb.hash[so + rank] = h;
+    mb.pos[so + rank] = static_cast<uint32_t>(pos) | st << 31;
+  };
+  const int cnt = (sp.k <= 15 && sp.w <= 32) ? warp_sketch_fast(code_at, len, sp.k, sp.w, emit)
+                                             : warp_sketch(code_at, len, sp.k, sp.w, sm[wib], emit);
   __syncwarp();
   long long anchors = 0;
   for (int j = lane; j < cnt; j += 32) {
@@ -552,12 +665,14 @@ __global__ void __launch_bounds__(kSeedWarps * 32)
   const int64_t so = seq_off[r];
   const uint8_t* s = codes + so;
   const uint32_t po = pos_offset ? pos_offset[r] : 0u;
-  const int cnt = warp_sketch([&](int i) { return static_cast<uint32_t>(s[i]); }, seq_len[r], k, w, sm[wib],
-                              [&](int rank, uint64_t h, int pos, uint32_t st) {
-                                out_hash[so + rank] = h;
-                                out_pos[so + rank] = static_cast<uint32_t>(pos) + po;
-                                out_strand[so + rank] = st;
-                              });
+  const auto code_at = [&](int i) { return static_cast<uint32_t>(s[i]); };
+  const auto emit = [&](int rank, uint64_t h, int pos, uint32_t st) {
+    out_hash[so + rank] = h;
+    out_pos[so + rank] = static_cast<uint32_t>(pos) + po;
+    out_strand[so + rank] = st;
+  };
+  const int cnt = (k <= 15 && w <= 32) ? warp_sketch_fast(code_at, seq_len[r], k, w, emit)
+                                       : warp_sketch(code_at, seq_len[r], k, w, sm[wib], emit);
   if (lane == 0) out_count[r] = cnt;
 }
 
