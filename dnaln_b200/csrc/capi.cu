@@ -191,24 +191,23 @@ int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks,
                       const uint8_t* qbase, const uint8_t* tbase, const SwParams& sp, SwResult* res, int rows_max,
                       uint32_t* cig, const int64_t* cig_off) {
   if (n_max <= 0) return DNALN_OK;
-  const size_t dir_w = tb ? sw_dir_bytes_per_warp(sp.W, rows_max > 0 ? rows_max : 1) : 0;
-  const size_t band_w = sw_band_bytes_per_warp(sp.W, bytes_ok);
-  const size_t per_warp = dir_w + band_w;
-  int64_t chunk = n_max;
-  if (per_warp > 0) {
-    const int64_t warps = static_cast<int64_t>(c->dir_cap_bytes / per_warp);
-    chunk = (warps < 1 ? 1 : warps) * 32;
-    if (chunk > n_max) chunk = ((n_max + 31) / 32) * 32;
+  const int64_t G = kSwTaskGroup;
+  const size_t dir_t = tb ? sw_dir_bytes_per_task(sp.W, rows_max) : 0;
+  const size_t band_t = sw_band_bytes_per_task(sp.W, bytes_ok);
+  const size_t per_group = G * (dir_t + band_t);
+  int64_t chunk = ((n_max + G - 1) / G) * G;
+  if (per_group > 0) {
+    const int64_t groups = static_cast<int64_t>(c->dir_cap_bytes / per_group);
+    chunk = std::min<int64_t>(chunk, (groups < 1 ? 1 : groups) * G);
   }
-  const int64_t chunk_warps = (chunk + 31) / 32;
   uint32_t* dir = nullptr;
   int* band = nullptr;
-  if (dir_w) {
-    dir = dbuf<uint32_t>(c, "sw_dir", static_cast<size_t>(chunk_warps) * dir_w / sizeof(uint32_t));
+  if (dir_t) {
+    dir = dbuf<uint32_t>(c, "sw_dir", static_cast<size_t>(chunk) * dir_t / sizeof(uint32_t));
     if (!dir) return DNALN_ERR_OOM;
   }
-  if (band_w) {
-    band = dbuf<int>(c, "sw_band", static_cast<size_t>(chunk_warps) * band_w / sizeof(int));
+  if (band_t) {
+    band = dbuf<int>(c, "sw_band", static_cast<size_t>(chunk) * band_t / sizeof(int));
     if (!band) return DNALN_ERR_OOM;
   }
   for (int64_t b = 0; b < n_max; b += chunk) {

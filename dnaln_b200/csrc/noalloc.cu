@@ -141,14 +141,17 @@ extern "C" int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_of
   const SwParams p = make_sw_params(*sp);
   const bool bytes_ok = sw_bytes_ok(*sp);
   const int rows = max_qlen > 0 ? max_qlen : 1;
-  const size_t dir_w = tb ? sw_dir_bytes_per_warp(p.W, rows) : 0;
-  const size_t band_w = sw_band_bytes_per_warp(p.W, bytes_ok);
-  // scratch per warp of 32 tasks: descriptors, CIGAR offsets, results, direction bits, band rows
-  const size_t per_warp = 32 * (sizeof(SwTask) + sizeof(int64_t) + sizeof(SwResult)) + dir_w + band_w;
+  const size_t dir_t = tb ? sw_dir_bytes_per_task(p.W, rows) : 0;
+  const size_t band_t = sw_band_bytes_per_task(p.W, bytes_ok);
+  // scratch per group of kSwTaskGroup tasks: descriptors, CIGAR offsets, results,
+  // direction codes, band rows
+  const int64_t G = kSwTaskGroup;
+  const size_t per_group = G * (sizeof(SwTask) + sizeof(int64_t) + sizeof(SwResult) + dir_t + band_t);
   const size_t avail = kNoAllocScratchBytes - kHeader - 4 * 256;
-  const int64_t warps = static_cast<int64_t>(avail / per_warp);
-  if (warps < 1) return DNALN_ERR_INVALID_ARG;  // one warp of this query length / band does not fit 64 MiB
-  const int64_t chunk = std::min<int64_t>(warps * 32, ((n + 31) / 32) * 32);
+  const int64_t groups = static_cast<int64_t>(avail / per_group);
+  if (groups < 1) return DNALN_ERR_INVALID_ARG;  // one group of this query length / band does not fit 64 MiB
+  const int64_t chunk = std::min<int64_t>(groups * G, ((n + G - 1) / G) * G);
+  const size_t dir_w = dir_t, band_w = band_t;
 
   uint32_t* err = reinterpret_cast<uint32_t*>(base_ptr);
   unsigned char* cur = base_ptr + kHeader;
@@ -159,7 +162,7 @@ extern "C" int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_of
   SwResult* res = reinterpret_cast<SwResult*>(cur);
   cur += align256(chunk * sizeof(SwResult));
   uint32_t* dir = dir_w ? reinterpret_cast<uint32_t*>(cur) : nullptr;
-  cur += align256((chunk / 32) * dir_w);
+  cur += align256(chunk * dir_w);
   int* band = band_w ? reinterpret_cast<int*>(cur) : nullptr;
 
   if (cudaMemsetAsync(err, 0, sizeof(uint32_t), st) != cudaSuccess) return DNALN_ERR_CUDA;
