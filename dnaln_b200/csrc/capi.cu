@@ -41,7 +41,7 @@ struct DevBuf {
 };
 
 struct IndexRes {
-  DevBuf table, positions, genome, coff, clen;
+  DevBuf table, positions, genome, coff, clen, nruns;
   uint64_t n_keys = 0, n_pos = 0, n_buckets = 0, n_bases = 0;
   uint32_t max_count = 0;
   int32_t n_contigs = 0, k = 0, w = 0;
@@ -210,12 +210,14 @@ int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks,
     band = dbuf<int>(c, "sw_band", static_cast<size_t>(chunk) * band_t / sizeof(int));
     if (!band) return DNALN_ERR_OOM;
   }
+  int* fb = dbuf<int>(c, "sw_fb", static_cast<size_t>(chunk) + 1);
+  if (!fb) return DNALN_ERR_OOM;
   for (int64_t b = 0; b < n_max; b += chunk) {
     const int cnt = static_cast<int>(n_max - b < chunk ? n_max - b : chunk);
     if (!launch_sw(c->st, tb, bytes_ok, tasks, static_cast<int>(b), cnt, n_max, n_dev, qbase, tbase, sp, res, dir,
-                   rows_max, cig, cig_off, band, c->d_err))
+                   rows_max, cig, cig_off, band, fb, c->d_err))
       return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
-    ++c->stats.launches;
+    c->stats.launches += static_cast<uint64_t>(sw_launches(sp.W, bytes_ok, tb));
   }
   CK(cudaGetLastError());
   return DNALN_OK;
@@ -417,7 +419,7 @@ int dalloc(dnaln_ctx* c, DevBuf& b, size_t bytes) {
 }
 
 void free_index(IndexRes& r) {
-  for (DevBuf* b : {&r.table, &r.positions, &r.genome, &r.coff, &r.clen})
+  for (DevBuf* b : {&r.table, &r.positions, &r.genome, &r.coff, &r.clen, &r.nruns})
     if (b->p) cudaFree(b->p);
 }
 
@@ -542,8 +544,20 @@ int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases,
   std::vector<ulonglong2> table(h.keys.size());
   for (size_t i = 0; i < table.size(); ++i)
     table[i] = make_ulonglong2(h.keys[i], static_cast<uint64_t>(h.offs[i]) | static_cast<uint64_t>(h.cnts[i]) << 32);
+  // maximal runs of non-ACGT codes: SW tasks whose window avoids them skip the N scan
+  std::vector<uint2> runs;
+  for (uint64_t i = 0; i < n_bases;) {
+    if (genome[i] <= 3) {
+      ++i;
+      continue;
+    }
+    uint64_t j = i;
+    while (j < n_bases && genome[j] > 3) ++j;
+    runs.push_back(make_uint2(static_cast<uint32_t>(i), static_cast<uint32_t>(j)));
+    i = j;
+  }
   int e = DNALN_OK;
-  if ((e = dalloc(c, r.table, table.size() * sizeof(ulonglong2))) ||
+  if ((e = dalloc(c, r.nruns, runs.size() * sizeof(uint2))) || (e = dalloc(c, r.table, table.size() * sizeof(ulonglong2))) ||
       (e = dalloc(c, r.positions, h.pos.size() * sizeof(uint32_t))) || (e = dalloc(c, r.genome, n_bases)) ||
       (e = dalloc(c, r.coff, n_contigs * sizeof(uint64_t))) || (e = dalloc(c, r.clen, n_contigs * sizeof(uint32_t)))) {
     free_index(r);
@@ -558,6 +572,7 @@ int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases,
   up(r.genome, genome, n_bases);
   up(r.coff, contig_off, n_contigs * sizeof(uint64_t));
   up(r.clen, contig_len, n_contigs * sizeof(uint32_t));
+  up(r.nruns, runs.data(), runs.size() * sizeof(uint2));
   if (x != cudaSuccess) {
     free_index(r);
     return fail(c, DNALN_ERR_CUDA, "index upload: %s", cudaGetErrorString(x));
@@ -567,6 +582,8 @@ int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases,
   r.dev.genome = static_cast<const uint8_t*>(r.genome.p);
   r.dev.contig_off = static_cast<const uint64_t*>(r.coff.p);
   r.dev.contig_len = static_cast<const uint32_t*>(r.clen.p);
+  r.dev.n_runs = static_cast<const uint2*>(r.nruns.p);
+  r.dev.n_n_runs = static_cast<int32_t>(runs.size());
   r.dev.mask = h.mask;
   r.dev.n_contigs = n_contigs;
   r.dev.k = k;
@@ -587,7 +604,7 @@ int dnaln_gpu_index_stats(const dnaln_ctx* cc, int32_t id, uint64_t out6[6]) {
   out6[2] = r->max_count;
   out6[3] = r->n_buckets * 16 + r->n_pos * 4;  // src/index.hpp:46
   out6[4] = r->n_buckets;
-  out6[5] = r->table.cap + r->positions.cap + r->genome.cap + r->coff.cap + r->clen.cap;
+  out6[5] = r->table.cap + r->positions.cap + r->genome.cap + r->coff.cap + r->clen.cap + r->nruns.cap;
   return DNALN_OK;
 }
 

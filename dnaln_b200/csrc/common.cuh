@@ -53,8 +53,11 @@ struct SwTask {
   int64_t q_off;
   int64_t t_start, t_lo, t_hi;
   int32_t qlen;
-  int32_t slot;  // result / CIGAR slot
+  int32_t slot;   // result / CIGAR slot
+  int32_t flags;  // kTaskNoN: the producer checked that the window [0, qlen + W - 1) has no N
+  int32_t pad_;
 };
+constexpr int32_t kTaskNoN = 1;
 
 struct SwResult {
   int32_t score, qb, qe, tb, te, nm;

@@ -29,6 +29,9 @@ __device__ __forceinline__ SwTask cand_task(int64_t r, int c, const int64_t* pof
   t.t_lo = ws > cb0 ? ws : cb0;
   t.t_hi = we < ce ? we : ce;
   t.slot = 0;
+  // the whole window inside the contig and clear of the genome's N runs: no N to score
+  t.flags = (t.t_lo == ws && t.t_hi == we && !genome_has_n(ix, ws, we)) ? kTaskNoN : 0;
+  t.pad_ = 0;
   return t;
 }
 

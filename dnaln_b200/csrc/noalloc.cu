@@ -65,6 +65,8 @@ __global__ void k_na_tasks(int64_t base, int count, const int64_t* __restrict__ 
   t.t_lo = t_off[i];
   t.t_hi = t_off[i] + (tl < tmax ? tl : tmax);
   t.slot = j;
+  t.flags = 0;
+  t.pad_ = 0;
   tasks[j] = t;
   cig_off[j] = i * cigar_stride;
 }
@@ -144,10 +146,10 @@ extern "C" int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_of
   const size_t dir_t = tb ? sw_dir_bytes_per_task(p.W, rows) : 0;
   const size_t band_t = sw_band_bytes_per_task(p.W, bytes_ok);
   // scratch per group of kSwTaskGroup tasks: descriptors, CIGAR offsets, results,
-  // direction codes, band rows
+  // direction codes, band rows, int32-path task list (one more int for its count)
   const int64_t G = kSwTaskGroup;
-  const size_t per_group = G * (sizeof(SwTask) + sizeof(int64_t) + sizeof(SwResult) + dir_t + band_t);
-  const size_t avail = kNoAllocScratchBytes - kHeader - 4 * 256;
+  const size_t per_group = G * (sizeof(SwTask) + sizeof(int64_t) + sizeof(SwResult) + dir_t + band_t + sizeof(int));
+  const size_t avail = kNoAllocScratchBytes - kHeader - 6 * 256;
   const int64_t groups = static_cast<int64_t>(avail / per_group);
   if (groups < 1) return DNALN_ERR_INVALID_ARG;  // one group of this query length / band does not fit 64 MiB
   const int64_t chunk = std::min<int64_t>(groups * G, ((n + G - 1) / G) * G);
@@ -164,6 +166,8 @@ extern "C" int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_of
   uint32_t* dir = dir_w ? reinterpret_cast<uint32_t*>(cur) : nullptr;
   cur += align256(chunk * dir_w);
   int* band = band_w ? reinterpret_cast<int*>(cur) : nullptr;
+  cur += align256(chunk * band_w);
+  int* fb = reinterpret_cast<int*>(cur);
 
   if (cudaMemsetAsync(err, 0, sizeof(uint32_t), st) != cudaSuccess) return DNALN_ERR_CUDA;
   for (int64_t b = 0; b < n; b += chunk) {
@@ -172,7 +176,7 @@ extern "C" int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_of
     k_na_tasks<<<blocks, 128, 0, st>>>(b, cnt, d_q_off, d_q_len, d_t_off, d_t_len, max_qlen, p.W,
                                        tb ? cigar_stride : 0, tasks, cig_off, err);
     if (!launch_sw(st, tb, bytes_ok, tasks, 0, cnt, cnt, nullptr, d_q, d_t, p, res, dir, rows,
-                   tb ? d_cigar : nullptr, cig_off, band, err))
+                   tb ? d_cigar : nullptr, cig_off, band, fb, err))
       return DNALN_ERR_DEVICE;
     k_na_finish<<<blocks, 128, 0, st>>>(b, cnt, res, tb ? cigar_stride : 0, tb, d_out, d_cigar);
     if (cudaGetLastError() != cudaSuccess) return DNALN_ERR_CUDA;

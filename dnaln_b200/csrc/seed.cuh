@@ -14,9 +14,21 @@ struct DevIndex {
   const uint8_t* genome;
   const uint64_t* contig_off;
   const uint32_t* contig_len;
+  const uint2* n_runs;  // maximal runs of non-ACGT codes, [x, y), sorted
   uint64_t mask;
-  int32_t n_contigs, k, w;
+  int32_t n_contigs, k, w, n_n_runs;
 };
+
+// True when genome[a, b) holds a non-ACGT code (binary search over the N runs).
+__device__ __forceinline__ bool genome_has_n(const DevIndex& ix, int64_t a, int64_t b) {
+  int lo = 0, hi = ix.n_n_runs;  // first run with end > a
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (static_cast<int64_t>(ix.n_runs[mid].y) <= a) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < ix.n_n_runs && static_cast<int64_t>(ix.n_runs[lo].x) < b;
+}
 
 struct SeedParams {
   int32_t k, w;

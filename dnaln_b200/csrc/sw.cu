@@ -9,27 +9,34 @@
 // with H = E = 0 for row -1 and for the fixed out-of-band cell d = W, F = H(left) = 0 at
 // each row start, and the target N-padded to qlen + W - 1.
 //
-// Kernels (inter-sequence: every thread owns whole alignments, no intra-row shuffles):
-//  * k_sw_x2<W>: two alignments per thread, one in each 16-bit half of 32-bit registers,
-//    the band row (H, E of W+1 cells, W target selectors) in registers. Each cell is a
-//    handful of Blackwell DPX instructions: __viaddmax_s16x2 for the adds,
-//    __vibmax_s16x2 for the maxima — which also yields, per half, the predicate a >= b
-//    the traceback needs, so direction bits come with the max — and
-//    __vimax_s16x2_relu for H. The substitution score of both alignments is one
-//    prmt.b32 from an 8-byte per-row profile {s(qA,A..T), s(qB,A..T)}. 16-bit scores are
-//    exact while match * qlen stays far from 32767 (checked per pair).
-//  * A pair whose target window contains an N (or is too long for 16 bits) runs the
-//    int32 form of the same cell update, one alignment after the other (sw_one_reg).
+// Kernels (inter-sequence: a thread owns whole alignments, no intra-row shuffles):
+//  * k_sw_u2<W>: two alignments per thread, one in each 16-bit half of 32-bit
+//    registers, the band row (H, E of W+1 cells, W target selectors) in registers.
+//    Values are kept biased by +16384, so every half stays positive and every add or
+//    subtract of the recurrence is one 32-bit integer add on both halves (no borrow can
+//    cross halves) — these run on the FMA pipe; maxima are unsigned 16x2 max
+//    (vmaxu2 / DPX vimax3_u16x2). The substitution scores of both alignments are one
+//    prmt.b32 from an 8-byte per-row profile {s(qA, A..T) + 64, s(qB, A..T) + 64}.
+//    Direction bits come from non-negative differences (hd vs max(hd, E), ...)
+//    saturated to 0/1 with vminu2 and combined with integer multiply-adds.
+//    With traceback it stores the direction codes and only the best cell; the walk is a
+//    separate kernel (k_sw_walk, one thread per alignment, few registers, full occupancy)
+//    so the DP kernel's register footprint does not carry the walk.
+//  * A task whose target window may contain an N (the 4-entry profile cannot score it),
+//    or whose scores or lengths do not fit the biased 16-bit range, is appended by
+//    k_sw_u2 to a device-side list; k_sw_fb runs the same cell update in int32 for the
+//    listed tasks (sw_one_reg), same outputs and codes. Genome windows that the task
+//    builder marked N-free (kTaskNoN) skip the per-task N scan.
 //  * k_sw_any: any band width and any scores (int32, band rows in per-warp scratch).
 //
-// Traceback: a 4-bit direction code per cell, packed 8 cells per word and stored
-// lane-interleaved (word (i, d/8) of 32 alignments is one 128-byte line). The code is
-//   bit 3: p1 = hd >= E     bit 2: p2 = max(hd, E) >= F
-//   bit 1: E(i,d) extends E(i-1,d+1) (ee > eo)     bit 0: F extends (fe > fo)
-// On every cell the walk reads, H is the positive value being traced, and there
-// "H from the diagonal" (h == hd in src/align.cpp:67) is p1 && p2 and "H from E"
-// (h == e) with no diagonal is !p1 && p2, so the walk (src/align.cpp:87-143) takes the
-// reference's steps. The best cell is the first strict maximum in row-major order.
+// Direction code of a cell (4 bits):
+//   bit 3: hd < E            bit 2: max(hd, E) < F
+//   bit 1: E extends E(i-1,d+1) (ee > eo)    bit 0: F extends F(i,d-1) (fe > fo)
+// On every cell the walk reads, H is the positive value being traced; there "H from the
+// diagonal" (h == hd, src/align.cpp:67) is bits 3,2 = 0,0, "H from E" with no diagonal
+// (h == e) is 1,0, and otherwise H came from F — so the walk (src/align.cpp:87-143)
+// takes the reference's steps. The best cell is the first strict maximum in row-major
+// order (per-row maximum with its first column, then strict across rows).
 #include "common.cuh"
 #include "sw.cuh"
 
@@ -38,7 +45,9 @@ namespace dnb {
 namespace {
 
 constexpr int kSwThreads = 128;
-constexpr uint32_t kP1 = 8u, kP2 = 4u, kExtE = 2u, kExtF = 1u;
+constexpr uint32_t kNotDiagE = 8u, kFromF = 4u, kExtE = 2u, kExtF = 1u;
+constexpr uint32_t kBias = 16384u, kBias2 = 0x40004000u, kOne2 = 0x00010001u;
+constexpr int kScoreBias = 64;  // profile bytes are score + 64, in [0, 127]
 
 // prmt.b32 in its default mode (the sign-replicate bit of each selector nibble is
 // honoured; the __byte_perm intrinsic uses only the low 3 bits of each nibble).
@@ -54,8 +63,9 @@ __device__ __forceinline__ uint32_t sel1(uint32_t c) {
   return c | (s << 4) | (s << 8) | (s << 12);
 }
 
-// Selector of two sign-extended 16-bit scores: alignment A's byte a (0..3) into the low
-// half, alignment B's byte 4 + b into the high half.
+// Selector of two zero-extended 16-bit values: byte a (0..3) of the low profile word into
+// the low half, byte b of the high word into the high half (the profile bytes are
+// below 128, so the sign-replicating nibbles give zero high bytes).
 __device__ __forceinline__ uint32_t sel2(uint32_t a, uint32_t b) {
   const uint32_t x = 4u + b;
   return a | ((a | 8u) << 4) | (x << 8) | ((x | 8u) << 12);
@@ -68,8 +78,8 @@ __device__ __forceinline__ uint32_t tcode(const uint8_t* __restrict__ tbase, con
   return c > 3 ? 4u : c;
 }
 
-// Profile word of query code qc: byte t = match if t == qc else -mismatch; an N query
-// row scores -ambig everywhere.
+// Profile word of query code qc for the int32 path: byte t = match if t == qc else
+// -mismatch; an N query row scores -ambig everywhere.
 __device__ __forceinline__ uint32_t prof_lo(const SwParams& p, uint32_t qc) {
   if (qc > 3) return p.prof_n;
   const uint32_t mm = (static_cast<uint32_t>(static_cast<uint8_t>(-p.mismatch))) * 0x01010101u;
@@ -77,12 +87,18 @@ __device__ __forceinline__ uint32_t prof_lo(const SwParams& p, uint32_t qc) {
   return (mm & ~(0xFFu << sh)) | (static_cast<uint32_t>(static_cast<uint8_t>(p.match)) << sh);
 }
 
-__device__ __forceinline__ uint32_t pack2(int v) { return (static_cast<uint32_t>(v) & 0xFFFFu) * 0x10001u; }
-__device__ __forceinline__ int lo16(uint32_t x) { return static_cast<int>(static_cast<int16_t>(x & 0xFFFFu)); }
-__device__ __forceinline__ int hi16(uint32_t x) { return static_cast<int>(static_cast<int16_t>(x >> 16)); }
+// The same profile biased by +64 (every byte in [0, 127]) for the 16-bit path.
+__device__ __forceinline__ uint32_t prof_biased(const SwParams& p, uint32_t qc) {
+  if (qc > 3) return static_cast<uint32_t>(kScoreBias - p.ambig) * 0x01010101u;
+  const uint32_t mm = static_cast<uint32_t>(kScoreBias - p.mismatch) * 0x01010101u;
+  const uint32_t sh = 8u * qc;
+  return (mm & ~(0xFFu << sh)) | (static_cast<uint32_t>(kScoreBias + p.match) << sh);
+}
 
-__device__ __forceinline__ uint32_t dir_code(bool p1, bool p2, bool e_not_ext, bool f_not_ext) {
-  return (p1 ? kP1 : 0u) | (p2 ? kP2 : 0u) | (e_not_ext ? 0u : kExtE) | (f_not_ext ? 0u : kExtF);
+__device__ __forceinline__ uint32_t pack2(uint32_t v) { return (v & 0xFFFFu) * 0x10001u; }
+
+__device__ __forceinline__ uint32_t dir_code32(bool hd_ge_e, bool m1_ge_f, bool e_not_ext, bool f_not_ext) {
+  return (hd_ge_e ? 0u : kNotDiagE) | (m1_ge_f ? 0u : kFromF) | (e_not_ext ? 0u : kExtE) | (f_not_ext ? 0u : kExtF);
 }
 
 struct CigarWriter {
@@ -108,25 +124,48 @@ struct CigarWriter {
   }
 };
 
-// Walks the direction codes back from (bi, bd) (src/align.cpp:87-143). `D` points at
-// this alignment's first word; word (i, w) is D[(i * WW + w) * stride]. CIGAR ops are
+// Direction codes of the pair layout: word (i, g), g < WQ = ceil(W/4), holds cells 4g..4g+3
+// of both alignments of a thread (A in the low 16 bits, B in the high 16), cell 4g+c at
+// bits 4*(3-c) of its half; the 32 pairs of a warp are interleaved word by word.
+struct PairCodes {
+  const uint32_t* D;  // this pair's first word
+  int WQ, half;
+  __device__ uint32_t operator()(int i, int d) const {
+    const uint32_t w = D[(static_cast<size_t>(i) * WQ + (d >> 2)) * 32];
+    return (w >> (16 * half + 4 * (3 - (d & 3)))) & 0xFu;
+  }
+};
+
+// Direction codes of the generic kernel: word (i, w), w < WW = ceil(W/8), holds cells
+// 8w..8w+7, cell 8w+c at bits 4c; 32 alignments of a warp interleaved word by word.
+struct NibbleCodes {
+  const uint32_t* D;
+  int WW;
+  __device__ uint32_t operator()(int i, int d) const {
+    return (D[(static_cast<size_t>(i) * WW + (d >> 3)) * 32] >> (4 * (d & 7))) & 0xFu;
+  }
+};
+
+// Walks the direction codes back from (bi, bd) (src/align.cpp:87-143). CIGAR ops are
 // written in walk order (last op first), adjacent equal ops merged as the reference's
-// push() does.
-__device__ void traceback(const uint32_t* __restrict__ D, int stride, int WW, int W, int bi, int bd, int best,
-                          const uint8_t* __restrict__ q, const uint8_t* __restrict__ tbase, const SwTask& tk,
-                          const SwParams& p, SwResult& r, uint32_t* __restrict__ cig, int cap,
-                          uint32_t* __restrict__ err) {
-  auto code = [&](int i, int d) -> uint32_t {
-    return (D[(static_cast<size_t>(i) * WW + (d >> 3)) * stride] >> (4 * (d & 7))) & 0xFu;
-  };
+// push() does. Guards flag, and never read, a cell outside the band.
+template <class Codes>
+__device__ void traceback(const Codes& code, int W, int bi, int bd, int best, const uint8_t* __restrict__ q,
+                          const uint8_t* __restrict__ tbase, const SwTask& tk, const SwParams& p, SwResult& r,
+                          uint32_t* __restrict__ cig, int cap, uint32_t* __restrict__ err) {
   CigarWriter cw{cig, cap, 0, 0xFu, 0};
   int i = bi, d = bd, v = best, nm = 0;
+  if (d < 0 || d >= W) {
+    atomicOr(err, kErrTracebackBounds);
+    i = -1;
+    v = 0;
+  }
   for (;;) {
     int run = 0;
     uint32_t x = 0;
     while (i >= 0 && v > 0) {
       x = code(i, d);
-      if ((x & (kP1 | kP2)) != (kP1 | kP2)) break;  // not from the diagonal
+      if (x & (kNotDiagE | kFromF)) break;  // not from the diagonal
       const int a = q[i];
       const int b = static_cast<int>(tcode(tbase, tk, static_cast<int64_t>(i) + d));
       v -= sub_score(p, a, b);
@@ -138,7 +177,7 @@ __device__ void traceback(const uint32_t* __restrict__ D, int stride, int WW, in
     if (i < 0 || v <= 0) break;
     run = 0;
     bool ext;
-    if (x & kP2) {  // from E, an insertion: E(i,d) <- (i-1, d+1)
+    if (!(x & kFromF)) {  // from E, an insertion: E(i,d) <- (i-1, d+1)
       do {
         if (i < 0 || d >= W) {
           atomicOr(err, kErrTracebackBounds);
@@ -177,13 +216,23 @@ done:
   r.n_ops = cw.n < cap ? cw.n : cap;
 }
 
-// One alignment, int32 scores, band row of compile-time width W in registers. D is this
-// alignment's direction-word base (words `stride` apart).
+
+// The DP kernels leave, for the walk, the best cell in the result: qb = its row, qe = its
+// column (the walk kernel then writes the final coordinates).
+__device__ __forceinline__ SwResult stash(int score, int bi, int bd) { return SwResult{score, bi, bd, 0, 0, 0, 0, 0}; }
+
+// Direction-code base of local task lt (pairs 2p, 2p+1 share words; 32 pairs per warp).
+__device__ __forceinline__ uint32_t* pair_base(uint32_t* dir, int lt, int rows_max, int WQ) {
+  const int pair = lt >> 1;
+  return dir + static_cast<size_t>(pair >> 5) * rows_max * WQ * 32 + (pair & 31);
+}
+
+// One alignment, int32 scores, band row of compile-time width W in registers; direction
+// codes into its half of the pair layout (DP = the pair's first word).
 template <int W, bool TB>
 __device__ SwResult sw_one_reg(const SwTask& tk, const uint8_t* __restrict__ qbase, const uint8_t* __restrict__ tbase,
-                               const SwParams& p, uint32_t* __restrict__ D, int stride, uint32_t* __restrict__ cig,
-                               const int64_t* __restrict__ cig_off, uint32_t* __restrict__ err) {
-  constexpr int WW = (W + 7) / 8;
+                               const SwParams& p, uint32_t* __restrict__ DP, int half) {
+  constexpr int WQ = (W + 3) / 4;
   const uint8_t* __restrict__ q = qbase + tk.q_off;
   const int ql = tk.qlen;
   int H[W + 1], E[W + 1];
@@ -199,32 +248,31 @@ __device__ SwResult sw_one_reg(const SwTask& tk, const uint8_t* __restrict__ qba
   for (int i = 0; i < ql; ++i) {
     const uint32_t qc = min(static_cast<uint32_t>(q[i]), 4u);
     const uint32_t plo = prof_lo(p, qc), phi = p.prof_n;
+    const uint32_t t_next = sel1(tcode(tbase, tk, static_cast<int64_t>(i) + W));
     int f = 0, hleft = 0, hdiag = H[0], rmax = 0, rd = -1;
     uint32_t dw = 0;
 #pragma unroll
     for (int d = 0; d < W; ++d) {
       const int hup = H[d + 1], eup = E[d + 1];
       const int hd = hdiag + static_cast<int>(prmt(plo, phi, T[d]));
-      bool pe, pf, p1, p2;
-      const int e = __vibmax_s32(hup - p.oe, eup - p.ge, &pe);
-      f = __vibmax_s32(hleft - p.oe, f - p.ge, &pf);
-      const int m1 = __vibmax_s32(hd, e, &p1);
-      const int h = __vimax_s32_relu(__vibmax_s32(m1, f, &p2), 0);
+      const int eo = hup - p.oe, ee = eup - p.ge, fo = hleft - p.oe, fe = f - p.ge;
+      const int e = max(eo, ee);
+      f = max(fo, fe);
+      const int m1 = max(hd, e);
+      const int h = max(max(m1, f), 0);
       H[d] = h;
       E[d] = e;
       if constexpr (TB) {
-        dw |= dir_code(p1, p2, pe, pf) << (4 * (d & 7));
-        if ((d & 7) == 7 || d == W - 1) {
-          D[(static_cast<size_t>(i) * WW + (d >> 3)) * stride] = dw;
+        dw = dw * 16u + dir_code32(hd >= e, m1 >= f, eo >= ee, fo >= fe);
+        if ((d & 3) == 3 || d == W - 1) {
+          if ((d & 3) != 3) dw <<= 4 * (3 - (d & 3));
+          reinterpret_cast<uint16_t*>(DP + (static_cast<size_t>(i) * WQ + (d >> 2)) * 32)[half] =
+              static_cast<uint16_t>(dw);
           dw = 0;
         }
-        if (d == 0) {  // the row's first cell starts its running maximum (every H >= 0)
+        if (d == 0 || h > rmax) {  // first strict maximum of the row (every H >= 0)
           rmax = h;
-          rd = 0;
-        } else {
-          bool pr;
-          rmax = __vibmax_s32(rmax, h, &pr);
-          if (!pr) rd = d;  // strictly above the row's running max: first occurrence wins
+          rd = d;
         }
       } else {
         best = max(best, h);
@@ -239,52 +287,50 @@ __device__ SwResult sw_one_reg(const SwTask& tk, const uint8_t* __restrict__ qba
     }
 #pragma unroll
     for (int d = 0; d + 1 < W; ++d) T[d] = T[d + 1];
-    T[W - 1] = sel1(tcode(tbase, tk, static_cast<int64_t>(i) + W));
+    T[W - 1] = t_next;
   }
-  SwResult r{best, 0, 0, 0, 0, 0, 0, 0};
-  if (TB && best > 0) traceback(D, stride, WW, W, bi, bd, best, q, tbase, tk, p, r, cig + cig_off[tk.slot], 2 * ql + 1, err);
-  return r;
+  return TB ? stash(best, bi, bd) : stash(best, 0, 0);
 }
 
 // True if the target window [0, qlen + W - 1) of the task reads any N, including the
 // padding outside the candidate's contig or past a short target.
 __device__ bool window_has_n(const SwTask& tk, int W, const uint8_t* __restrict__ tbase) {
+  if (tk.flags & kTaskNoN) return false;
   const int64_t tmax = static_cast<int64_t>(tk.qlen) + W - 1;
   if (tk.t_lo > tk.t_start || tk.t_hi < tk.t_start + tmax) return true;
   const uint8_t* t = tbase + tk.t_start;
-  for (int64_t j = 0; j < tmax; ++j)
-    if (__ldg(t + j) > 3) return true;
-  return false;
+  bool any = false;
+  for (int64_t j = 0; j < tmax; ++j) any |= __ldg(t + j) > 3;
+  return any;
 }
 
-// Two alignments per thread in 16-bit halves (A low, B high).
+// Two alignments per thread in biased 16-bit halves (A low, B high). Pairs it cannot take
+// (an N in a target window, or scores/lengths outside the 16-bit range) are listed in
+// fb (fb[0] = count, then local task indices) for k_sw_fb.
 template <int W, bool TB>
-__global__ void __launch_bounds__(kSwThreads) k_sw_x2(const SwTask* __restrict__ tasks, int base, int n,
+__global__ void __launch_bounds__(kSwThreads) k_sw_u2(const SwTask* __restrict__ tasks, int base, int n,
                                                       const int* __restrict__ n_dev, const uint8_t* __restrict__ qbase,
                                                       const uint8_t* __restrict__ tbase, SwParams p,
                                                       SwResult* __restrict__ res, uint32_t* __restrict__ dir,
-                                                      int rows_max, uint32_t* __restrict__ cig,
-                                                      const int64_t* __restrict__ cig_off,
-                                                      uint32_t* __restrict__ err) {
-  constexpr int WW = (W + 7) / 8;
+                                                      int rows_max, int* __restrict__ fb) {
+  constexpr int WQ = (W + 3) / 4;
   const int lt = blockIdx.x * blockDim.x + threadIdx.x;  // pair index within this launch
   const int nn = n_dev ? min(n, *n_dev) : n;
   const int ia = base + 2 * lt, ib = ia + 1;
   if (ia >= nn) return;
   const bool has_b = ib < nn;
-  const int lane = threadIdx.x & 31;
-  // direction words: 64 alignments per warp, word (i, w) = [32 A lanes][32 B lanes]
-  uint32_t* DA = TB ? dir + static_cast<size_t>(lt >> 5) * rows_max * WW * 64 + lane : nullptr;
-  uint32_t* DB = TB ? DA + 32 : nullptr;
+  uint32_t* DP = TB ? pair_base(dir, 2 * lt, rows_max, WQ) : nullptr;
   const SwTask ta = tasks[ia];
   SwTask tb = ta;
   if (has_b) tb = tasks[ib];
   else tb.qlen = 0;
   const int qmax = max(ta.qlen, tb.qlen);
-  const bool fits16 = qmax * p.match + 2 * (p.oe + p.ge + p.mismatch + p.ambig) < 30000;
-  if (!fits16 || window_has_n(ta, W, tbase) || (has_b && window_has_n(tb, W, tbase))) {
-    res[ta.slot] = sw_one_reg<W, TB>(ta, qbase, tbase, p, DA, 64, cig, cig_off, err);
-    if (has_b) res[tb.slot] = sw_one_reg<W, TB>(tb, qbase, tbase, p, DB, 64, cig, cig_off, err);
+  const bool fits = qmax * p.match + 2 * (p.oe + p.ge + p.mismatch + p.ambig) < 16000 &&
+                    p.match + kScoreBias <= 127 && p.mismatch <= kScoreBias && p.ambig <= kScoreBias;
+  if (!fits || window_has_n(ta, W, tbase) || (has_b && window_has_n(tb, W, tbase))) {
+    const int k = atomicAdd(fb, has_b ? 2 : 1);
+    fb[1 + k] = 2 * lt;
+    if (has_b) fb[2 + k] = 2 * lt + 1;
     return;
   }
   const uint8_t* __restrict__ qa = qbase + ta.q_off;
@@ -295,96 +341,136 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_x2(const SwTask* __restrict__
     const uint32_t a = tcode(tbase, ta, j), b = has_b ? tcode(tbase, tb, j) : 0u;
     return sel2(a > 3 ? 0u : a, b > 3 ? 0u : b);
   };
+  auto qcode = [&](const uint8_t* __restrict__ q, int ql, int i) {
+    return i < ql ? min(static_cast<uint32_t>(q[i]), 4u) : 4u;
+  };
   uint32_t H[W + 1], E[W + 1], T[W];
 #pragma unroll
   for (int d = 0; d <= W; ++d) {
-    H[d] = 0;
-    E[d] = 0;
+    H[d] = kBias2;
+    E[d] = kBias2;
   }
 #pragma unroll
   for (int d = 0; d < W; ++d) T[d] = tc2(d);
-  const uint32_t NOE = pack2(-p.oe), NGE = pack2(-p.ge), NEG = 0x80008000u;
-  uint32_t best2 = 0;
-  int best_a = 0, bi_a = -1, bd_a = -1, best_b = 0, bi_b = -1, bd_b = -1;
+  const uint32_t OE = pack2(p.oe), GE = pack2(p.ge), SB = pack2(kScoreBias);
+  uint32_t best2 = kBias2;
+  uint32_t best_a = kBias, best_b = kBias;
+  int bi_a = -1, bd_a = -1, bi_b = -1, bd_b = -1;
+  uint32_t ca = qcode(qa, qla, 0), cb = qcode(qb, qlb, 0);
   for (int i = 0; i < qmax; ++i) {
-    // rows past a query's end are N rows for it: they cannot raise its best (src of the
-    // values only decreases) and its walk never reaches them
-    const uint32_t ca = i < qla ? min(static_cast<uint32_t>(qa[i]), 4u) : 4u;
-    const uint32_t cb = i < qlb ? min(static_cast<uint32_t>(qb[i]), 4u) : 4u;
-    const uint32_t plo = prof_lo(p, ca), phi = prof_lo(p, cb);
-    uint32_t f = 0, hleft = 0, hdiag = H[0], rmax = 0, dwa = 0, dwb = 0;
-    int rda = -1, rdb = -1;
+    // rows past a query's end are N rows for it: they cannot raise its best (values only
+    // decrease) and its walk never reaches them. Next row's codes are loaded up front so
+    // their latency hides behind this row.
+    const uint32_t plo = prof_biased(p, ca), phi = prof_biased(p, cb);
+    const uint32_t t_next = tc2(static_cast<int64_t>(i) + W);
+    const uint32_t ca_next = qcode(qa, qla, i + 1), cb_next = qcode(qb, qlb, i + 1);
+    uint32_t f = kBias2, hleft = kBias2, hdiag = H[0], rmax = 0, dw = 0;
+    int rda = 0, rdb = 0;
 #pragma unroll
     for (int d = 0; d < W; ++d) {
       const uint32_t hup = H[d + 1], eup = E[d + 1];
-      const uint32_t hd = __viaddmax_s16x2(hdiag, prmt(plo, phi, T[d]), NEG);
-      bool peh, pel, pfh, pfl, p1h, p1l, p2h, p2l;
-      const uint32_t e = __vibmax_s16x2(__viaddmax_s16x2(hup, NOE, NEG), __viaddmax_s16x2(eup, NGE, NEG), &peh, &pel);
-      f = __vibmax_s16x2(__viaddmax_s16x2(hleft, NOE, NEG), __viaddmax_s16x2(f, NGE, NEG), &pfh, &pfl);
-      const uint32_t m1 = __vibmax_s16x2(hd, e, &p1h, &p1l);
-      const uint32_t h = __vimax_s16x2_relu(__vibmax_s16x2(m1, f, &p2h, &p2l), 0u);
+      const uint32_t hd = hdiag + prmt(plo, phi, T[d]) - SB;
+      const uint32_t eo = hup - OE, ee = eup - GE, fo = hleft - OE, fe = f - GE;
+      const uint32_t e = __vmaxu2(eo, ee);
+      f = __vmaxu2(fo, fe);
+      const uint32_t m1 = __vmaxu2(hd, e);
+      const uint32_t h = __vimax3_u16x2(m1, f, kBias2);
       H[d] = h;
       E[d] = e;
       if constexpr (TB) {
-        dwa |= dir_code(p1l, p2l, pel, pfl) << (4 * (d & 7));
-        dwb |= dir_code(p1h, p2h, peh, pfh) << (4 * (d & 7));
-        if ((d & 7) == 7 || d == W - 1) {
-          const size_t o = (static_cast<size_t>(i) * WW + (d >> 3)) * 64;
-          DA[o] = dwa;
-          DB[o] = dwb;
-          dwa = dwb = 0;
+        // each difference is >= 0 per half; saturated to 0/1 it is one code bit
+        const uint32_t c = ((__vminu2(m1 - hd, kOne2) * 2u + __vminu2(h - m1, kOne2)) * 2u +
+                            __vminu2(e - eo, kOne2)) * 2u + __vminu2(f - fo, kOne2);
+        dw = dw * 16u + c;
+        if ((d & 3) == 3 || d == W - 1) {
+          if ((d & 3) != 3) dw <<= 4 * (3 - (d & 3));
+          DP[(static_cast<size_t>(i) * WQ + (d >> 2)) * 32] = dw;
+          dw = 0;
         }
-        // row maximum, first strict occurrence; the row starts at cell 0 (every H >= 0,
-        // so cell 0 is the first maximum of the cells seen so far)
         if (d == 0) {
           rmax = h;
-          rda = rdb = 0;
-        } else {
-          bool rh, rl;
-          rmax = __vibmax_s16x2(rmax, h, &rh, &rl);
-          if (!rl) rda = d;
-          if (!rh) rdb = d;
+        } else {  // first strict maximum of the row, per half
+          const uint32_t nm = __vmaxu2(rmax, h);
+          const uint32_t up = nm ^ rmax;  // nonzero half where h beat the row maximum
+          rda = (up & 0xFFFFu) ? d : rda;
+          rdb = (up >> 16) ? d : rdb;
+          rmax = nm;
         }
       } else {
-        best2 = __vimax_s16x2_relu(best2, h);
+        best2 = __vmaxu2(best2, h);
       }
       hleft = h;
       hdiag = hup;
     }
     if constexpr (TB) {
-      if (lo16(rmax) > best_a) {
-        best_a = lo16(rmax);
+      if ((rmax & 0xFFFFu) > best_a) {
+        best_a = rmax & 0xFFFFu;
         bi_a = i;
         bd_a = rda;
       }
-      if (hi16(rmax) > best_b) {
-        best_b = hi16(rmax);
+      if ((rmax >> 16) > best_b) {
+        best_b = rmax >> 16;
         bi_b = i;
         bd_b = rdb;
       }
     }
 #pragma unroll
     for (int d = 0; d + 1 < W; ++d) T[d] = T[d + 1];
-    T[W - 1] = tc2(static_cast<int64_t>(i) + W);
+    T[W - 1] = t_next;
+    ca = ca_next;
+    cb = cb_next;
   }
   if constexpr (!TB) {
-    best_a = lo16(best2);
-    best_b = hi16(best2);
+    best_a = best2 & 0xFFFFu;
+    best_b = best2 >> 16;
   }
-  SwResult ra{best_a, 0, 0, 0, 0, 0, 0, 0};
-  if (TB && best_a > 0)
-    traceback(DA, 64, WW, W, bi_a, bd_a, best_a, qa, tbase, ta, p, ra, cig + cig_off[ta.slot], 2 * qla + 1, err);
-  res[ta.slot] = ra;
-  if (has_b) {
-    SwResult rb{best_b, 0, 0, 0, 0, 0, 0, 0};
-    if (TB && best_b > 0)
-      traceback(DB, 64, WW, W, bi_b, bd_b, best_b, qb, tbase, tb, p, rb, cig + cig_off[tb.slot], 2 * qlb + 1, err);
-    res[tb.slot] = rb;
+  res[ta.slot] = stash(static_cast<int>(best_a) - static_cast<int>(kBias), TB ? bi_a : 0, TB ? bd_a : 0);
+  if (has_b) res[tb.slot] = stash(static_cast<int>(best_b) - static_cast<int>(kBias), TB ? bi_b : 0, TB ? bd_b : 0);
+}
+
+// The pairs k_sw_u2 listed, one alignment per thread, int32.
+template <int W, bool TB>
+__global__ void __launch_bounds__(kSwThreads) k_sw_fb(const SwTask* __restrict__ tasks, int base,
+                                                      const uint8_t* __restrict__ qbase,
+                                                      const uint8_t* __restrict__ tbase, SwParams p,
+                                                      SwResult* __restrict__ res, uint32_t* __restrict__ dir,
+                                                      int rows_max, const int* __restrict__ fb) {
+  constexpr int WQ = (W + 3) / 4;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= fb[0]) return;
+  const int lt = fb[1 + j];
+  const SwTask tk = tasks[base + lt];
+  res[tk.slot] = sw_one_reg<W, TB>(tk, qbase, tbase, p, TB ? pair_base(dir, lt, rows_max, WQ) : nullptr, lt & 1);
+}
+
+// Traceback of every task of the launch from the stashed best cell (one task per thread;
+// the DP kernels are done with the scratch, so this runs at full occupancy).
+template <int W>
+__global__ void __launch_bounds__(kSwThreads) k_sw_walk(const SwTask* __restrict__ tasks, int base, int count, int n,
+                                                        const int* __restrict__ n_dev,
+                                                        const uint8_t* __restrict__ qbase,
+                                                        const uint8_t* __restrict__ tbase, SwParams p,
+                                                        SwResult* __restrict__ res, const uint32_t* __restrict__ dir,
+                                                        int rows_max, uint32_t* __restrict__ cig,
+                                                        const int64_t* __restrict__ cig_off,
+                                                        uint32_t* __restrict__ err) {
+  constexpr int WQ = (W + 3) / 4;
+  const int lt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nn = n_dev ? min(n, *n_dev) : n;
+  if (lt >= count || base + lt >= nn) return;
+  const SwTask tk = tasks[base + lt];
+  const SwResult s = res[tk.slot];
+  SwResult r{s.score, 0, 0, 0, 0, 0, 0, 0};
+  if (s.score > 0) {
+    const PairCodes codes{pair_base(const_cast<uint32_t*>(dir), lt, rows_max, WQ), WQ, lt & 1};
+    traceback(codes, W, s.qb, s.qe, s.score, qbase + tk.q_off, tbase, tk, p, r, cig + cig_off[tk.slot],
+              2 * tk.qlen + 1, err);
   }
+  res[tk.slot] = r;
 }
 
 // Any band width and any scores: one alignment per thread, int32, band rows H, E in
-// per-warp scratch, lane-interleaved ([d][lane]).
+// per-warp scratch, lane-interleaved ([d][lane]); walks its own traceback.
 template <bool TB>
 __global__ void __launch_bounds__(kSwThreads) k_sw_any(const SwTask* __restrict__ tasks, int base, int n,
                                                        const int* __restrict__ n_dev,
@@ -418,22 +504,23 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_any(const SwTask* __restrict_
       const int hup = Hs[(d + 1) * 32], eup = Es[(d + 1) * 32];
       const int tc = static_cast<int>(tcode(tbase, tk, static_cast<int64_t>(i) + d));
       const int hd = hdiag + sub_score(p, qc, tc);
-      bool pe, pf, p1, p2;
-      const int e = __vibmax_s32(hup - p.oe, eup - p.ge, &pe);
-      f = __vibmax_s32(hleft - p.oe, f - p.ge, &pf);
-      const int m1 = __vibmax_s32(hd, e, &p1);
-      const int h = __vimax_s32_relu(__vibmax_s32(m1, f, &p2), 0);
+      const int eo = hup - p.oe, ee = eup - p.ge, fo = hleft - p.oe, fe = f - p.ge;
+      const int e = max(eo, ee);
+      f = max(fo, fe);
+      const int m1 = max(hd, e);
+      const int h = max(max(m1, f), 0);
       Hs[d * 32] = h;
       Es[d * 32] = e;
       if (TB) {
-        dw |= dir_code(p1, p2, pe, pf) << (4 * (d & 7));
+        dw |= dir_code32(hd >= e, m1 >= f, eo >= ee, fo >= fe) << (4 * (d & 7));
         if ((d & 7) == 7 || d == W - 1) {
           D[(static_cast<size_t>(i) * WW + (d >> 3)) * 32] = dw;
           dw = 0;
         }
-        bool pr;
-        rmax = __vibmax_s32(rmax, h, &pr);
-        if (!pr) rd = d;
+        if (d == 0 || h > rmax) {
+          rmax = h;
+          rd = d;
+        }
       } else {
         best = max(best, h);
       }
@@ -448,22 +535,29 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_any(const SwTask* __restrict_
   }
   SwResult r{best, 0, 0, 0, 0, 0, 0, 0};
   if (TB && best > 0)
-    traceback(D, 32, WW, W, bi, bd, best, q, tbase, tk, p, r, cig + cig_off[tk.slot], 2 * ql + 1, err);
+    traceback(NibbleCodes{D, WW}, W, bi, bd, best, q, tbase, tk, p, r, cig + cig_off[tk.slot], 2 * ql + 1, err);
   res[tk.slot] = r;
 }
 
 template <int W>
-void launch_x2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int count, int n, const int* n_dev,
+void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int count, int n, const int* n_dev,
                const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res, uint32_t* dir,
-               int rows_max, uint32_t* cig, const int64_t* cig_off, uint32_t* err) {
+               int rows_max, uint32_t* cig, const int64_t* cig_off, int* fb, uint32_t* err) {
   const int pairs = (count + 1) / 2;
-  const int blocks = (pairs + kSwThreads - 1) / kSwThreads;
-  if (tb)
-    k_sw_x2<W, true><<<blocks, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig,
-                                                    cig_off, err);
-  else
-    k_sw_x2<W, false><<<blocks, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig,
-                                                     cig_off, err);
+  const int blocks_pairs = (pairs + kSwThreads - 1) / kSwThreads;
+  const int blocks_tasks = (count + kSwThreads - 1) / kSwThreads;
+  cudaMemsetAsync(fb, 0, sizeof(int), st);
+  if (tb) {
+    k_sw_u2<W, true><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max,
+                                                          fb);
+    k_sw_fb<W, true><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    k_sw_walk<W><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, count, n, n_dev, qbase, tbase, p, res, dir,
+                                                      rows_max, cig, cig_off, err);
+  } else {
+    k_sw_u2<W, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max,
+                                                           fb);
+    k_sw_fb<W, false><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+  }
 }
 
 }  // namespace
@@ -490,33 +584,38 @@ SwParams make_sw_params(const dnaln_score_params& s) {
 }
 
 size_t sw_dir_bytes_per_task(int W, int rows_max) {
-  return static_cast<size_t>(rows_max > 0 ? rows_max : 1) * ((W + 7) / 8) * sizeof(uint32_t);
+  const size_t pair = static_cast<size_t>((W + 3) / 4) * 2, nib = static_cast<size_t>((W + 7) / 8) * 4;
+  return static_cast<size_t>(rows_max > 0 ? rows_max : 1) * (pair > nib ? pair : nib);
 }
 
 size_t sw_band_bytes_per_task(int W, bool bytes_ok) {
   return sw_uses_generic(W, bytes_ok) ? static_cast<size_t>(2) * (W + 1) * sizeof(int) : 0;
 }
 
+int sw_launches(int W, bool bytes_ok, bool tb) { return sw_uses_generic(W, bytes_ok) ? 1 : (tb ? 3 : 2); }
+
 bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int base, int count, int n,
                const int* n_dev, const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res,
-               uint32_t* dir, int rows_max, uint32_t* cig, const int64_t* cig_off, int* band, uint32_t* err) {
+               uint32_t* dir, int rows_max, uint32_t* cig, const int64_t* cig_off, int* band, int* fb,
+               uint32_t* err) {
   if (count <= 0) return true;
-  if ((tb && !dir) || (sw_uses_generic(p.W, bytes_ok) && !band) || (base % kSwTaskGroup) != 0) return false;
-  if (bytes_ok) {
-#define DNB_SW_X2(WV)                                                                                       \
+  const bool generic = sw_uses_generic(p.W, bytes_ok);
+  if ((tb && !dir) || (generic && !band) || (!generic && !fb) || (base % kSwTaskGroup) != 0) return false;
+  if (!generic) {
+#define DNB_SW_U2(WV)                                                                                       \
   case WV:                                                                                                  \
-    launch_x2<WV>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, \
-                  err);                                                                                     \
+    launch_u2<WV>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, \
+                  fb, err);                                                                                 \
     return true;
     switch (p.W) {
-      DNB_SW_X2(11)
-      DNB_SW_X2(17)
-      DNB_SW_X2(33)
-      DNB_SW_X2(43)
-      DNB_SW_X2(65)
+      DNB_SW_U2(11)
+      DNB_SW_U2(17)
+      DNB_SW_U2(33)
+      DNB_SW_U2(43)
+      DNB_SW_U2(65)
       default: break;
     }
-#undef DNB_SW_X2
+#undef DNB_SW_U2
   }
   const int blocks = (count + kSwThreads - 1) / kSwThreads;
   if (tb)
