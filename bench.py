@@ -36,6 +36,7 @@ sys.path.insert(0, str(ROOT))
 WORKLOAD = "ecoli-4.6Mbp-1M-150bp"
 BATCH = 262_144
 METRIC = "reads/s"
+PROFILE_STEPS = 2  # untimed steps whose every kernel launch is timed (the per-kernel breakdown)
 
 
 def parse():
@@ -114,23 +115,29 @@ def measured_peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def stage_bytes(stage: str, st: dict, reads_per_step: float, mean_len: float, bw: int = 16) -> float:
-    """Algorithmic HBM bytes of one step for each pipeline stage (definitions in DESIGN.md)."""
-    n = reads_per_step
-    mins = st.get("minimizers_per_read", 0.18 * mean_len) * n
-    anchors = st["anchors"]
+TASK_BYTES = 48 + 32  # SW task descriptor in, result out
+
+
+def kernel_bytes(kernel: str, st: dict, mean_len: float, bw: int = 16) -> float | None:
+    """Algorithmic HBM bytes of all launches of one kernel, from the batch counters in st
+    (reads, minimizers, anchors, candidates, SW tasks). None for kernels not modelled."""
+    n = st["reads"]
+    mins = st["minimizers"] if st.get("minimizers") else 0.18 * mean_len * n
     W = 2 * bw + 1
-    if stage == "seed":      # ASCII in, codes out (both strands), minimizers + probe results out, one bucket per probe
-        return n * mean_len * (1 + 2) + mins * (16 + 8 + 16) + n * 12
-    if stage == "chain":     # minimizers + probe results in, occurrence positions in, candidates out
-        return mins * 24 + anchors * 4 + st["candidates"] * 28 + n * 4
-    if stage == "sw_tb":     # query + target window in, direction nibbles written once, result out
-        tasks = st["sw_tasks_tb"]
-        return tasks * (mean_len + (mean_len + 2 * bw) + mean_len * ((W + 7) // 8) * 4 + 32)
-    if stage == "sw_score":
-        tasks = st["sw_tasks_score"]
-        return tasks * (mean_len + (mean_len + 2 * bw) + 32)
-    return n * (40 + 16)     # post: records + CIGARs out
+    if kernel == "k_seed":        # ASCII in, codes of both strands out, 20-B minimizer slot out + 16-B bucket
+        return n * mean_len * (1 + 2) + mins * (20 + 16) + n * 24
+    if kernel == "k_chain_map":   # minimizer slots in, 4-B occurrence per anchor, 21-B candidate out
+        return mins * 20 + st["anchors"] * 4 + st["candidates"] * 21 + n * 28
+    if kernel == "k_sw_u2<tb>":   # query + window in, direction words out (W/4 words of 2 B per row), task/result
+        t = st["sw_tasks_tb"]
+        return t * (mean_len + (mean_len + 2 * bw) + mean_len * ((W + 3) // 4) * 2 + TASK_BYTES)
+    if kernel == "k_sw_u2<score>":
+        t = st["sw_tasks_score"]
+        return t * (mean_len + (mean_len + 2 * bw) + TASK_BYTES)
+    if kernel == "k_sw_walk":     # one direction word per step (~len steps), query/window bytes on the path, CIGAR
+        t = st["sw_tasks_tb"]
+        return t * (mean_len * (4 + 2) + 16 + TASK_BYTES)
+    return None
 
 
 def cpu_baseline(g, reads, params) -> dict:
@@ -277,8 +284,18 @@ def run_ours(args) -> None:
 
     for _ in range(max(args.warmup, 3)):
         step_device()
+    # kernel breakdown: every launch of PROFILE_STEPS untimed steps bracketed by event pairs
     barrier()
     ctx.reset_stats()
+    ctx.set_kernel_trace(True)
+    for _ in range(PROFILE_STEPS):
+        step_device()
+    barrier()
+    breakdown = ctx.kernel_times()
+    dom = max(breakdown, key=lambda k: breakdown[k][1])
+    # timed region: only the dominant kernel's launches carry event pairs (one per batch)
+    ctx.reset_stats()
+    ctx.set_kernel_trace(True, only=dom)
     clocks = ClockSampler(local)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -290,6 +307,8 @@ def run_ours(args) -> None:
     clk = clocks.result()
     ms = max_over_ranks(e0.elapsed_time(e1))
     st = ctx.stats()
+    ktimes = ctx.kernel_times()
+    ctx.set_kernel_trace(False)
     value = world * n_reads * args.steps / (ms / 1e3)
 
     # ---- end to end through the host-buffer C call (e2e) ----------------------------
@@ -333,19 +352,17 @@ def run_ours(args) -> None:
     h2d = sum(h["h2d"] for h in host)
     d2h = sum(40 * h["n"] for h in host) + 4 * sum(e2e_used)
 
-    # ---- roofline of the dominant stage ---------------------------------------------
+    # ---- roofline of the dominant kernel ----------------------------------------------
     stage_ms = {"seed": st["ms_seed"], "chain": st["ms_chain"], "sw_score": st["ms_sw_score"], "sw_tb": st["ms_sw_tb"],
                 "post": st["ms_post"]}
-    dom = max(stage_ms, key=stage_ms.get)
-    per_step = {k: v / args.steps for k, v in st.items() if isinstance(v, (int, float))}
     mean_len = float(np.mean(reads.seq_len))
-    launches_per_step = len(parts)  # one launch of the dominant stage's kernel per batch
-    bytes_step = stage_bytes(dom, per_step, n_reads, mean_len)
-    avg_launch_ms = stage_ms[dom] / (args.steps * launches_per_step)
-    achieved = (bytes_step / launches_per_step) / (avg_launch_ms / 1e3) / 1e9
+    launches, dom_ms = ktimes[dom]
+    avg_launch_ms = dom_ms / launches
+    algo = kernel_bytes(dom, st, mean_len)
     peak, peak_kind = measured_peaks()
+    achieved = (algo / launches) / (avg_launch_ms / 1e3) / 1e9 if algo is not None else None
     traffic = None
-    tf = ROOT / "profiles" / f"traffic_{dom}.json"
+    tf = ROOT / "profiles" / f"traffic_{dom.split('<')[0]}.json"
     if tf.exists():
         try:
             traffic = json.loads(tf.read_text()).get("bytes_per_launch")
@@ -353,6 +370,11 @@ def run_ours(args) -> None:
             traffic = None
     cells = st["cells"]
     sw_ms = st["ms_sw_score"] + st["ms_sw_tb"]
+    kernels = {k: {"launches_per_step": n / PROFILE_STEPS, "ms_per_step": t / PROFILE_STEPS}
+               for k, (n, t) in sorted(breakdown.items(), key=lambda kv: -kv[1][1])}
+    kernels_total = sum(v["ms_per_step"] for v in kernels.values())
+    for v in kernels.values():
+        v["share"] = v["ms_per_step"] / kernels_total
 
     out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -362,9 +384,11 @@ def run_ours(args) -> None:
                    "ms_per_step": ms_e2e / e2e_steps, "wall_s": wall_e2e},
            "gpu_launches": int(st["launches"]),
            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                        "algorithmic_bytes_per_launch": bytes_step / launches_per_step,
-                        "avg_launch_ms": avg_launch_ms},
+                        "frac": achieved / peak if achieved is not None else None, "traffic": traffic,
+                        "peak_kind": peak_kind,
+                        "algorithmic_bytes_per_launch": algo / launches if algo is not None else None,
+                        "avg_launch_ms": avg_launch_ms, "launches_timed": launches},
+           "kernels": kernels, "kernels_note": f"untimed breakdown over {PROFILE_STEPS} steps, every launch traced",
            "stages_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
            "sw_gcups": cells / (sw_ms / 1e3) / 1e9 if sw_ms > 0 else None,
            "sw_cells_per_step": cells / args.steps,

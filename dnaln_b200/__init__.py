@@ -221,6 +221,28 @@ class Context:
     def reset_stats(self) -> None:
         self._check(self._lib.dnaln_gpu_reset_stats(self._h))
 
+    def set_kernel_trace(self, on: bool, only: str | None = None) -> None:
+        """Times every kernel launch (or only those of kernel `only`) with a CUDA event pair
+        on its stream."""
+        self._check(self._lib.dnaln_gpu_set_kernel_trace(self._h, 1 if on else 0,
+                                                         only.encode() if only else None))
+
+    def kernel_times(self) -> dict:
+        """{kernel name: (launches, total ms)} since the last reset_stats()."""
+        n = C.c_int32()
+        self._check(self._lib.dnaln_gpu_kernel_times(self._h, None, 0, C.byref(n)))
+        arr = (N.KernelTime * max(n.value, 1))()
+        self._check(self._lib.dnaln_gpu_kernel_times(self._h, arr, n.value, C.byref(n)))
+        return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].ms)) for i in range(n.value)}
+
+    def set_option(self, name: str, value: int) -> None:
+        """Tuning switch (sub_batch, warp_seed_only, dir_cap_bytes); results do not change."""
+        self._check(self._lib.dnaln_gpu_set_option(self._h, name.encode(), int(value)))
+
+    def set_sub_batch(self, reads: int) -> None:
+        """Reads per pipelined sub-batch of map_batch (0 = the whole batch at once)."""
+        self._check(self._lib.dnaln_gpu_set_sub_batch(self._h, int(reads)))
+
     # -- index --------------------------------------------------------------------------
     def index_build(self, g: Genome, k: int = 15, w: int = 10) -> int:
         iid = C.c_int32()
@@ -322,9 +344,9 @@ class Context:
         cig = np.zeros(max(cap, 1), np.uint32)
         used = C.c_int64()
         off = np.ascontiguousarray(reads.seq_off[:-1])
-        self._check(self._lib.dnaln_gpu_map_batch(self._h, iid, ptr(reads.seq), ptr(off), ptr(lens),
-                                                  ptr(reads.name_hash()), n, C.byref(p), ptr(rec), ptr(cig), cap,
-                                                  C.byref(used)))
+        nh = reads.name_hash()
+        self._check(self._lib.dnaln_gpu_map_batch(self._h, iid, ptr(reads.seq), ptr(off), ptr(lens), ptr(nh), n,
+                                                  C.byref(p), ptr(rec), ptr(cig), cap, C.byref(used)))
         return MapResult(rec[:n], cig[:used.value])
 
 

@@ -53,6 +53,10 @@ class Stats(C.Structure):
                                           "ms_d2h", "ms_total")] + [("launches", C.c_uint64)]
 
 
+class KernelTime(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("launches", C.c_int64), ("ms", C.c_double)]
+
+
 class SynthGenomeSpec(C.Structure):
     _fields_ = [("n_contigs", C.c_int32), ("contig_len", C.c_uint32), ("gc", C.c_double),
                 ("n_repeat_units", C.c_int32), ("repeat_unit_len", C.c_int32), ("repeat_frac", C.c_double),
@@ -88,6 +92,10 @@ SIGNATURES = {
     "dnaln_gpu_set_stream": (C.c_int, [P, P]),
     "dnaln_gpu_get_stats": (C.c_int, [P, C.POINTER(Stats)]),
     "dnaln_gpu_reset_stats": (C.c_int, [P]),
+    "dnaln_gpu_set_kernel_trace": (C.c_int, [P, i32, C.c_char_p]),
+    "dnaln_gpu_kernel_times": (C.c_int, [P, C.POINTER(KernelTime), i32, C.POINTER(i32)]),
+    "dnaln_gpu_set_sub_batch": (C.c_int, [P, i64]),
+    "dnaln_gpu_set_option": (C.c_int, [P, C.c_char_p, i64]),
     "dnaln_gpu_host_alloc": (C.c_int, [P, C.c_size_t, C.POINTER(P)]),
     "dnaln_gpu_host_free": (C.c_int, [P, P]),
     "dnaln_gpu_index_build": (C.c_int, [P, P, u64, P, P, i32, i32, i32, C.POINTER(i32)]),

@@ -12,7 +12,9 @@
 //   k_records: MAPQ, positions, soft clips; CIGAR offsets (scan)  [1 host read-back]
 //   k_cigar_gather: final CIGARs
 // Task counts produced on the device are consumed on the device (kernels read them), so
-// the host only waits where it must size a buffer.
+// the host only waits where it must size a buffer. The host-buffer entry point splits a
+// batch into sub-batches and overlaps their copies in and out with the compute (two
+// device slots, two copy streams); it knows the lengths, so it skips the first read-back.
 #include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -48,8 +50,22 @@ struct IndexRes {
   DevIndex dev{};
 };
 
-enum Ev { kEvSeed0, kEvSeed1, kEvChain0, kEvChain1, kEvSc0, kEvSc1, kEvTb0, kEvTb1, kEvPost0, kEvPost1, kEvH2d0,
-          kEvH2d1, kEvD2h0, kEvD2h1, kNumEv };
+enum Ev { kEvSeed0, kEvSeed1, kEvChain0, kEvChain1, kEvSc0, kEvSc1, kEvTb0, kEvTb1, kEvPost0, kEvPost1, kNumEv };
+
+constexpr int kMaxTrace = 256;  // traced launches per batch
+
+struct KernelTime {
+  int64_t launches = 0;
+  double ms = 0.0;
+};
+
+// Per-batch facts the caller may already know (host-buffer path), sparing a device read-back.
+struct BatchHints {
+  int64_t seq_base = 0;    // subtracted from every read offset (sub-batch staged on the device)
+  int64_t bases = -1;      // total bases of the batch, -1 = read back from the device
+  int64_t max_len = -1;    // longest read, -1 = read back from the device
+  int64_t cigar_base = 0;  // added to every record's cigar_off
+};
 
 }  // namespace
 
@@ -61,11 +77,27 @@ struct dnaln_ctx {
   int32_t next_id = 1;
   std::map<std::string, DevBuf> bufs;
   uint32_t* d_err = nullptr;   // kernel error flags
-  int* d_count = nullptr;      // [0] score tasks, [1] traceback tasks
+  int* d_count = nullptr;      // [0] score tasks, [1] traceback tasks, [2] reads listed for the warp path
   int64_t* h_info = nullptr;   // pinned read-back slots
   cudaEvent_t ev[kNumEv] = {};
   dnaln_stats stats{};
   size_t dir_cap_bytes = size_t(1) << 30;  // direction-bit scratch per traceback launch
+  // pipelined host-buffer path: copy streams, per-slot events, sub-batch size (reads)
+  cudaStream_t cp_in = nullptr, cp_out = nullptr;
+  cudaEvent_t in_ready[2] = {}, out_free[2] = {}, h2d_ev[4] = {}, d2h_ev[4] = {};
+  int64_t sub_batch = 65536;
+  bool warp_seed_only = false;  // option: every read through the warp-per-read seeding kernels
+  // kernel trace: event pairs of the current batch, totals per kernel name
+  bool trace_on = false, trace_open = false;
+  std::string trace_only;  // non-empty: trace only the kernel of this name
+  int trace_n = 0;
+  std::vector<cudaEvent_t> trace_ev;
+  const char* trace_name[kMaxTrace] = {};
+  std::map<std::string, KernelTime> ktimes;
+  // chaining gap-cost table on the device, for (lut_k, lut_band); re-uploaded on change
+  int lut_k = -1, lut_band = -1;
+  int32_t* h_lut = nullptr;  // page-locked staging of the table
+  size_t h_lut_cap = 0;
 };
 
 namespace {
@@ -120,21 +152,62 @@ int set_device(dnaln_ctx* c) {
   return DNALN_OK;
 }
 
-int exclusive_scan(dnaln_ctx* c, const int64_t* in, int64_t* out, int64_t n) {
-  size_t tmp = 0;
-  CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, c->st));
-  DBUF(t, uint8_t, "cub_tmp", tmp);
-  CK(cub::DeviceScan::ExclusiveSum(t, tmp, in, out, n, c->st));
-  return DNALN_OK;
-}
+int exclusive_scan(dnaln_ctx* c, const int64_t* in, int64_t* out, int64_t n);
 
-double ev_ms(dnaln_ctx* c, int a, int b) {
+double ev_ms(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0;
-  if (cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]) != cudaSuccess) {
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
     cudaGetLastError();
     return 0.0;
   }
   return ms;
+}
+
+double ev_ms(dnaln_ctx* c, int a, int b) { return ev_ms(c->ev[a], c->ev[b]); }
+
+void trace_mark(void* self, cudaStream_t st, const char* kernel) {
+  auto* c = static_cast<dnaln_ctx*>(self);
+  if (kernel) {
+    c->trace_open = c->trace_n < kMaxTrace && (c->trace_only.empty() || c->trace_only == kernel) &&
+                    cudaEventRecord(c->trace_ev[2 * c->trace_n], st) == cudaSuccess;
+    if (c->trace_open) c->trace_name[c->trace_n] = kernel;
+  } else if (c->trace_open) {
+    if (cudaEventRecord(c->trace_ev[2 * c->trace_n + 1], st) == cudaSuccess) ++c->trace_n;
+    c->trace_open = false;
+  }
+}
+
+// The context's tracer (a no-op when tracing is off).
+KernelTrace tracer(dnaln_ctx* c) {
+  KernelTrace t;
+  if (c->trace_on) {
+    t.mark = trace_mark;
+    t.self = c;
+  }
+  return t;
+}
+
+// Adds the traced launches of the batch to the totals; call once the stream is idle.
+void trace_collect(dnaln_ctx* c) {
+  for (int i = 0; i < c->trace_n; ++i) {
+    KernelTime& k = c->ktimes[c->trace_name[i]];
+    ++k.launches;
+    k.ms += ev_ms(c->trace_ev[2 * i], c->trace_ev[2 * i + 1]);
+  }
+  c->trace_n = 0;
+  c->trace_open = false;
+}
+
+int exclusive_scan(dnaln_ctx* c, const int64_t* in, int64_t* out, int64_t n) {
+  size_t tmp = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, c->st));
+  DBUF(t, uint8_t, "cub_tmp", tmp);
+  const KernelTrace kt = tracer(c);
+  kt.begin(c->st, "cub_scan");
+  const cudaError_t e = cub::DeviceScan::ExclusiveSum(t, tmp, in, out, n, c->st);
+  kt.end(c->st);
+  CK(e);
+  return DNALN_OK;
 }
 
 bool score_params_ok(const dnaln_score_params& s, std::string& why) {
@@ -154,6 +227,31 @@ std::vector<int32_t> chain_cost_lut(int k, int band) {
     lut[static_cast<size_t>(dd)] = static_cast<int>(0.01 * k * static_cast<double>(dd) + 0.5 * lg);
   }
   return lut;
+}
+
+// The gap-cost table on the device for (k, band), uploaded (stream-ordered, from
+// page-locked staging) only when the pair changes: a pageable upload per batch would
+// block the host behind copies in flight on other streams.
+int chain_lut_dev(dnaln_ctx* c, int k, int band, const int32_t** out) {
+  const size_t n = static_cast<size_t>(band) + 1;
+  DBUF(d, int32_t, "chain_lut", n);
+  if (c->lut_k != k || c->lut_band != band) {
+    const std::vector<int32_t> lut = chain_cost_lut(k, band);
+    CK(cudaStreamSynchronize(c->st));  // the staging buffer may still feed an earlier upload
+    if (c->h_lut_cap < n) {
+      if (c->h_lut) cudaFreeHost(c->h_lut);
+      c->h_lut = nullptr;
+      c->h_lut_cap = 0;
+      CK(cudaHostAlloc(&c->h_lut, n * sizeof(int32_t), cudaHostAllocDefault));
+      c->h_lut_cap = n;
+    }
+    std::memcpy(c->h_lut, lut.data(), n * sizeof(int32_t));
+    CK(cudaMemcpyAsync(d, c->h_lut, n * sizeof(int32_t), cudaMemcpyHostToDevice, c->st));
+    c->lut_k = k;
+    c->lut_band = band;
+  }
+  *out = d;
+  return DNALN_OK;
 }
 
 __global__ void k_len64(const int32_t* __restrict__ len, int64_t n, int64_t* __restrict__ out,
@@ -212,10 +310,11 @@ int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks,
   }
   int* fb = dbuf<int>(c, "sw_fb", static_cast<size_t>(chunk) + 1);
   if (!fb) return DNALN_ERR_OOM;
+  const KernelTrace kt = tracer(c);
   for (int64_t b = 0; b < n_max; b += chunk) {
     const int cnt = static_cast<int>(n_max - b < chunk ? n_max - b : chunk);
     if (!launch_sw(c->st, tb, bytes_ok, tasks, static_cast<int>(b), cnt, n_max, n_dev, qbase, tbase, sp, res, dir,
-                   rows_max, cig, cig_off, band, fb, c->d_err))
+                   rows_max, cig, cig_off, band, fb, c->d_err, &kt))
       return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
     c->stats.launches += static_cast<uint64_t>(sw_launches(sp.W, bytes_ok, tb));
   }
@@ -240,8 +339,11 @@ int validate_map_params(dnaln_ctx* c, const dnaln_map_params* p, const IndexRes&
 // *cigar_dev. *cigar_used = total ops.
 int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_off, const int32_t* d_seq_len,
             const uint32_t* d_hash, int64_t n, const dnaln_map_params& p, dnaln_map_record* d_out, uint32_t* d_cigar,
-            int64_t cigar_cap, int64_t* cigar_used, uint32_t** cigar_dev) {
+            int64_t cigar_cap, int64_t* cigar_used, uint32_t** cigar_dev, const BatchHints& hint) {
   cudaStream_t st = c->st;
+  const KernelTrace kt = tracer(c);
+  c->trace_n = 0;
+  c->trace_open = false;
   const int bw = p.sc.bw, W = 2 * bw + 1, MC = p.max_cand;
   const int chain_band = p.ch.band < bw ? p.ch.band : bw;  // src/mapper.cpp:9
   *cigar_used = 0;
@@ -250,18 +352,24 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   // packed offsets, total bases, longest read
   DBUF(len64, int64_t, "len64", n + 1);
   DBUF(pofs, int64_t, "pofs", n + 1);
-  DBUF(info, unsigned long long, "info", 4);
-  CK(cudaMemsetAsync(info, 0, 4 * sizeof(unsigned long long), st));
+  // info: [0] longest read, [1..3] cells, mapped, candidates (map.cuh), [4] minimizers
+  DBUF(info, unsigned long long, "info", 5);
+  CK(cudaMemsetAsync(info, 0, 5 * sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
-  CK(cudaMemsetAsync(c->d_count, 0, 2 * sizeof(int), st));
+  CK(cudaMemsetAsync(c->d_count, 0, 3 * sizeof(int), st));
   unsigned long long* ctr = info + 1;  // cells, mapped, candidates (map.cuh)
+  kt.begin(st, "k_len64");
   k_len64<<<nblk(n + 1), 256, 0, st>>>(d_seq_len, n, len64, info);
+  kt.end(st);
   if (int e = exclusive_scan(c, len64, pofs, n + 1)) return e;
-  CK(cudaMemcpyAsync(c->h_info, pofs + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(c->h_info + 1, info, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  const int64_t B = c->h_info[0];
-  const int64_t max_len = c->h_info[1];
+  int64_t B = hint.bases, max_len = hint.max_len;
+  if (B < 0 || max_len < 0) {
+    CK(cudaMemcpyAsync(c->h_info, pofs + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c->h_info + 1, info, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    B = c->h_info[0];
+    max_len = c->h_info[1];
+  }
   if (max_len > (1 << 28)) return fail(c, DNALN_ERR_INVALID_ARG, "read longer than 2^28 bases");
 
   // pass 1: encode, sketch, probe
@@ -277,16 +385,58 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   DBUF(anchor_off, int64_t, "anchor_off", n + 1);
   CK(cudaMemsetAsync(n_anchor + n, 0, sizeof(int64_t), st));
   SeedParams sp{p.k, p.w, p.max_occ};
+  CandBuf cb;
+  cb.n_cand = dbuf<int32_t>(c, "cand_n", n);
+  cb.rev = dbuf<uint8_t>(c, "cand_rev", n * MC);
+  cb.contig = dbuf<int32_t>(c, "cand_contig", n * MC);
+  cb.diag = dbuf<int64_t>(c, "cand_diag", n * MC);
+  cb.wstart = dbuf<int64_t>(c, "cand_wstart", n * MC);
+  if (!cb.n_cand || !cb.rev || !cb.contig || !cb.diag || !cb.wstart) return DNALN_ERR_OOM;
+  const int32_t* d_lut = nullptr;
+  if (int e = chain_lut_dev(c, p.k, chain_band, &d_lut)) return e;
+  ChainParamsDev cp{p.ch.max_gap, chain_band, p.ch.lookback, p.ch.min_score, p.ch.min_anchors, p.k, d_lut};
+  CandParams cand{MC, bw, p.pri_ratio};
+  // short reads run passes 1 and 2 one thread per read; the rest (listed) one warp per read
+  const bool thread_path = !c->warp_seed_only && seed_thread_supported(sp, cp);
+  DBUF(big_list, int32_t, "big_list", n);
+  int* big_n = c->d_count + 2;
   CK(cudaEventRecord(c->ev[kEvSeed0], st));
-  launch_seed(st, d_seq, d_seq_off, d_seq_len, pofs, n, codes, ix.dev, sp, mb, n_min, n_anchor, c->d_err);
+  if (thread_path) {
+    kt.begin(st, "k_seed_chain_t");
+    const bool ok = launch_seed_chain_thread(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, codes, ix.dev,
+                                             sp, cp, cand, cb, n_min, n_anchor, big_list, big_n, c->d_err);
+    kt.end(st);
+    if (!ok) return fail(c, DNALN_ERR_CUDA, "thread-per-read seeding kernel could not be configured");
+    kt.begin(st, "k_seed<list>");
+    launch_seed_list(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, big_list, big_n, codes, ix.dev, sp, mb,
+                     n_min, n_anchor, c->d_err);
+    kt.end(st);
+  } else {
+    kt.begin(st, "k_seed");
+    launch_seed(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, codes, ix.dev, sp, mb, n_min, n_anchor,
+                c->d_err);
+    kt.end(st);
+  }
   CK(cudaEventRecord(c->ev[kEvSeed1], st));
   CK(cudaGetLastError());
   if (int e = exclusive_scan(c, n_anchor, anchor_off, n + 1)) return e;
+  {  // minimizer total (MapStats-style counter), read back with the anchor total
+    size_t tmp = 0;
+    int64_t* total = reinterpret_cast<int64_t*>(info + 4);
+    CK(cub::DeviceReduce::Sum(nullptr, tmp, n_min, total, n, st));
+    DBUF(t, uint8_t, "cub_tmp_red", tmp);
+    CK(cub::DeviceReduce::Sum(t, tmp, n_min, total, n, st));
+  }
   CK(cudaMemcpyAsync(c->h_info, anchor_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 1, info + 4, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 2, big_n, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   const int64_t A = c->h_info[0];
+  const int64_t n_minimizers = c->h_info[1];
+  int n_big = 0;
+  std::memcpy(&n_big, c->h_info + 2, sizeof n_big);
 
-  // pass 2: anchors, chains, candidates
+  // pass 2 of the warp path: anchors, chains, candidates
   AnchorScratch as;
   as.keys = dbuf<uint64_t>(c, "a_keys", A);
   as.f = dbuf<int32_t>(c, "a_f", A);
@@ -301,23 +451,15 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   if (!as.keys || !as.f || !as.prev || !as.ord || !as.used || !as.ch_score || !as.ch_sn || !as.ch_dmin ||
       !as.ch_dmax || !as.ch_rpos)
     return DNALN_ERR_OOM;
-  CandBuf cb;
-  cb.n_cand = dbuf<int32_t>(c, "cand_n", n);
-  cb.rev = dbuf<uint8_t>(c, "cand_rev", n * MC);
-  cb.contig = dbuf<int32_t>(c, "cand_contig", n * MC);
-  cb.diag = dbuf<int64_t>(c, "cand_diag", n * MC);
-  cb.wstart = dbuf<int64_t>(c, "cand_wstart", n * MC);
-  if (!cb.n_cand || !cb.rev || !cb.contig || !cb.diag || !cb.wstart) return DNALN_ERR_OOM;
-  const std::vector<int32_t> lut = chain_cost_lut(p.k, chain_band);
-  DBUF(d_lut, int32_t, "chain_lut", lut.size());
-  CK(cudaMemcpyAsync(d_lut, lut.data(), lut.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-  ChainParamsDev cp{p.ch.max_gap, chain_band, p.ch.lookback, p.ch.min_score, p.ch.min_anchors, p.k, d_lut};
-  CandParams cand{MC, bw, p.pri_ratio};
   CK(cudaEventRecord(c->ev[kEvChain0], st));
-  launch_chain_map(st, pofs, d_seq_len, n, n_min, anchor_off, mb, ix.dev, cp, cand, as, cb, c->d_err);
+  if (!thread_path || n_big > 0) {
+    kt.begin(st, thread_path ? "k_chain_map<list>" : "k_chain_map");
+    launch_chain_map(st, pofs, d_seq_len, thread_path ? n_big : n, thread_path ? big_list : nullptr, n_min, anchor_off,
+                     mb, ix.dev, cp, cand, as, cb, c->d_err);
+    kt.end(st);
+  }
   CK(cudaEventRecord(c->ev[kEvChain1], st));
   CK(cudaGetLastError());
-
   // score-only ranking of multi-candidate reads
   const dnaln_score_params& sc = p.sc;
   const SwParams swp = make_sw_params(sc);
@@ -326,7 +468,9 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   DBUF(sc_tasks, SwTask, "sc_tasks", n * MC);
   DBUF(res_sc, SwResult, "res_sc", n * MC);
   CK(cudaEventRecord(c->ev[kEvSc0], st));
+  kt.begin(st, "k_score_tasks");
   launch_score_tasks(st, n, pofs, d_seq_len, cb, ix.dev, mc, sc_tasks, c->d_count, ctr);
+  kt.end(st);
   if (int e = launch_sw_chunked(c, false, bytes_ok, sc_tasks, static_cast<int>(n * MC), c->d_count, codes,
                                 ix.dev.genome, swp, res_sc, static_cast<int>(max_len), nullptr, nullptr))
     return e;
@@ -340,8 +484,12 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   DBUF(cig_tb, uint32_t, "cig_tb", 2 * B + n);
   DBUF(cig_slot, int64_t, "cig_slot", n);
   CK(cudaEventRecord(c->ev[kEvTb0], st));
+  kt.begin(st, "k_choose");
   launch_choose(st, n, pofs, d_seq_len, cb, res_sc, d_hash, ix.dev, mc, chosen, s2, tb_tasks, c->d_count + 1, ctr);
+  kt.end(st);
+  kt.begin(st, "k_cig_slots");
   k_cig_slots<<<nblk(n), 256, 0, st>>>(pofs, n, cig_slot);
+  kt.end(st);
   if (int e = launch_sw_chunked(c, true, bytes_ok, tb_tasks, static_cast<int>(n), c->d_count + 1, codes,
                                 ix.dev.genome, swp, res_tb, static_cast<int>(max_len), cig_tb, cig_slot))
     return e;
@@ -351,7 +499,9 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   DBUF(cig_cnt, int64_t, "cig_cnt", n + 1);
   DBUF(cig_off, int64_t, "cig_off", n + 1);
   CK(cudaEventRecord(c->ev[kEvPost0], st));
+  kt.begin(st, "k_records");
   launch_records(st, n, d_seq_len, cb, chosen, s2, res_tb, ix.dev, mc, d_out, cig_cnt, ctr);
+  kt.end(st);
   if (int e = exclusive_scan(c, cig_cnt, cig_off, n + 1)) return e;
   CK(cudaMemcpyAsync(c->h_info, cig_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(c->h_info + 1, c->d_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -376,20 +526,25 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   if (total_ops > cigar_cap)
     return fail(c, DNALN_ERR_CAPACITY, "CIGAR buffer holds %lld ops, batch needs %lld",
                 static_cast<long long>(cigar_cap), static_cast<long long>(total_ops));
-  launch_cigar_gather(st, n, pofs, d_seq_len, res_tb, cig_tb, cig_off, d_out, d_cigar);
+  kt.begin(st, "k_cigar_gather");
+  launch_cigar_gather(st, n, pofs, d_seq_len, res_tb, cig_tb, cig_off, hint.cigar_base, d_out, d_cigar);
+  kt.end(st);
   CK(cudaEventRecord(c->ev[kEvPost1], st));
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
+  trace_collect(c);
 
   dnaln_stats& s = c->stats;
   s.reads += static_cast<uint64_t>(n);
   s.anchors += static_cast<uint64_t>(A);
+  s.minimizers += static_cast<uint64_t>(n_minimizers);
   s.sw_tasks_score += static_cast<uint64_t>(counts[0]);
   s.sw_tasks_tb += static_cast<uint64_t>(counts[1]);
   s.cells += n_cells;
   s.mapped += n_mapped;
   s.candidates += n_cands;
-  s.launches += 8;  // k_len64, k_seed, k_chain_map, k_score_tasks, k_choose, k_cig_slots, k_records, k_cigar_gather
+  // k_len64, k_score_tasks, k_choose, k_cig_slots, k_records, k_cigar_gather, plus pass 1 / 2
+  s.launches += 6 + (thread_path ? 2 + (n_big > 0 ? 1 : 0) : 2);
   s.ms_seed += ev_ms(c, kEvSeed0, kEvSeed1);
   s.ms_chain += ev_ms(c, kEvChain0, kEvChain1);
   s.ms_sw_score += ev_ms(c, kEvSc0, kEvSc1);
@@ -458,6 +613,12 @@ int dnaln_gpu_ctx_create(int device, dnaln_ctx** out) {
   bad(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
   c->st = c->own;
   for (auto& x : c->ev) bad(cudaEventCreate(&x));
+  bad(cudaStreamCreateWithFlags(&c->cp_in, cudaStreamNonBlocking));
+  bad(cudaStreamCreateWithFlags(&c->cp_out, cudaStreamNonBlocking));
+  for (auto& x : c->in_ready) bad(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+  for (auto& x : c->out_free) bad(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+  for (auto& x : c->h2d_ev) bad(cudaEventCreate(&x));
+  for (auto& x : c->d2h_ev) bad(cudaEventCreate(&x));
   bad(cudaMalloc(&c->d_err, sizeof(uint32_t)));
   bad(cudaMalloc(&c->d_count, 4 * sizeof(int)));
   bad(cudaHostAlloc(&c->h_info, 8 * sizeof(int64_t), cudaHostAllocDefault));
@@ -476,11 +637,24 @@ int dnaln_gpu_ctx_destroy(dnaln_ctx* c) {
   for (auto& kv : c->idx) free_index(kv.second);
   for (auto& kv : c->bufs)
     if (kv.second.p) cudaFree(kv.second.p);
+  if (c->cp_in) cudaStreamSynchronize(c->cp_in);
+  if (c->cp_out) cudaStreamSynchronize(c->cp_out);
   for (auto& x : c->ev)
     if (x) cudaEventDestroy(x);
+  for (cudaEvent_t* set : {c->in_ready, c->out_free})
+    for (int i = 0; i < 2; ++i)
+      if (set[i]) cudaEventDestroy(set[i]);
+  for (cudaEvent_t* set : {c->h2d_ev, c->d2h_ev})
+    for (int i = 0; i < 4; ++i)
+      if (set[i]) cudaEventDestroy(set[i]);
+  for (auto& x : c->trace_ev)
+    if (x) cudaEventDestroy(x);
+  if (c->cp_in) cudaStreamDestroy(c->cp_in);
+  if (c->cp_out) cudaStreamDestroy(c->cp_out);
   if (c->d_err) cudaFree(c->d_err);
   if (c->d_count) cudaFree(c->d_count);
   if (c->h_info) cudaFreeHost(c->h_info);
+  if (c->h_lut) cudaFreeHost(c->h_lut);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
   return DNALN_OK;
@@ -503,7 +677,61 @@ int dnaln_gpu_get_stats(const dnaln_ctx* c, dnaln_stats* out) {
 int dnaln_gpu_reset_stats(dnaln_ctx* c) {
   if (!c) return DNALN_ERR_INVALID_ARG;
   c->stats = dnaln_stats{};
+  c->ktimes.clear();
   return DNALN_OK;
+}
+
+int dnaln_gpu_set_kernel_trace(dnaln_ctx* c, int32_t on, const char* only) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  c->trace_only = only ? only : "";
+  if (on && c->trace_ev.empty()) {
+    if (int e = set_device(c)) return e;
+    c->trace_ev.assign(2 * kMaxTrace, nullptr);
+    for (auto& x : c->trace_ev) CK(cudaEventCreate(&x));
+  }
+  c->trace_on = on != 0;
+  c->trace_n = 0;
+  c->trace_open = false;
+  return DNALN_OK;
+}
+
+int dnaln_gpu_kernel_times(const dnaln_ctx* c, dnaln_kernel_time* out, int32_t cap, int32_t* n_out) {
+  if (!c || !n_out || cap < 0 || (cap > 0 && !out)) return DNALN_ERR_INVALID_ARG;
+  int32_t i = 0;
+  for (const auto& kv : c->ktimes) {
+    if (i < cap) {
+      dnaln_kernel_time& o = out[i];
+      std::memset(&o, 0, sizeof o);
+      std::snprintf(o.name, sizeof o.name, "%s", kv.first.c_str());
+      o.launches = kv.second.launches;
+      o.ms = kv.second.ms;
+    }
+    ++i;
+  }
+  *n_out = i;
+  return DNALN_OK;
+}
+
+int dnaln_gpu_set_sub_batch(dnaln_ctx* c, int64_t reads) {
+  if (!c || reads < 0) return DNALN_ERR_INVALID_ARG;
+  c->sub_batch = reads;
+  return DNALN_OK;
+}
+
+int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
+  if (!c || !name) return DNALN_ERR_INVALID_ARG;
+  const std::string k = name;
+  if (k == "sub_batch") return dnaln_gpu_set_sub_batch(c, value);
+  if (k == "warp_seed_only") {
+    c->warp_seed_only = value != 0;
+    return DNALN_OK;
+  }
+  if (k == "dir_cap_bytes") {
+    if (value < (int64_t(1) << 20)) return fail(c, DNALN_ERR_INVALID_ARG, "dir_cap_bytes must be >= 1 MiB");
+    c->dir_cap_bytes = static_cast<size_t>(value);
+    return DNALN_OK;
+  }
+  return fail(c, DNALN_ERR_INVALID_ARG, "unknown option '%s'", name);
 }
 
 int dnaln_gpu_host_alloc(dnaln_ctx* c, size_t bytes, void** out) {
@@ -732,12 +960,11 @@ int dnaln_gpu_chain(dnaln_ctx* c, uint32_t* rpos, int32_t* qpos, uint32_t* stran
     return DNALN_ERR_OOM;
   DBUF(d_set, int64_t, "ch_set", n_sets + 1);
   DBUF(d_cnt, int32_t, "ch_cnt", n_sets);
-  const std::vector<int32_t> lut = chain_cost_lut(k, p->band);
-  DBUF(d_lut, int32_t, "chain_lut", lut.size());
+  const int32_t* d_lut = nullptr;
+  if (int e = chain_lut_dev(c, k, p->band, &d_lut)) return e;
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
   CK(cudaMemcpyAsync(as.keys, keys.data(), total * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(d_set, set_off, (n_sets + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(d_lut, lut.data(), lut.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   ChainParamsDev cp{p->max_gap, p->band, p->lookback, p->min_score, p->min_anchors, k, d_lut};
   launch_chain_sets(st, d_set, n_sets, cp, as, d_cnt, c->d_err);
   CK(cudaGetLastError());
@@ -832,6 +1059,8 @@ int dnaln_gpu_align(dnaln_ctx* c, const uint8_t* q, const int64_t* q_off, const 
     if (!d_cig || !d_slot) return DNALN_ERR_OOM;
     CK(cudaMemcpyAsync(d_slot, slot_off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
   }
+  c->trace_n = 0;
+  c->trace_open = false;
   CK(cudaEventRecord(c->ev[tb ? kEvTb0 : kEvSc0], st));
   if (int e = launch_sw_chunked(c, tb, sw_bytes_ok(*sp), d_tasks, static_cast<int>(n), nullptr, d_q, d_t, swp, d_res,
                                 rows_max, d_cig, d_slot))
@@ -864,6 +1093,7 @@ int dnaln_gpu_align(dnaln_ctx* c, const uint8_t* q, const int64_t* q_off, const 
       CK(cudaMemcpyAsync(cigar, d_final, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
   }
+  trace_collect(c);
   uint32_t bits = 0;
   CK(cudaMemcpy(&bits, c->d_err, sizeof bits, cudaMemcpyDeviceToHost));
   if (int e = check_device_errors(c, bits)) return e;
@@ -895,7 +1125,7 @@ int dnaln_gpu_map_batch_device(dnaln_ctx* c, int32_t id, const char* d_seq, cons
   if (int e = validate_map_params(c, p, *r)) return e;
   if (!d_cigar) return fail(c, DNALN_ERR_INVALID_ARG, "null CIGAR buffer");
   const int e = run_map(c, *r, d_seq, d_seq_off, d_seq_len, d_name_hash, n, *p, d_out, d_cigar, cigar_cap,
-                        cigar_used, nullptr);
+                        cigar_used, nullptr, BatchHints{});
   if (e == DNALN_OK) c->stats.cells += 0;
   return e;
 }
@@ -911,37 +1141,124 @@ int dnaln_gpu_map_batch(dnaln_ctx* c, int32_t id, const char* seq, const int64_t
   if (int e = validate_map_params(c, p, *r)) return e;
   *cigar_used = 0;
   if (n == 0) return DNALN_OK;
-  int64_t ext = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    if (seq_len[i] < 0 || seq_off[i] < 0) return fail(c, DNALN_ERR_INVALID_ARG, "negative offset or length");
-    ext = std::max<int64_t>(ext, seq_off[i] + seq_len[i]);
+
+  // Sub-batches of at most sub_batch reads go through two device slots: while one
+  // sub-batch computes, the next one's reads are copied in and the previous one's records
+  // and CIGARs are copied out, on the context's two copy streams.
+  struct Sub {
+    int64_t a, b, lo, hi, bases, max_len, cig_bound;
+  };
+  const int64_t S = c->sub_batch > 0 ? c->sub_batch : n;
+  std::vector<Sub> subs;
+  int64_t span = 0, rmax = 0, cmax = 0;
+  for (int64_t a = 0; a < n; a += S) {
+    Sub sb{a, std::min(n, a + S), seq_off[a], 0, 0, 0, 0};
+    for (int64_t i = sb.a; i < sb.b; ++i) {
+      if (seq_len[i] < 0 || seq_off[i] < 0) return fail(c, DNALN_ERR_INVALID_ARG, "negative offset or length");
+      sb.lo = std::min(sb.lo, seq_off[i]);
+      sb.hi = std::max(sb.hi, seq_off[i] + seq_len[i]);
+      sb.bases += seq_len[i];
+      sb.max_len = std::max<int64_t>(sb.max_len, seq_len[i]);
+      sb.cig_bound += 2 * static_cast<int64_t>(seq_len[i]) + 3;  // walk ops (<= 2*len+1) + 2 clips
+    }
+    span = std::max(span, sb.hi - sb.lo);
+    rmax = std::max(rmax, sb.b - sb.a);
+    cmax = std::max(cmax, sb.cig_bound);
+    subs.push_back(sb);
+  }
+  const int J = static_cast<int>(subs.size());
+  char* d_seq[2] = {};
+  int64_t* d_off[2] = {};
+  int32_t* d_len[2] = {};
+  uint32_t* d_hash[2] = {};
+  dnaln_map_record* d_out[2] = {};
+  uint32_t* d_cig[2] = {};
+  static const char* const kSlotNames[2][6] = {{"in_seq0", "in_off0", "in_len0", "in_hash0", "out_rec0", "out_cig0"},
+                                               {"in_seq1", "in_off1", "in_len1", "in_hash1", "out_rec1", "out_cig1"}};
+  for (int k = 0; k < 2 && k < J; ++k) {
+    d_seq[k] = dbuf<char>(c, kSlotNames[k][0], span);
+    d_off[k] = dbuf<int64_t>(c, kSlotNames[k][1], rmax);
+    d_len[k] = dbuf<int32_t>(c, kSlotNames[k][2], rmax);
+    d_hash[k] = dbuf<uint32_t>(c, kSlotNames[k][3], rmax);
+    d_out[k] = dbuf<dnaln_map_record>(c, kSlotNames[k][4], rmax);
+    d_cig[k] = dbuf<uint32_t>(c, kSlotNames[k][5], cmax);
+    if (!d_seq[k] || !d_off[k] || !d_len[k] || !d_hash[k] || !d_out[k] || !d_cig[k]) return DNALN_ERR_OOM;
   }
   cudaStream_t st = c->st;
-  DBUF(d_seq, char, "in_seq", ext);
-  DBUF(d_off, int64_t, "in_off", n);
-  DBUF(d_len, int32_t, "in_len", n);
-  DBUF(d_hash, uint32_t, "in_hash", n);
-  DBUF(d_out, dnaln_map_record, "out_rec", n);
-  CK(cudaEventRecord(c->ev[kEvH2d0], st));
-  CK(cudaMemcpyAsync(d_seq, seq, ext, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(d_off, seq_off, n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(d_len, seq_len, n * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(d_hash, name_hash, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-  CK(cudaEventRecord(c->ev[kEvH2d1], st));
-  uint32_t* d_cig = nullptr;
-  int e = run_map(c, *r, d_seq, d_off, d_len, d_hash, n, *p, d_out, nullptr, 0, cigar_used, &d_cig);
+  bool h2d_rec[2] = {false, false}, d2h_rec[2] = {false, false};
+  const auto drain = [&]() {
+    cudaStreamSynchronize(c->cp_in);
+    cudaStreamSynchronize(c->cp_out);
+    for (int k = 0; k < 2; ++k) {
+      if (h2d_rec[k]) c->stats.ms_h2d += ev_ms(c->h2d_ev[2 * k], c->h2d_ev[2 * k + 1]);
+      if (d2h_rec[k]) c->stats.ms_d2h += ev_ms(c->d2h_ev[2 * k], c->d2h_ev[2 * k + 1]);
+      h2d_rec[k] = d2h_rec[k] = false;
+    }
+  };
+  const auto h2d = [&](int j) -> int {
+    const Sub& sb = subs[j];
+    const int k = j & 1;
+    const int64_t m = sb.b - sb.a;
+    if (h2d_rec[k]) c->stats.ms_h2d += ev_ms(c->h2d_ev[2 * k], c->h2d_ev[2 * k + 1]);  // done: its slot was used
+    CK(cudaEventRecord(c->h2d_ev[2 * k], c->cp_in));
+    if (sb.hi > sb.lo) CK(cudaMemcpyAsync(d_seq[k], seq + sb.lo, sb.hi - sb.lo, cudaMemcpyHostToDevice, c->cp_in));
+    CK(cudaMemcpyAsync(d_off[k], seq_off + sb.a, m * sizeof(int64_t), cudaMemcpyHostToDevice, c->cp_in));
+    CK(cudaMemcpyAsync(d_len[k], seq_len + sb.a, m * sizeof(int32_t), cudaMemcpyHostToDevice, c->cp_in));
+    CK(cudaMemcpyAsync(d_hash[k], name_hash + sb.a, m * sizeof(uint32_t), cudaMemcpyHostToDevice, c->cp_in));
+    CK(cudaEventRecord(c->h2d_ev[2 * k + 1], c->cp_in));
+    CK(cudaEventRecord(c->in_ready[k], c->cp_in));
+    h2d_rec[k] = true;
+    return DNALN_OK;
+  };
+  const auto d2h = [&](int j, int64_t base, int64_t used) -> int {
+    const Sub& sb = subs[j];
+    const int k = j & 1;
+    if (d2h_rec[k]) c->stats.ms_d2h += ev_ms(c->d2h_ev[2 * k], c->d2h_ev[2 * k + 1]);
+    CK(cudaEventRecord(c->d2h_ev[2 * k], c->cp_out));
+    CK(cudaMemcpyAsync(out + sb.a, d_out[k], (sb.b - sb.a) * sizeof(dnaln_map_record), cudaMemcpyDeviceToHost,
+                       c->cp_out));
+    if (used > 0)
+      CK(cudaMemcpyAsync(cigar + base, d_cig[k], used * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->cp_out));
+    CK(cudaEventRecord(c->d2h_ev[2 * k + 1], c->cp_out));
+    CK(cudaEventRecord(c->out_free[k], c->cp_out));
+    d2h_rec[k] = true;
+    return DNALN_OK;
+  };
+
+  int64_t base = 0;
+  int e = DNALN_OK;
+  for (int j = 0; j < 2 && j < J && e == DNALN_OK; ++j) e = h2d(j);
+  for (int j = 0; j < J && e == DNALN_OK; ++j) {
+    const Sub& sb = subs[j];
+    const int k = j & 1;
+    if (cudaStreamWaitEvent(st, c->in_ready[k], 0) != cudaSuccess ||
+        (j >= 2 && cudaStreamWaitEvent(st, c->out_free[k], 0) != cudaSuccess)) {
+      e = fail(c, DNALN_ERR_CUDA, "stream wait: %s", cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    BatchHints hint;
+    hint.seq_base = sb.lo;
+    hint.bases = sb.bases;
+    hint.max_len = sb.max_len;
+    hint.cigar_base = base;
+    int64_t used = 0;
+    e = run_map(c, *r, d_seq[k], d_off[k], d_len[k], d_hash[k], sb.b - sb.a, *p, d_out[k], d_cig[k], cmax, &used,
+                nullptr, hint);
+    if (e != DNALN_OK) break;
+    // run_map returns with its stream idle, so slot k's inputs are free for sub-batch j + 2
+    if (j + 2 < J && (e = h2d(j + 2)) != DNALN_OK) break;
+    if (base + used > cigar_cap || (used > 0 && !cigar)) {
+      e = fail(c, DNALN_ERR_CAPACITY, "CIGAR buffer holds %lld ops, batch needs at least %lld",
+               static_cast<long long>(cigar_cap), static_cast<long long>(base + used));
+      break;
+    }
+    if ((e = d2h(j, base, used)) != DNALN_OK) break;
+    base += used;
+  }
+  drain();
   if (e != DNALN_OK) return e;
-  if (*cigar_used > cigar_cap || (*cigar_used > 0 && !cigar))
-    return fail(c, DNALN_ERR_CAPACITY, "CIGAR buffer holds %lld ops, batch needs %lld",
-                static_cast<long long>(cigar_cap), static_cast<long long>(*cigar_used));
-  CK(cudaEventRecord(c->ev[kEvD2h0], st));
-  CK(cudaMemcpyAsync(out, d_out, n * sizeof(dnaln_map_record), cudaMemcpyDeviceToHost, st));
-  if (*cigar_used > 0)
-    CK(cudaMemcpyAsync(cigar, d_cig, *cigar_used * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  CK(cudaEventRecord(c->ev[kEvD2h1], st));
-  CK(cudaStreamSynchronize(st));
-  c->stats.ms_h2d += ev_ms(c, kEvH2d0, kEvH2d1);
-  c->stats.ms_d2h += ev_ms(c, kEvD2h0, kEvD2h1);
+  if (cudaGetLastError() != cudaSuccess) return fail(c, DNALN_ERR_CUDA, "copy stream error");
+  *cigar_used = base;
   return DNALN_OK;
 }
 

@@ -70,6 +70,20 @@ struct SwParams {
   uint32_t prof_n;  // 4 bytes of -ambig (table entries 4..7 of the byte-permute profile)
 };
 
+// Optional per-kernel timing hook of the orchestrator: begin() before a launch and end()
+// after it record an event pair on the launching stream under the kernel's name. A null
+// hook (or one with no callback) costs nothing.
+struct KernelTrace {
+  void (*mark)(void* self, cudaStream_t st, const char* kernel) = nullptr;  // kernel == nullptr: end
+  void* self = nullptr;
+  void begin(cudaStream_t st, const char* kernel) const {
+    if (mark) mark(self, st, kernel);
+  }
+  void end(cudaStream_t st) const {
+    if (mark) mark(self, st, nullptr);
+  }
+};
+
 __host__ __device__ __forceinline__ int sub_score(const SwParams& p, int a, int b) {
   return (a > 3 || b > 3) ? -p.ambig : (a == b ? p.match : -p.mismatch);  // src/align.hpp:39
 }

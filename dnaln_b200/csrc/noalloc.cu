@@ -176,7 +176,7 @@ extern "C" int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_of
     k_na_tasks<<<blocks, 128, 0, st>>>(b, cnt, d_q_off, d_q_len, d_t_off, d_t_len, max_qlen, p.W,
                                        tb ? cigar_stride : 0, tasks, cig_off, err);
     if (!launch_sw(st, tb, bytes_ok, tasks, 0, cnt, cnt, nullptr, d_q, d_t, p, res, dir, rows,
-                   tb ? d_cigar : nullptr, cig_off, band, fb, err))
+                   tb ? d_cigar : nullptr, cig_off, band, fb, err, nullptr))
       return DNALN_ERR_DEVICE;
     k_na_finish<<<blocks, 128, 0, st>>>(b, cnt, res, tb ? cigar_stride : 0, tb, d_out, d_cigar);
     if (cudaGetLastError() != cudaSuccess) return DNALN_ERR_CUDA;

@@ -28,6 +28,8 @@
 // points in (f desc, index asc) order — another bitonic sort of packed keys — walked by
 // one lane, and ordered by score with ties in extraction order (the reference's
 // stable_sort). Candidate loci follow src/mapper.cpp:40-62.
+#include <algorithm>
+
 #include "common.cuh"
 #include "seed.cuh"
 
@@ -117,19 +119,6 @@ __device__ __forceinline__ uint32_t spread16(uint32_t x) {
   return x;
 }
 
-// hash64 for 2k <= 32: every step is either reduced mod 2^32 and then masked to 2k bits,
-// or a right shift of a value below 2^2k, so 32-bit arithmetic gives the same bits.
-__device__ __forceinline__ uint32_t hash32(uint32_t key, uint32_t mask) {
-  key = (~key + (key << 21)) & mask;
-  key = key ^ key >> 24;
-  key = ((key + (key << 3)) + (key << 8)) & mask;
-  key = key ^ key >> 14;
-  key = ((key + (key << 2)) + (key << 4)) & mask;
-  key = key ^ key >> 28;
-  key = (key + (key << 31)) & mask;
-  return key;
-}
-
 // Value of `cur` held d lanes to the left (0 <= d <= 31); lanes left of d read `prv`, the
 // previous chunk's value.
 __device__ __forceinline__ uint64_t from_left(uint64_t cur, uint64_t prv, int d) {
@@ -217,34 +206,6 @@ __device__ int warp_sketch_fast(CodeAt code_at, int len, int k, int w, Emit emit
     p_arg = __shfl_sync(FULL, arg, 31);
   }
   return count;
-}
-
-__device__ __forceinline__ void probe(const DevIndex& ix, uint64_t h, uint32_t& off, uint32_t& cnt,
-                                      uint32_t* err) {
-  uint64_t i = h & ix.mask;
-  off = 0;
-  cnt = 0;
-  for (uint64_t it = 0; it <= ix.mask; ++it) {  // load <= 0.5: an empty bucket always ends the walk
-    const ulonglong2 b = __ldg(ix.table + i);
-    if (b.x == h) {
-      off = static_cast<uint32_t>(b.y);
-      cnt = static_cast<uint32_t>(b.y >> 32);
-      return;
-    }
-    if (b.x == kInvalidHash) return;
-    i = (i + 1) & ix.mask;
-  }
-  atomicOr(err, kErrProbeLoop);
-}
-
-__device__ __forceinline__ int contig_of(const DevIndex& ix, uint64_t gpos) {  // src/reference.cpp:25-32
-  int64_t lo = 0, hi = ix.n_contigs;
-  while (hi - lo > 1) {
-    const int64_t mid = (lo + hi) / 2;
-    if (ix.contig_off[mid] <= gpos) lo = mid;
-    else hi = mid;
-  }
-  return static_cast<int>(lo);
 }
 
 // Ascending sort of a[0, n) by the warp: bitonic network in its all-ascending form (the
@@ -529,23 +490,25 @@ struct ChainSmem {
   uint8_t used[kSmCap];
 };
 
-__global__ void __launch_bounds__(kSeedWarps * 32)
-    k_seed(const char* __restrict__ seq, const int64_t* __restrict__ seq_off, const int32_t* __restrict__ seq_len,
-           const int64_t* __restrict__ pofs, int64_t n, uint8_t* __restrict__ codes, DevIndex ix, SeedParams sp,
-           MinBuf mb, int32_t* __restrict__ n_min, int64_t* __restrict__ n_anchor, uint32_t* __restrict__ err) {
-  __shared__ SketchSmem sm[kSeedWarps];
-  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t r = static_cast<int64_t>(blockIdx.x) * kSeedWarps + wib;
-  if (r >= n) return;
+// Pass 1 of read r by one warp (codes of both strands unless `encode` is false, because
+// another kernel already wrote them).
+__device__ void seed_read(int64_t r, bool encode, const char* __restrict__ seq, const int64_t* __restrict__ seq_off,
+                          int64_t seq_base, const int32_t* __restrict__ seq_len, const int64_t* __restrict__ pofs,
+                          uint8_t* __restrict__ codes, const DevIndex& ix, const SeedParams& sp, const MinBuf& mb,
+                          int32_t* __restrict__ n_min, int64_t* __restrict__ n_anchor, uint32_t* __restrict__ err,
+                          SketchSmem& smw) {
+  const int lane = threadIdx.x & 31;
   const int64_t so = pofs[r];  // packed offset of this read's codes and minimizer slots
   const int len = seq_len[r];
-  const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + seq_off[r];
+  const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + (seq_off[r] - seq_base);
   uint8_t* fw = codes + 2 * so;
   uint8_t* rc = fw + len;
-  for (int i = lane; i < len; i += 32) {  // src/mapper.cpp:88-99
-    const uint8_t c = nt4(s[i]);
-    fw[i] = c;
-    rc[len - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
+  if (encode) {
+    for (int i = lane; i < len; i += 32) {  // src/mapper.cpp:88-99
+      const uint8_t c = nt4(s[i]);
+      fw[i] = c;
+      rc[len - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
+    }
   }
   const auto code_at = [&](int i) { return nt4(s[i]); };
   const auto emit = [&](int rank, uint64_t h, int pos, uint32_t st) {
@@ -553,7 +516,7 @@ __global__ void __launch_bounds__(kSeedWarps * 32)
     mb.pos[so + rank] = static_cast<uint32_t>(pos) | st << 31;
   };
   const int cnt = (sp.k <= 15 && sp.w <= 32) ? warp_sketch_fast(code_at, len, sp.k, sp.w, emit)
-                                             : warp_sketch(code_at, len, sp.k, sp.w, sm[wib], emit);
+                                             : warp_sketch(code_at, len, sp.k, sp.w, smw, emit);
   __syncwarp();
   long long anchors = 0;
   for (int j = lane; j < cnt; j += 32) {
@@ -571,14 +534,31 @@ __global__ void __launch_bounds__(kSeedWarps * 32)
   }
 }
 
-__global__ void __launch_bounds__(kChainWarps * 32)
-    k_chain_map(const int64_t* __restrict__ pofs, const int32_t* __restrict__ seq_len, int64_t n,
-                const int32_t* __restrict__ n_min, const int64_t* __restrict__ anchor_off, MinBuf mb, DevIndex ix,
-                ChainParamsDev cp, CandParams cand, AnchorScratch as, CandBuf cb, uint32_t* __restrict__ err) {
-  __shared__ ChainSmem sm[kChainWarps];
-  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t r = static_cast<int64_t>(blockIdx.x) * kChainWarps + wib;
-  if (r >= n) return;
+// One warp per read: reads [0, n), or with a list the reads list[0, *list_n) (grid-stride).
+__global__ void __launch_bounds__(kSeedWarps * 32)
+    k_seed(const char* __restrict__ seq, const int64_t* __restrict__ seq_off, int64_t seq_base,
+           const int32_t* __restrict__ seq_len, const int64_t* __restrict__ pofs, int64_t n,
+           const int32_t* __restrict__ list, const int* __restrict__ list_n, uint8_t* __restrict__ codes,
+           DevIndex ix, SeedParams sp, MinBuf mb, int32_t* __restrict__ n_min, int64_t* __restrict__ n_anchor,
+           uint32_t* __restrict__ err) {
+  __shared__ SketchSmem sm[kSeedWarps];
+  const int wib = threadIdx.x >> 5;
+  const int64_t gw = static_cast<int64_t>(blockIdx.x) * kSeedWarps + wib;
+  if (!list) {
+    if (gw < n) seed_read(gw, true, seq, seq_off, seq_base, seq_len, pofs, codes, ix, sp, mb, n_min, n_anchor, err, sm[wib]);
+    return;
+  }
+  const int m = *list_n;
+  for (int64_t x = gw; x < m; x += static_cast<int64_t>(gridDim.x) * kSeedWarps)
+    seed_read(list[x], false, seq, seq_off, seq_base, seq_len, pofs, codes, ix, sp, mb, n_min, n_anchor, err, sm[wib]);
+}
+
+// Pass 2 of read r by one warp.
+__device__ void chain_read(int64_t r, const int64_t* __restrict__ pofs, const int32_t* __restrict__ seq_len,
+                           const int32_t* __restrict__ n_min, const int64_t* __restrict__ anchor_off, const MinBuf& mb,
+                           const DevIndex& ix, const ChainParamsDev& cp, const CandParams& cand,
+                           const AnchorScratch& as, const CandBuf& cb, uint32_t* __restrict__ err, ChainSmem& smw) {
+  const int lane = threadIdx.x & 31;
   const int64_t a0 = anchor_off[r];
   const int64_t na64 = anchor_off[r + 1] - a0;
   if (na64 > 0x3FFFFFFF) {
@@ -591,11 +571,11 @@ __global__ void __launch_bounds__(kChainWarps * 32)
   const int na = static_cast<int>(na64);
   const bool small = na <= kSmCap;
   ChainArrays a;
-  a.keys = small ? sm[wib].keys : as.keys + a0;
-  a.ord = small ? sm[wib].ord : as.ord + a0;
-  a.f = small ? sm[wib].f : as.f + a0;
-  a.prev = small ? sm[wib].prev : as.prev + a0;
-  a.used = small ? sm[wib].used : as.used + a0;
+  a.keys = small ? smw.keys : as.keys + a0;
+  a.ord = small ? smw.ord : as.ord + a0;
+  a.f = small ? smw.f : as.f + a0;
+  a.prev = small ? smw.prev : as.prev + a0;
+  a.used = small ? smw.used : as.used + a0;
   const int64_t so = pofs[r];
   const int len = seq_len[r], nm = n_min[r], k = cp.k;
   // anchors in minimizer order x occurrence order (src/mapper.cpp:32-40)
@@ -653,6 +633,19 @@ __global__ void __launch_bounds__(kChainWarps * 32)
   }
 }
 
+// One warp per read: reads [0, n), or with a list the reads list[0, list_n) (grid-stride).
+__global__ void __launch_bounds__(kChainWarps * 32)
+    k_chain_map(const int64_t* __restrict__ pofs, const int32_t* __restrict__ seq_len, int64_t n,
+                const int32_t* __restrict__ list, const int32_t* __restrict__ n_min,
+                const int64_t* __restrict__ anchor_off, MinBuf mb, DevIndex ix, ChainParamsDev cp, CandParams cand,
+                AnchorScratch as, CandBuf cb, uint32_t* __restrict__ err) {
+  __shared__ ChainSmem sm[kChainWarps];
+  const int wib = threadIdx.x >> 5;
+  const int64_t gw = static_cast<int64_t>(blockIdx.x) * kChainWarps + wib;
+  for (int64_t x = gw; x < n; x += static_cast<int64_t>(gridDim.x) * kChainWarps)
+    chain_read(list ? list[x] : x, pofs, seq_len, n_min, anchor_off, mb, ix, cp, cand, as, cb, err, sm[wib]);
+}
+
 __global__ void __launch_bounds__(kSeedWarps * 32)
     k_sketch_codes(const uint8_t* __restrict__ codes, const int64_t* __restrict__ seq_off,
                    const int32_t* __restrict__ seq_len, const uint32_t* __restrict__ pos_offset, int64_t n, int k,
@@ -708,22 +701,34 @@ __global__ void __launch_bounds__(kChainWarps * 32)
 
 }  // namespace
 
-void launch_seed(cudaStream_t st, const char* seq, const int64_t* seq_off, const int32_t* seq_len,
+void launch_seed(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base, const int32_t* seq_len,
                  const int64_t* pofs, int64_t n, uint8_t* codes, const DevIndex& ix, const SeedParams& sp, MinBuf mb,
                  int32_t* n_min, int64_t* n_anchor, uint32_t* err) {
   if (n <= 0) return;
   const int64_t blocks = (n + kSeedWarps - 1) / kSeedWarps;
-  k_seed<<<static_cast<unsigned>(blocks), kSeedWarps * 32, 0, st>>>(seq, seq_off, seq_len, pofs, n, codes, ix, sp, mb,
-                                                                   n_min, n_anchor, err);
+  k_seed<<<static_cast<unsigned>(blocks), kSeedWarps * 32, 0, st>>>(seq, seq_off, seq_base, seq_len, pofs, n, nullptr,
+                                                                   nullptr, codes, ix, sp, mb, n_min, n_anchor, err);
 }
 
-void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* n_min,
-                      const int64_t* anchor_off, MinBuf mb, const DevIndex& ix, const ChainParamsDev& cp,
-                      const CandParams& cand, AnchorScratch as, CandBuf cb, uint32_t* err) {
+void launch_seed_list(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+                      const int32_t* seq_len, const int64_t* pofs, int64_t n_max, const int32_t* list,
+                      const int* list_n, uint8_t* codes, const DevIndex& ix, const SeedParams& sp, MinBuf mb,
+                      int32_t* n_min, int64_t* n_anchor, uint32_t* err) {
+  if (n_max <= 0) return;
+  // grid-stride over a list whose length is only known on the device: a few resident waves
+  const int64_t blocks = std::min<int64_t>((n_max + kSeedWarps - 1) / kSeedWarps, 148 * 8);
+  k_seed<<<static_cast<unsigned>(blocks), kSeedWarps * 32, 0, st>>>(seq, seq_off, seq_base, seq_len, pofs, n_max,
+                                                                   list, list_n, codes, ix, sp, mb, n_min, n_anchor,
+                                                                   err);
+}
+
+void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* list,
+                      const int32_t* n_min, const int64_t* anchor_off, MinBuf mb, const DevIndex& ix,
+                      const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as, CandBuf cb, uint32_t* err) {
   if (n <= 0) return;
   const int64_t blocks = (n + kChainWarps - 1) / kChainWarps;
-  k_chain_map<<<static_cast<unsigned>(blocks), kChainWarps * 32, 0, st>>>(pofs, seq_len, n, n_min, anchor_off, mb, ix,
-                                                                         cp, cand, as, cb, err);
+  k_chain_map<<<static_cast<unsigned>(blocks), kChainWarps * 32, 0, st>>>(pofs, seq_len, n, list, n_min, anchor_off,
+                                                                         mb, ix, cp, cand, as, cb, err);
 }
 
 void launch_sketch_codes(cudaStream_t st, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,

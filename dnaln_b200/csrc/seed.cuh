@@ -30,6 +30,51 @@ __device__ __forceinline__ bool genome_has_n(const DevIndex& ix, int64_t a, int6
   return lo < ix.n_n_runs && static_cast<int64_t>(ix.n_runs[lo].x) < b;
 }
 
+// hash64 for 2k <= 32: every step is either reduced mod 2^32 and then masked to 2k bits,
+// or a right shift of a value below 2^2k, so 32-bit arithmetic gives the same bits.
+__device__ __forceinline__ uint32_t hash32(uint32_t key, uint32_t mask) {
+  key = (~key + (key << 21)) & mask;
+  key = key ^ key >> 24;
+  key = ((key + (key << 3)) + (key << 8)) & mask;
+  key = key ^ key >> 14;
+  key = ((key + (key << 2)) + (key << 4)) & mask;
+  key = key ^ key >> 28;
+  key = (key + (key << 31)) & mask;
+  return key;
+}
+
+// Probes the table for key h (src/index.hpp:24-38): off/cnt of its position list, cnt = 0
+// when absent. The table is at most half full, so an empty bucket always ends the walk;
+// the loop bound only guards a corrupted table.
+__device__ __forceinline__ void probe(const DevIndex& ix, uint64_t h, uint32_t& off, uint32_t& cnt,
+                                      uint32_t* err) {
+  uint64_t i = h & ix.mask;
+  off = 0;
+  cnt = 0;
+  for (uint64_t it = 0; it <= ix.mask; ++it) {  // load <= 0.5: an empty bucket always ends the walk
+    const ulonglong2 b = __ldg(ix.table + i);
+    if (b.x == h) {
+      off = static_cast<uint32_t>(b.y);
+      cnt = static_cast<uint32_t>(b.y >> 32);
+      return;
+    }
+    if (b.x == kInvalidHash) return;
+    i = (i + 1) & ix.mask;
+  }
+  atomicOr(err, kErrProbeLoop);
+}
+
+// Contig holding genome position gpos (src/reference.cpp:25-32).
+__device__ __forceinline__ int contig_of(const DevIndex& ix, uint64_t gpos) {
+  int64_t lo = 0, hi = ix.n_contigs;
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) / 2;
+    if (ix.contig_off[mid] <= gpos) lo = mid;
+    else hi = mid;
+  }
+  return static_cast<int>(lo);
+}
+
 struct SeedParams {
   int32_t k, w;
   uint32_t max_occ;
@@ -74,18 +119,37 @@ struct CandBuf {
   int64_t* wstart;
 };
 
-// Pass 1 of a read batch: encode the ASCII read seq[seq_off[r], + seq_len[r]) to codes
-// (forward at 2*pofs[r], reverse complement right after it; pofs = exclusive prefix of
-// the lengths), sketch, probe (minimizer slots at pofs[r]); writes n_min[r] and
-// n_anchor[r].
-void launch_seed(cudaStream_t st, const char* seq, const int64_t* seq_off, const int32_t* seq_len,
+// Pass 1 of a read batch: encode the ASCII read seq[seq_off[r] - seq_base, + seq_len[r])
+// to codes (forward at 2*pofs[r], reverse complement right after it; pofs = exclusive
+// prefix of the lengths), sketch, probe (minimizer slots at pofs[r]); writes n_min[r] and
+// n_anchor[r]. seq_base lets a sub-batch staged on the device keep the caller's offsets.
+void launch_seed(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base, const int32_t* seq_len,
                  const int64_t* pofs, int64_t n, uint8_t* codes, const DevIndex& ix, const SeedParams& sp, MinBuf mb,
                  int32_t* n_min, int64_t* n_anchor, uint32_t* err);
 
+// Pass 1 for the reads list[0, *list_n) only (n_max >= *list_n), codes already written.
+void launch_seed_list(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+                      const int32_t* seq_len, const int64_t* pofs, int64_t n_max, const int32_t* list,
+                      const int* list_n, uint8_t* codes, const DevIndex& ix, const SeedParams& sp, MinBuf mb,
+                      int32_t* n_min, int64_t* n_anchor, uint32_t* err);
+
 // Pass 2: anchors, chaining, candidates. anchor_off = exclusive prefix of n_anchor (n+1).
-void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* n_min,
-                      const int64_t* anchor_off, MinBuf mb, const DevIndex& ix, const ChainParamsDev& cp,
-                      const CandParams& cand, AnchorScratch as, CandBuf cb, uint32_t* err);
+// With a list, the reads list[0, n) instead of [0, n).
+void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* list,
+                      const int32_t* n_min, const int64_t* anchor_off, MinBuf mb, const DevIndex& ix,
+                      const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as, CandBuf cb, uint32_t* err);
+
+// One thread per read (seed_thread.cu): passes 1 and 2 of the reads the per-thread budgets
+// admit, writing codes of every read, candidates of the admitted ones, n_min and
+// n_anchor = 0; the others are appended to big_list (count in *big_n, zeroed by the caller)
+// for launch_seed_list / launch_chain_map. Returns false, launching nothing, when the
+// parameters are outside the path's range.
+bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp);
+bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+                              const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes,
+                              const DevIndex& ix, const SeedParams& sp, const ChainParamsDev& cp,
+                              const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
+                              int32_t* big_list, int* big_n, uint32_t* err);
 
 // Stage entry points: sketch of code sequences, lookups, chaining of given anchor sets.
 void launch_sketch_codes(cudaStream_t st, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,

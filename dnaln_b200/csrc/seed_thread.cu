@@ -1,0 +1,387 @@
+// seed_thread.cu — one thread per read: sketch, probe, anchors, chaining DP, chain
+// extraction and candidate loci of a short read, in one pass with the read's whole state
+// in shared memory (sm_100a).
+//
+// The warp-per-read kernels of seed.cu spend most of their instructions on warp
+// collectives (ballots, shuffles, reductions) over reads whose work is a few dozen
+// sequential steps. Here each thread owns a read and runs the reference's sequential
+// algorithms directly; the 32 reads of a warp advance in lockstep (same k-mer index, same
+// DP row), so the shared-memory layouts [slot][thread] are bank-conflict free.
+//
+//  * Staging: the warp encodes its 32 reads cooperatively (coalesced ASCII loads, forward
+//    and reverse-complement codes written coalesced, src/mapper.cpp:88-99) and leaves each
+//    read's codes, four per word, in shared memory for its thread.
+//  * Sketch (src/minimizer.cpp:5-68): rolling 2-bit forward / reverse-complement words,
+//    canonical strand, 32-bit hash (hash32); the window minimum of w keys (hash, position,
+//    strand) by van Herk / Gil-Werman blocks of w: a running prefix minimum of the current
+//    block and the suffix minima of the previous one, so each window costs one compare.
+//    Emission follows the same local rule as the warp sketch (emit unless the previous
+//    window was full and valid and picked the same position).
+//  * Probe (src/index.hpp:24-38) in groups of four independent bucket loads; anchors
+//    (src/mapper.cpp:32-40) in minimizer x occurrence order.
+//  * Chaining (src/chain.cpp:12-69): the anchors are sorted as 64-bit keys (insertion sort
+//    after reversing a descending run, which is how reverse-strand anchors arrive), the DP
+//    scans j = i-1 down with the reference's break / skip rules and strict '>'. Extraction
+//    repeatedly walks from the unused anchor of largest f (ties: smallest index): every
+//    walk of the reference's (f desc, index asc) loop starts at exactly that anchor, since
+//    all anchors before it in that order are used. Chains are taken in (score desc,
+//    extraction order) order, which is the reference's stable_sort.
+//  * Candidates (src/mapper.cpp:40-62).
+//
+// A read leaves this path — listed for the warp kernels, which recompute it from scratch —
+// when it is longer than kTMaxLen, has more than kTMaxMin minimizers, kTMaxAnc anchors or
+// kTMaxChains chains, or when the parameters are outside this path's range (see
+// seed_thread_supported).
+#include "common.cuh"
+#include "seed.cuh"
+
+namespace dnb {
+
+namespace {
+
+constexpr int kTT = 128;                  // threads (= reads) per block
+constexpr int kTMaxLen = 256;             // longest read staged
+constexpr int kTWords = kTMaxLen / 4;     // staged code words per read
+constexpr int kTPitch = kTT + 1;          // word pitch of the staging layout (spreads banks)
+constexpr int kTMaxMin = 32;              // minimizers per read
+constexpr int kTMaxAnc = 32;              // anchors per read (one bit each in a 32-bit mask)
+constexpr int kTMaxChains = 8;            // chains per read passing the score / anchor filters
+constexpr int kTW = 10;                   // window length of the compiled sketch
+
+// Dynamic shared memory of a block: two regions of 32-bit words, each thread owning one
+// column of each (word w of thread T at w * pitch + T), so that after the cooperative
+// encode no thread ever touches another thread's words. Region A (pitch kTPitch): the
+// staged codes, later the anchor keys (two words each). Region B (pitch kTT): the
+// minimizers {hash, pos | strand << 31} (two words each), later f << 8 | (prev + 1) of
+// each anchor (words 0..31) and the chain table (words 32..63).
+constexpr int kWordsA = kTWords;
+constexpr int kWordsB = 64;
+static_assert(2 * kTMaxAnc <= kWordsA, "anchor keys must fit a staging column");
+static_assert(2 * kTMaxMin <= kWordsB && kTMaxAnc + 4 * kTMaxChains <= kWordsB, "region B column too small");
+constexpr int kRegionA = kWordsA * kTPitch * 4;
+constexpr int kRegionB = kWordsB * kTT * 4;
+constexpr int kThreadSmem = kRegionA + kRegionB;
+
+__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return b < a ? b : a; }
+
+template <int W>
+__global__ void __launch_bounds__(kTT)
+    k_seed_chain_t(const char* __restrict__ seq, const int64_t* __restrict__ seq_off, int64_t seq_base,
+                   const int32_t* __restrict__ seq_len, const int64_t* __restrict__ pofs, int64_t n,
+                   uint8_t* __restrict__ codes, DevIndex ix, SeedParams sp, ChainParamsDev cp, CandParams cand,
+                   CandBuf cb, int32_t* __restrict__ n_min, int64_t* __restrict__ n_anchor,
+                   int32_t* __restrict__ big_list, int* __restrict__ big_n, uint32_t* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* const stg = reinterpret_cast<uint32_t*>(smem);  // region A (all columns, for the encode)
+  const int T = threadIdx.x, lane = T & 31;
+  uint32_t* const ca = stg + T;                                                   // this thread's A column
+  uint32_t* const cbw = reinterpret_cast<uint32_t*>(smem + kRegionA) + T;         // this thread's B column
+  const auto key_ld = [&](int a) {
+    return static_cast<uint64_t>(ca[(2 * a + 1) * kTPitch]) << 32 | ca[2 * a * kTPitch];
+  };
+  const auto key_st = [&](int a, uint64_t v) {
+    ca[2 * a * kTPitch] = static_cast<uint32_t>(v);
+    ca[(2 * a + 1) * kTPitch] = static_cast<uint32_t>(v >> 32);
+  };
+  const auto fp_at = [&](int i) -> int32_t& { return reinterpret_cast<int32_t&>(cbw[i * kTT]); };
+  const auto ch_at = [&](int field, int c) -> int32_t& {
+    return reinterpret_cast<int32_t&>(cbw[(kTMaxAnc + field * kTMaxChains + c) * kTT]);
+  };
+
+  const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kTT + (T & ~31);  // first read of this warp
+  const int64_t r = r0 + lane;
+  int len = 0;
+  int64_t soff = 0, po = 0;
+  if (r < n) {
+    len = seq_len[r];
+    soff = seq_off[r] - seq_base;
+    po = pofs[r];
+  }
+
+  // ---- cooperative encode: codes of both strands to HBM, staged codes to shared memory
+  for (int j = 0; j < 32; ++j) {
+    if (r0 + j >= n) break;
+    const int lj = __shfl_sync(0xffffffffu, len, j);
+    const int64_t sj = __shfl_sync(0xffffffffu, soff, j);
+    const int64_t pj = __shfl_sync(0xffffffffu, po, j);
+    const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + sj;
+    uint8_t* fw = codes + 2 * pj;
+    uint8_t* rc = fw + lj;
+    uint8_t* st8 = reinterpret_cast<uint8_t*>(stg);
+    const int tj = (T & ~31) + j;
+    const bool stage = lj <= kTMaxLen;
+    for (int i = lane; i < lj; i += 32) {
+      const uint8_t c = static_cast<uint8_t>(nt4(s[i]));
+      fw[i] = c;
+      rc[lj - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
+      if (stage) st8[((i >> 2) * kTPitch + tj) * 4 + (i & 3)] = c;
+    }
+  }
+  __syncwarp();
+  if (r >= n) return;
+
+  const int k = sp.k;
+  bool big = len > kTMaxLen;
+  int nmin = 0;
+  // ---- sketch (src/minimizer.cpp:5-68)
+  if (!big && len >= k) {
+    const uint32_t mask2k = (1u << (2 * k)) - 1u;
+    const int nk = len - k + 1;
+    uint32_t fwd = 0, rev = 0, wcur = 0;
+    int run = 0;
+    auto roll = [&](int i) {  // consumes code i (called with i = 0, 1, 2, ...)
+      if ((i & 3) == 0) wcur = ca[(i >> 2) * kTPitch];
+      const uint32_t c = (wcur >> (8 * (i & 3))) & 0xFFu;
+      run = c < 4 ? run + 1 : 0;
+      fwd = ((fwd << 2) | (c & 3u)) & mask2k;
+      rev = (rev >> 2) | ((3u - (c & 3u)) << (2 * k - 2));
+    };
+    for (int i = 0; i < k - 1; ++i) roll(i);
+    uint64_t cur[W], suf[W];
+#pragma unroll
+    for (int u = 0; u < W; ++u) suf[u] = ~0ULL;
+    uint64_t pre = ~0ULL;
+    int lastbad = -1, prev_arg = -1;
+    for (int s0 = 0; s0 < nk; s0 += W) {
+#pragma unroll
+      for (int u = 0; u < W; ++u) {
+        const int s = s0 + u;
+        cur[u] = ~0ULL;
+        if (s < nk) {
+          roll(s + k - 1);
+          uint64_t key = ~0ULL;
+          if (run >= k) {
+            const uint32_t st = rev < fwd;
+            const uint32_t h = fwd != rev ? hash32(st ? rev : fwd, mask2k) : 0xFFFFFFFFu;
+            key = static_cast<uint64_t>(h) << 32 | static_cast<uint32_t>(s) << 1 | st;
+          } else {
+            lastbad = s;
+          }
+          cur[u] = key;
+          pre = u == 0 ? key : umin64(pre, key);
+          // window [s - W + 1, s]: suffix of the previous block from u + 1, prefix of this one
+          const uint64_t m = u + 1 < W ? umin64(suf[u + 1 < W ? u + 1 : 0], pre) : pre;
+          int arg = -1;
+          if (s >= W - 1 && lastbad < s - W + 1 && static_cast<uint32_t>(m >> 32) != 0xFFFFFFFFu)
+            arg = static_cast<int>(static_cast<uint32_t>(m) >> 1);
+          if (arg >= 0 && arg != prev_arg) {
+            if (nmin < kTMaxMin) {
+              cbw[2 * nmin * kTT] = static_cast<uint32_t>(m >> 32);
+              cbw[(2 * nmin + 1) * kTT] = static_cast<uint32_t>(arg) | (static_cast<uint32_t>(m) & 1u) << 31;
+            }
+            ++nmin;
+          }
+          prev_arg = arg;
+        }
+      }
+      // suffix minima of this block for the next one
+      suf[W - 1] = cur[W - 1];
+#pragma unroll
+      for (int u = W - 2; u >= 0; --u) suf[u] = umin64(cur[u], suf[u + 1]);
+    }
+    if (nmin > kTMaxMin) big = true;
+  }
+
+  // ---- probe and anchors (src/mapper.cpp:16-40); region A becomes the anchor keys
+  int na = 0;
+  if (!big) {
+    for (int j0 = 0; j0 < nmin && !big; j0 += 4) {
+      uint2 m[4];
+      ulonglong2 b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        m[q] = make_uint2(0, 0);
+        b[q] = make_ulonglong2(kInvalidHash, 0);
+        if (j0 + q < nmin) {
+          m[q] = make_uint2(cbw[2 * (j0 + q) * kTT], cbw[(2 * (j0 + q) + 1) * kTT]);
+          b[q] = __ldg(ix.table + (static_cast<uint64_t>(m[q].x) & ix.mask));
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (j0 + q >= nmin || big) break;
+        const uint64_t h = m[q].x;
+        uint32_t off = 0, cnt = 0;
+        if (b[q].x == h) {
+          off = static_cast<uint32_t>(b[q].y);
+          cnt = static_cast<uint32_t>(b[q].y >> 32);
+        } else if (b[q].x != kInvalidHash) {
+          probe(ix, h, off, cnt, err);  // a collision in the first bucket: walk on
+        }
+        if (cnt > sp.max_occ) cnt = 0;
+        if (cnt == 0) continue;
+        if (na + static_cast<int>(cnt) > kTMaxAnc) {
+          big = true;
+          break;
+        }
+        const int32_t pos = static_cast<int32_t>(m[q].y & 0x7FFFFFFFu);
+        const uint32_t mst = m[q].y >> 31;
+        for (uint32_t t = 0; t < cnt; ++t) {
+          const uint32_t v = __ldg(ix.positions + off + t);
+          const uint32_t rv = (v & 1u) ^ mst;
+          const int32_t qpos = rv ? len - pos - k : pos;
+          key_st(na, anchor_key(rv, v >> 1, qpos));
+          ++na;
+        }
+      }
+    }
+  }
+
+  int nd = 0;
+  if (!big && na > 0) {
+    // ---- sort the anchor keys ascending (src/chain.cpp:16-20; keys are unique)
+    if (key_ld(0) > key_ld(na - 1)) {
+      for (int a = 0, b2 = na - 1; a < b2; ++a, --b2) {
+        const uint64_t x = key_ld(a);
+        key_st(a, key_ld(b2));
+        key_st(b2, x);
+      }
+    }
+    for (int i = 1; i < na; ++i) {
+      const uint64_t x = key_ld(i);
+      int j = i - 1;
+      while (j >= 0) {
+        const uint64_t y = key_ld(j);
+        if (y <= x) break;
+        key_st(j + 1, y);
+        --j;
+      }
+      key_st(j + 1, x);
+    }
+    // ---- DP (src/chain.cpp:22-45); region B becomes f << 8 | (prev + 1)
+    for (int i = 0; i < na; ++i) {
+      const uint64_t ki = key_ld(i);
+      const uint32_t si = key_strand(ki), ri = key_rpos(ki);
+      const int32_t qi = key_qpos(ki);
+      int best = k, bj = -1;
+      const int lo = i - cp.lookback > 0 ? i - cp.lookback : 0;
+      for (int j = i - 1; j >= lo; --j) {
+        const uint64_t kj = key_ld(j);
+        if (key_strand(kj) != si) break;
+        const int64_t dr = static_cast<int64_t>(ri) - key_rpos(kj);
+        if (dr > cp.max_gap) break;
+        const int32_t dq = qi - key_qpos(kj);
+        if (dr <= 0 || dq <= 0) continue;
+        const int64_t dd = dr > dq ? dr - dq : dq - dr;
+        if (dd > cp.band) continue;
+        int g = dq < dr ? dq : static_cast<int>(dr);
+        if (g > k) g = k;
+        const int sc = (fp_at(j) >> 8) + g - __ldg(cp.cost + dd);
+        if (sc > best) {
+          best = sc;
+          bj = j;
+        }
+      }
+      fp_at(i) = best << 8 | (bj + 1);
+    }
+    // ---- chains (src/chain.cpp:47-68)
+    uint32_t used = 0;
+    int nch = 0;
+    for (;;) {
+      int end = -1, bf = INT_MIN;
+      for (int i = 0; i < na; ++i) {
+        const int f = fp_at(i) >> 8;
+        if (!((used >> i) & 1u) && f > bf) {
+          bf = f;
+          end = i;
+        }
+      }
+      if (end < 0) break;
+      int i = end, cnt = 0;
+      int32_t dmin = INT_MAX, dmax = INT_MIN;
+      while (i >= 0 && !((used >> i) & 1u)) {
+        used |= 1u << i;
+        ++cnt;
+        const uint64_t key = key_ld(i);
+        const int32_t d = static_cast<int32_t>(key_rpos(key)) - key_qpos(key);
+        dmin = d < dmin ? d : dmin;
+        dmax = d > dmax ? d : dmax;
+        i = (fp_at(i) & 0xFF) - 1;
+      }
+      const int score = bf - (i >= 0 ? (fp_at(i) >> 8) : 0);
+      if (score < cp.min_score || cnt < cp.min_anchors) continue;
+      if (nch == kTMaxChains) {
+        big = true;
+        break;
+      }
+      const uint64_t ke = key_ld(end);
+      ch_at(0, nch) = score;
+      ch_at(1, nch) = static_cast<int32_t>(key_strand(ke));
+      ch_at(2, nch) = dmin + (dmax - dmin) / 2;
+      ch_at(3, nch) = static_cast<int32_t>(key_rpos(ke));
+      ++nch;
+    }
+    // ---- candidate loci (src/mapper.cpp:40-62), chains by (score desc, extraction order)
+    if (!big && nch > 0) {
+      const int64_t cbase = r * cand.max_cand;
+      int last_s = INT_MAX, last_i = -1;
+      double min_score = 0.0;
+      for (int c = 0; c < nch; ++c) {
+        int bi = -1, bs = INT_MIN;
+        for (int x = 0; x < nch; ++x) {
+          const int s = ch_at(0, x);
+          if ((s < last_s || (s == last_s && x > last_i)) && s > bs) {
+            bs = s;
+            bi = x;
+          }
+        }
+        last_s = bs;
+        last_i = bi;
+        if (c == 0) min_score = static_cast<double>(bs) * cand.pri_ratio;
+        if (static_cast<double>(bs) < min_score || nd >= cand.max_cand) break;
+        const uint8_t strand = static_cast<uint8_t>(ch_at(1, bi));
+        const int64_t diag = ch_at(2, bi);
+        bool dup = false;
+        for (int x = 0; x < nd && !dup; ++x) {
+          const int64_t dd = cb.diag[cbase + x] - diag;
+          dup = cb.rev[cbase + x] == strand && (dd < 0 ? -dd : dd) <= cand.bw;
+        }
+        if (dup) continue;
+        cb.rev[cbase + nd] = strand;
+        cb.contig[cbase + nd] = contig_of(ix, static_cast<uint32_t>(ch_at(3, bi)));
+        cb.diag[cbase + nd] = diag;
+        cb.wstart[cbase + nd] = diag - cand.bw;
+        ++nd;
+      }
+    }
+  }
+  n_anchor[r] = 0;  // no anchor scratch: this read either finished here or is listed below
+  if (big) {
+    n_min[r] = 0;
+    big_list[atomicAdd(big_n, 1)] = static_cast<int32_t>(r);
+    return;
+  }
+  n_min[r] = nmin;
+  cb.n_cand[r] = nd;
+}
+
+}  // namespace
+
+bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp) {
+  return sp.w == kTW && sp.k >= 4 && sp.k <= 15 && cp.max_gap >= 0 && cp.max_gap < (1 << 29) && cp.band >= 0 &&
+         cp.lookback >= 0;
+}
+
+bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+                              const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes,
+                              const DevIndex& ix, const SeedParams& sp, const ChainParamsDev& cp,
+                              const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
+                              int32_t* big_list, int* big_n, uint32_t* err) {
+  if (!seed_thread_supported(sp, cp)) return false;
+  if (n <= 0) return true;
+  static bool attr_set[64] = {};  // per device
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+  if (!attr_set[dev]) {
+    if (cudaFuncSetAttribute(k_seed_chain_t<kTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, kThreadSmem) !=
+        cudaSuccess)
+      return false;
+    attr_set[dev] = true;
+  }
+  const int64_t blocks = (n + kTT - 1) / kTT;
+  k_seed_chain_t<kTW><<<static_cast<unsigned>(blocks), kTT, kThreadSmem, st>>>(
+      seq, seq_off, seq_base, seq_len, pofs, n, codes, ix, sp, cp, cand, cb, n_min, n_anchor, big_list, big_n, err);
+  return true;
+}
+
+}  // namespace dnb

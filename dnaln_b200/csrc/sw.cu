@@ -48,6 +48,7 @@ constexpr int kSwThreads = 128;
 constexpr uint32_t kNotDiagE = 8u, kFromF = 4u, kExtE = 2u, kExtF = 1u;
 constexpr uint32_t kBias = 16384u, kBias2 = 0x40004000u, kOne2 = 0x00010001u;
 constexpr int kScoreBias = 64;  // profile bytes are score + 64, in [0, 127]
+constexpr int kAhead = 8;       // cells of a diagonal run the walk fetches at once
 
 // prmt.b32 in its default mode (the sign-replicate bit of each selector nibble is
 // honoured; the __byte_perm intrinsic uses only the low 3 bits of each nibble).
@@ -163,15 +164,43 @@ __device__ void traceback(const Codes& code, int W, int bi, int bd, int best, co
   for (;;) {
     int run = 0;
     uint32_t x = 0;
-    while (i >= 0 && v > 0) {
-      x = code(i, d);
-      if (x & (kNotDiagE | kFromF)) break;  // not from the diagonal
-      const int a = q[i];
-      const int b = static_cast<int>(tcode(tbase, tk, static_cast<int64_t>(i) + d));
-      v -= sub_score(p, a, b);
-      nm += (a != b || a > 3) ? 1 : 0;
-      ++run;
-      --i;
+    if (i >= 0 && v > 0 && (d < 0 || d >= W)) {
+      atomicOr(err, kErrTracebackBounds);
+      break;
+    }
+    // Diagonal run. The next kAhead cells (i-k, d) are fetched together (codes, query and
+    // target bases: independent loads, one memory latency per kAhead steps) and then
+    // consumed in order exactly as the one-cell-at-a-time walk would.
+    bool stop = false;
+    while (!stop && i >= 0 && v > 0) {
+      uint32_t cx[kAhead];
+      int qa[kAhead], ta[kAhead];
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) {
+        cx[k] = 0;
+        qa[k] = ta[k] = 0;
+        if (i - k >= 0) {
+          cx[k] = code(i - k, d);
+          qa[k] = q[i - k];
+          ta[k] = static_cast<int>(tcode(tbase, tk, static_cast<int64_t>(i - k) + d));
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) {
+        if (i < 0 || v <= 0) {
+          stop = true;
+          break;
+        }
+        x = cx[k];
+        if (x & (kNotDiagE | kFromF)) {  // not from the diagonal
+          stop = true;
+          break;
+        }
+        v -= sub_score(p, qa[k], ta[k]);
+        nm += (qa[k] != ta[k] || qa[k] > 3) ? 1 : 0;
+        ++run;
+        --i;
+      }
     }
     if (run) cw.push(0u /* M */, run);
     if (i < 0 || v <= 0) break;
@@ -542,21 +571,33 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_any(const SwTask* __restrict_
 template <int W>
 void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int count, int n, const int* n_dev,
                const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res, uint32_t* dir,
-               int rows_max, uint32_t* cig, const int64_t* cig_off, int* fb, uint32_t* err) {
+               int rows_max, uint32_t* cig, const int64_t* cig_off, int* fb, uint32_t* err, const KernelTrace* kt) {
   const int pairs = (count + 1) / 2;
   const int blocks_pairs = (pairs + kSwThreads - 1) / kSwThreads;
   const int blocks_tasks = (count + kSwThreads - 1) / kSwThreads;
+  const KernelTrace none;
+  const KernelTrace& t = kt ? *kt : none;
   cudaMemsetAsync(fb, 0, sizeof(int), st);
   if (tb) {
+    t.begin(st, "k_sw_u2<tb>");
     k_sw_u2<W, true><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max,
                                                           fb);
+    t.end(st);
+    t.begin(st, "k_sw_fb<tb>");
     k_sw_fb<W, true><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    t.end(st);
+    t.begin(st, "k_sw_walk");
     k_sw_walk<W><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, count, n, n_dev, qbase, tbase, p, res, dir,
                                                       rows_max, cig, cig_off, err);
+    t.end(st);
   } else {
+    t.begin(st, "k_sw_u2<score>");
     k_sw_u2<W, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max,
                                                            fb);
+    t.end(st);
+    t.begin(st, "k_sw_fb<score>");
     k_sw_fb<W, false><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    t.end(st);
   }
 }
 
@@ -597,7 +638,7 @@ int sw_launches(int W, bool bytes_ok, bool tb) { return sw_uses_generic(W, bytes
 bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int base, int count, int n,
                const int* n_dev, const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res,
                uint32_t* dir, int rows_max, uint32_t* cig, const int64_t* cig_off, int* band, int* fb,
-               uint32_t* err) {
+               uint32_t* err, const KernelTrace* kt) {
   if (count <= 0) return true;
   const bool generic = sw_uses_generic(p.W, bytes_ok);
   if ((tb && !dir) || (generic && !band) || (!generic && !fb) || (base % kSwTaskGroup) != 0) return false;
@@ -605,7 +646,7 @@ bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int
 #define DNB_SW_U2(WV)                                                                                       \
   case WV:                                                                                                  \
     launch_u2<WV>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, \
-                  fb, err);                                                                                 \
+                  fb, err, kt);                                                                             \
     return true;
     switch (p.W) {
       DNB_SW_U2(11)
@@ -618,12 +659,14 @@ bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int
 #undef DNB_SW_U2
   }
   const int blocks = (count + kSwThreads - 1) / kSwThreads;
+  if (kt) kt->begin(st, tb ? "k_sw_any<tb>" : "k_sw_any<score>");
   if (tb)
     k_sw_any<true><<<blocks, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig,
                                                  cig_off, band, err);
   else
     k_sw_any<false><<<blocks, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig,
                                                   cig_off, band, err);
+  if (kt) kt->end(st);
   return true;
 }
 

@@ -30,11 +30,12 @@ int sw_launches(int W, bool bytes_ok, bool tb);
 // cig_off[task.slot], capacity 2*qlen+1. base must be a multiple of kSwTaskGroup; `dir`
 // and `band` must hold count rounded up to kSwTaskGroup tasks of
 // sw_dir_bytes_per_task(W, rows_max) and sw_band_bytes_per_task(W, bytes_ok); `fb`
-// (count + 1 ints) lists the tasks the 16-bit kernel hands to the int32 one. Returns
-// false, launching nothing, when a needed scratch pointer is null or base is misaligned.
+// (count + 1 ints) lists the tasks the 16-bit kernel hands to the int32 one; kt (may be
+// null) times each kernel. Returns false, launching nothing, when a needed scratch pointer
+// is null or base is misaligned.
 bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int base, int count, int n,
                const int* n_dev, const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res,
                uint32_t* dir, int rows_max, uint32_t* cig, const int64_t* cig_off, int* band, int* fb,
-               uint32_t* err);
+               uint32_t* err, const KernelTrace* kt);
 
 }  // namespace dnb

@@ -100,7 +100,30 @@ const char* dnaln_gpu_last_error(const dnaln_ctx* ctx);
 /* Launch on `stream` (a cudaStream_t) instead of the context's own stream; NULL restores it. */
 int dnaln_gpu_set_stream(dnaln_ctx* ctx, void* stream);
 int dnaln_gpu_get_stats(const dnaln_ctx* ctx, dnaln_stats* out);
+/* Clears the counters and the kernel-time totals. */
 int dnaln_gpu_reset_stats(dnaln_ctx* ctx);
+
+/* Per-kernel timing (no reference counterpart; the reference reports stage totals in
+ * MapStats, src/mapper.hpp:46-52). When on, every kernel launch of the context is
+ * bracketed by a CUDA event pair on its stream and totals accumulate per kernel name;
+ * `only` (may be NULL) restricts the trace to the kernel of that name, so that timing one
+ * kernel inside a timed loop adds one event pair per launch of it and nothing else. */
+typedef struct dnaln_kernel_time {
+  char name[48];
+  int64_t launches;
+  double ms;
+} dnaln_kernel_time;
+int dnaln_gpu_set_kernel_trace(dnaln_ctx* ctx, int32_t on, const char* only);
+/* Writes min(cap, count) entries; *n_out = count of traced kernel names. */
+int dnaln_gpu_kernel_times(const dnaln_ctx* ctx, dnaln_kernel_time* out, int32_t cap, int32_t* n_out);
+/* Reads per sub-batch of dnaln_gpu_map_batch (default 65536; 0 = whole batch at once). */
+int dnaln_gpu_set_sub_batch(dnaln_ctx* ctx, int64_t reads);
+/* Tuning switches (none changes any result):
+ *   "sub_batch"      same as dnaln_gpu_set_sub_batch;
+ *   "warp_seed_only" 1 = seed and chain every read one warp per read (default 0: short
+ *                    reads one thread per read, the others one warp per read);
+ *   "dir_cap_bytes"  traceback direction-code scratch per launch (default 1 GiB). */
+int dnaln_gpu_set_option(dnaln_ctx* ctx, const char* name, int64_t value);
 /* Page-locked host buffers for fast transfers (pass to the *_batch calls). */
 int dnaln_gpu_host_alloc(dnaln_ctx* ctx, size_t bytes, void** out);
 int dnaln_gpu_host_free(dnaln_ctx* ctx, void* p);
@@ -176,8 +199,11 @@ int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_off, const in
 /* ---- whole batch: Mapper::map (src/mapper.cpp:75-223) --------------------------------
  * n reads, ASCII, read r = seq[seq_off[r] .. + seq_len[r]); name_hash[r] = FNV-1a of the
  * read name (src/common.hpp:136-140, dnaln_fnv1a below), the tie-break between equal
- * best candidates. Records go to out[r]; CIGARs to `cigar` (capacity cigar_cap ops,
- * DNALN_ERR_CAPACITY with *cigar_used = needed if short; sum of 2*len+3 suffices). */
+ * best candidates. Records go to out[r]; CIGARs to `cigar` (capacity cigar_cap ops;
+ * the sum over reads of 2*len+3 always suffices; DNALN_ERR_CAPACITY if it is short).
+ * The host-buffer call streams the batch through the device in sub-batches (see
+ * dnaln_gpu_set_sub_batch), overlapping copies with compute; page-locked buffers
+ * (dnaln_gpu_host_alloc) make the copies asynchronous. */
 int dnaln_gpu_map_batch(dnaln_ctx* ctx, int32_t index_id, const char* seq, const int64_t* seq_off,
                         const int32_t* seq_len, const uint32_t* name_hash, int64_t n, const dnaln_map_params* p,
                         dnaln_map_record* out, uint32_t* cigar, int64_t cigar_cap, int64_t* cigar_used);

@@ -121,6 +121,63 @@ def test_batch_invariance(ctx, repeat):
         ctx.index_free(iid)
 
 
+@pytest.mark.parametrize("wl", ["repeat", "mixed", "small"])
+def test_thread_and_warp_seed_paths_identical(ctx, request, wl):
+    # short reads are seeded and chained one thread per read, the others (long, or past a
+    # per-thread budget) one warp per read; forcing every read through the warp kernels
+    # must give the same records and CIGARs
+    g, reads, _ = request.getfixturevalue(wl)
+    p = D.default_map_params()
+    iid = ctx.index_build(g)
+    try:
+        mixed_path = ctx.map_batch(iid, reads, p)
+        ctx.set_option("warp_seed_only", 1)
+        warp_path = ctx.map_batch(iid, reads, p)
+    finally:
+        ctx.set_option("warp_seed_only", 0)
+        ctx.index_free(iid)
+    assert np.array_equal(gpu_records(mixed_path), gpu_records(warp_path))
+    assert np.array_equal(mixed_path.records["cigar_len"], warp_path.records["cigar_len"])
+    assert np.array_equal(mixed_path.cigar, warp_path.cigar)
+
+
+@pytest.mark.parametrize("sub_batch", [0, 997, 4096])
+def test_sub_batch_pipeline_identical(ctx, repeat, sub_batch):
+    # the host-buffer call streams sub-batches through two device slots; records and
+    # CIGARs must not depend on the split, also when reads sit out of order in the buffer
+    from dnaln_b200 import _native as N
+    g, reads, _ = repeat
+    p = D.default_map_params()
+    iid = ctx.index_build(g)
+    try:
+        ctx.set_sub_batch(0)
+        whole = ctx.map_batch(iid, reads, p)
+        n = len(reads)
+        lens = np.ascontiguousarray(reads.seq_len)
+        order = np.random.default_rng(5).permutation(n)  # buffer layout: reads stored in this order
+        chunks = [reads.read(int(i)) for i in order]
+        buf = np.frombuffer(b"".join(chunks), np.uint8).copy()
+        pos = np.zeros(n, np.int64)
+        pos[order] = np.concatenate([[0], np.cumsum([len(x) for x in chunks])[:-1]])
+        nh = reads.name_hash()
+        rec = np.zeros(n, dtype=D.MAP_RECORD_DTYPE)
+        cap = int(np.sum(2 * lens.astype(np.int64) + 3))
+        cig = np.zeros(cap, np.uint32)
+        used = D.C.c_int64()
+        ctx.set_sub_batch(sub_batch)
+        rc = N.lib().dnaln_gpu_map_batch(ctx.handle, iid, N.ptr(buf), N.ptr(pos), N.ptr(lens), N.ptr(nh), n,
+                                         D.C.byref(p), N.ptr(rec), N.ptr(cig), cap, D.C.byref(used))
+        assert rc == 0, N.lib().dnaln_gpu_last_error(ctx.handle).decode()
+        got = D.MapResult(rec, cig[:used.value])
+        assert np.array_equal(gpu_records(got), gpu_records(whole))
+        for i in range(0, n, 97):
+            assert np.array_equal(got.cigar_of(i), whole.cigar_of(i))
+        assert used.value == len(whole.cigar)
+    finally:
+        ctx.set_sub_batch(65536)
+        ctx.index_free(iid)
+
+
 def test_empty_and_degenerate_reads(ctx, port, small):
     g, _, _ = small
     exact = np.frombuffer(b"ACGTN", np.uint8)[g.codes[5000:5150]].tobytes()  # an exact genome substring
