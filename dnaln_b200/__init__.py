@@ -349,6 +349,41 @@ class Context:
                                                   C.byref(p), ptr(rec), ptr(cig), cap, C.byref(used)))
         return MapResult(rec[:n], cig[:used.value])
 
+    def map_submit(self, iid: int, reads: ReadBatch, p: MapParams | None = None) -> "MapTicket":
+        """Queues Mapper::map over one batch and returns at once (dnaln_gpu_map_submit);
+        map_wait(ticket) returns its MapResult. Batches run in submission order, the copies of
+        one overlapping the kernels of the others."""
+        p = p or default_map_params()
+        n = len(reads)
+        lens = np.ascontiguousarray(reads.seq_len)
+        cap = int(np.sum(2 * lens.astype(np.int64) + 3)) if n else 0
+        t = MapTicket(n=n, params=p, keep=[reads.seq, np.ascontiguousarray(reads.seq_off[:-1]), lens,
+                                           reads.name_hash()],
+                      records=np.zeros(max(n, 1), dtype=MAP_RECORD_DTYPE), cigar=np.zeros(max(cap, 1), np.uint32))
+        tid = C.c_int64()
+        seq, off, ln, nh = t.keep
+        self._check(self._lib.dnaln_gpu_map_submit(self._h, iid, ptr(seq), ptr(off), ptr(ln), ptr(nh), n,
+                                                   C.byref(t.params), ptr(t.records), ptr(t.cigar), cap,
+                                                   C.byref(t.used), C.byref(tid)))
+        t.ticket = tid.value
+        return t
+
+    def map_wait(self, t: "MapTicket") -> MapResult:
+        self._check(self._lib.dnaln_gpu_map_wait(self._h, t.ticket))
+        return MapResult(t.records[:t.n], t.cigar[:t.used.value])
+
+
+@dataclass
+class MapTicket:
+    """A queued batch: keeps its host buffers alive until map_wait."""
+    n: int
+    params: MapParams
+    keep: list
+    records: np.ndarray
+    cigar: np.ndarray
+    used: C.c_int64 = field(default_factory=C.c_int64)
+    ticket: int = 0
+
 
 def sam_format(reads: ReadBatch, res: MapResult, genome: Genome) -> bytes:
     """SAM body lines of a mapped batch (Mapper::append_sam, src/mapper.cpp:231-270)."""

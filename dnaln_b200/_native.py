@@ -96,6 +96,9 @@ SIGNATURES = {
     "dnaln_gpu_kernel_times": (C.c_int, [P, C.POINTER(KernelTime), i32, C.POINTER(i32)]),
     "dnaln_gpu_set_sub_batch": (C.c_int, [P, i64]),
     "dnaln_gpu_set_option": (C.c_int, [P, C.c_char_p, i64]),
+    "dnaln_gpu_map_submit": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64, C.POINTER(i64),
+                             C.POINTER(i64)]),
+    "dnaln_gpu_map_wait": (C.c_int, [P, i64]),
     "dnaln_gpu_host_alloc": (C.c_int, [P, C.c_size_t, C.POINTER(P)]),
     "dnaln_gpu_host_free": (C.c_int, [P, P]),
     "dnaln_gpu_index_build": (C.c_int, [P, P, u64, P, P, i32, i32, i32, C.POINTER(i32)]),

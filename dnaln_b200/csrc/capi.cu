@@ -19,11 +19,15 @@
 #include <cub/device/device_scan.cuh>
 
 #include <cmath>
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -59,6 +63,25 @@ struct KernelTime {
   double ms = 0.0;
 };
 
+// One queued part of a host-buffer batch (dnaln_gpu_map_submit): reads [a, b) of the
+// caller's arrays, with the facts the host knows about them.
+struct MapPart {
+  int64_t ticket = 0;
+  bool last = false;  // last part of its ticket
+  int32_t index_id = 0;
+  const char* seq = nullptr;
+  const int64_t* seq_off = nullptr;
+  const int32_t* seq_len = nullptr;
+  const uint32_t* name_hash = nullptr;
+  int64_t a = 0, b = 0;
+  int64_t lo = 0, hi = 0, bases = 0, max_len = 0, cig_bound = 0;
+  dnaln_map_params p{};
+  dnaln_map_record* out = nullptr;
+  uint32_t* cigar = nullptr;
+  int64_t cigar_cap = 0;
+  int64_t* cigar_used = nullptr;
+};
+
 // Per-batch facts the caller may already know (host-buffer path), sparing a device read-back.
 struct BatchHints {
   int64_t seq_base = 0;    // subtracted from every read offset (sub-batch staged on the device)
@@ -85,7 +108,19 @@ struct dnaln_ctx {
   // pipelined host-buffer path: copy streams, per-slot events, sub-batch size (reads)
   cudaStream_t cp_in = nullptr, cp_out = nullptr;
   cudaEvent_t in_ready[2] = {}, out_free[2] = {}, h2d_ev[4] = {}, d2h_ev[4] = {};
-  int64_t sub_batch = 65536;
+  int64_t sub_batch = 0;
+  // submit / wait: queue of parts, a worker thread, finished tickets with their status
+  mutable std::mutex mu;  // held by the worker while it drives the device, and by every other entry point
+  std::mutex err_mu;      // the last error message (set by the worker and by callers)
+  std::mutex qmu;   // queue, tickets, results
+  std::condition_variable qcv;
+  std::deque<MapPart> queue;
+  std::map<int64_t, int> results;     // finished tickets -> status
+  std::map<int64_t, int> first_err;   // status of a ticket's first failed part
+  std::map<int64_t, int64_t> ticket_ops;  // CIGAR ops written so far per ticket
+  int64_t next_ticket = 1;
+  std::thread worker;
+  bool stop = false;
   bool warp_seed_only = false;  // option: every read through the warp-per-read seeding kernels
   // kernel trace: event pairs of the current batch, totals per kernel name
   bool trace_on = false, trace_open = false;
@@ -108,7 +143,10 @@ int fail(dnaln_ctx* c, int code, const char* fmt, ...) {
   va_start(ap, fmt);
   std::vsnprintf(buf, sizeof buf, fmt, ap);
   va_end(ap);
-  if (c) c->err = buf;
+  if (c) {
+    std::lock_guard<std::mutex> g(c->err_mu);
+    c->err = buf;
+  }
   return code;
 }
 
@@ -322,15 +360,21 @@ int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks,
   return DNALN_OK;
 }
 
-int validate_map_params(dnaln_ctx* c, const dnaln_map_params* p, const IndexRes& ix) {
+// Checks that need no index.
+int validate_map_params_basic(dnaln_ctx* c, const dnaln_map_params* p) {
   if (!p) return fail(c, DNALN_ERR_INVALID_ARG, "null map params");
   std::string why;
   if (!score_params_ok(p->sc, why)) return fail(c, DNALN_ERR_INVALID_ARG, "%s", why.c_str());
-  if (p->k != ix.k || p->w != ix.w)
-    return fail(c, DNALN_ERR_INVALID_ARG, "map k/w (%d/%d) differ from the index's (%d/%d)", p->k, p->w, ix.k, ix.w);
   if (p->max_cand < 1 || p->max_cand > 1024) return fail(c, DNALN_ERR_INVALID_ARG, "max_cand must be in [1, 1024]");
   if (p->ch.lookback < 0 || p->ch.band < 0 || p->ch.band > (1 << 20))
     return fail(c, DNALN_ERR_INVALID_ARG, "chain lookback must be >= 0 and band in [0, 2^20]");
+  return DNALN_OK;
+}
+
+int validate_map_params(dnaln_ctx* c, const dnaln_map_params* p, const IndexRes& ix) {
+  if (int e = validate_map_params_basic(c, p)) return e;
+  if (p->k != ix.k || p->w != ix.w)
+    return fail(c, DNALN_ERR_INVALID_ARG, "map k/w (%d/%d) differ from the index's (%d/%d)", p->k, p->w, ix.k, ix.w);
   return DNALN_OK;
 }
 
@@ -352,9 +396,10 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   // packed offsets, total bases, longest read
   DBUF(len64, int64_t, "len64", n + 1);
   DBUF(pofs, int64_t, "pofs", n + 1);
-  // info: [0] longest read, [1..3] cells, mapped, candidates (map.cuh), [4] minimizers
-  DBUF(info, unsigned long long, "info", 5);
-  CK(cudaMemsetAsync(info, 0, 5 * sizeof(unsigned long long), st));
+  // info: [0] longest read, [1..3] cells, mapped, candidates (map.cuh), [4] minimizers,
+  // [5] anchors of the thread path
+  DBUF(info, unsigned long long, "info", 6);
+  CK(cudaMemsetAsync(info, 0, 6 * sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
   CK(cudaMemsetAsync(c->d_count, 0, 3 * sizeof(int), st));
   unsigned long long* ctr = info + 1;  // cells, mapped, candidates (map.cuh)
@@ -399,12 +444,13 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   // short reads run passes 1 and 2 one thread per read; the rest (listed) one warp per read
   const bool thread_path = !c->warp_seed_only && seed_thread_supported(sp, cp);
   DBUF(big_list, int32_t, "big_list", n);
+  DBUF(n_anc_t, int32_t, "n_anc_t", n);
   int* big_n = c->d_count + 2;
   CK(cudaEventRecord(c->ev[kEvSeed0], st));
   if (thread_path) {
     kt.begin(st, "k_seed_chain_t");
     const bool ok = launch_seed_chain_thread(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, codes, ix.dev,
-                                             sp, cp, cand, cb, n_min, n_anchor, big_list, big_n, c->d_err);
+                                             sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list, big_n, c->d_err);
     kt.end(st);
     if (!ok) return fail(c, DNALN_ERR_CUDA, "thread-per-read seeding kernel could not be configured");
     kt.begin(st, "k_seed<list>");
@@ -420,21 +466,23 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   CK(cudaEventRecord(c->ev[kEvSeed1], st));
   CK(cudaGetLastError());
   if (int e = exclusive_scan(c, n_anchor, anchor_off, n + 1)) return e;
-  {  // minimizer total (MapStats-style counter), read back with the anchor total
+  {  // minimizer and thread-path anchor totals (MapStats-style counters)
     size_t tmp = 0;
     int64_t* total = reinterpret_cast<int64_t*>(info + 4);
     CK(cub::DeviceReduce::Sum(nullptr, tmp, n_min, total, n, st));
     DBUF(t, uint8_t, "cub_tmp_red", tmp);
     CK(cub::DeviceReduce::Sum(t, tmp, n_min, total, n, st));
+    if (thread_path) CK(cub::DeviceReduce::Sum(t, tmp, n_anc_t, total + 1, n, st));
   }
   CK(cudaMemcpyAsync(c->h_info, anchor_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(c->h_info + 1, info + 4, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(c->h_info + 2, big_n, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 1, info + 4, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 3, big_n, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   const int64_t A = c->h_info[0];
   const int64_t n_minimizers = c->h_info[1];
+  const int64_t n_anchors_thread = c->h_info[2];
   int n_big = 0;
-  std::memcpy(&n_big, c->h_info + 2, sizeof n_big);
+  std::memcpy(&n_big, c->h_info + 3, sizeof n_big);
 
   // pass 2 of the warp path: anchors, chains, candidates
   AnchorScratch as;
@@ -536,7 +584,7 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
 
   dnaln_stats& s = c->stats;
   s.reads += static_cast<uint64_t>(n);
-  s.anchors += static_cast<uint64_t>(A);
+  s.anchors += static_cast<uint64_t>(A + n_anchors_thread);
   s.minimizers += static_cast<uint64_t>(n_minimizers);
   s.sw_tasks_score += static_cast<uint64_t>(counts[0]);
   s.sw_tasks_tb += static_cast<uint64_t>(counts[1]);
@@ -578,6 +626,177 @@ void free_index(IndexRes& r) {
     if (b->p) cudaFree(b->p);
 }
 
+
+// ---- the worker behind dnaln_gpu_map_submit ----------------------------------------------
+// Parts are taken from the queue in order. While part j computes on the context's stream
+// (run_map), part j+1's reads are already on their way into the other device slot (copy
+// stream cp_in) and part j-1's records and CIGARs are on their way back (cp_out), so the
+// host<->device traffic of full-size batches hides behind the kernels of their neighbours.
+
+struct SlotBufs {
+  char* seq = nullptr;
+  int64_t* off = nullptr;
+  int32_t* len = nullptr;
+  uint32_t* hash = nullptr;
+  dnaln_map_record* out = nullptr;
+  uint32_t* cig = nullptr;
+};
+
+const char* const kSlotNames[2][6] = {{"in_seq0", "in_off0", "in_len0", "in_hash0", "out_rec0", "out_cig0"},
+                                      {"in_seq1", "in_off1", "in_len1", "in_hash1", "out_rec1", "out_cig1"}};
+
+bool pop_part(dnaln_ctx* c, MapPart& pt) {
+  std::lock_guard<std::mutex> g(c->qmu);
+  if (c->queue.empty()) return false;
+  pt = c->queue.front();
+  c->queue.pop_front();
+  return true;
+}
+
+// Copies a part's reads into slot k (stream cp_in) and records in_ready[k].
+int stage_in(dnaln_ctx* c, int k, const MapPart& pt, SlotBufs& sb) {
+  const int64_t m = pt.b - pt.a;
+  sb.seq = dbuf<char>(c, kSlotNames[k][0], pt.hi - pt.lo);
+  sb.off = dbuf<int64_t>(c, kSlotNames[k][1], m);
+  sb.len = dbuf<int32_t>(c, kSlotNames[k][2], m);
+  sb.hash = dbuf<uint32_t>(c, kSlotNames[k][3], m);
+  if (!sb.seq || !sb.off || !sb.len || !sb.hash) return DNALN_ERR_OOM;
+  CK(cudaEventRecord(c->h2d_ev[2 * k], c->cp_in));
+  if (pt.hi > pt.lo) CK(cudaMemcpyAsync(sb.seq, pt.seq + pt.lo, pt.hi - pt.lo, cudaMemcpyHostToDevice, c->cp_in));
+  CK(cudaMemcpyAsync(sb.off, pt.seq_off + pt.a, m * sizeof(int64_t), cudaMemcpyHostToDevice, c->cp_in));
+  CK(cudaMemcpyAsync(sb.len, pt.seq_len + pt.a, m * sizeof(int32_t), cudaMemcpyHostToDevice, c->cp_in));
+  CK(cudaMemcpyAsync(sb.hash, pt.name_hash + pt.a, m * sizeof(uint32_t), cudaMemcpyHostToDevice, c->cp_in));
+  CK(cudaEventRecord(c->h2d_ev[2 * k + 1], c->cp_in));
+  CK(cudaEventRecord(c->in_ready[k], c->cp_in));
+  return DNALN_OK;
+}
+
+struct PendingPart {  // a part whose results are being copied out of slot k
+  bool active = false;
+  MapPart pt;
+  int status = DNALN_OK;
+};
+
+// Records a finished part; the last part of a ticket publishes the ticket's status.
+void finish_part(dnaln_ctx* c, int k, PendingPart& pp) {
+  if (!pp.active) return;
+  pp.active = false;
+  if (pp.status == DNALN_OK) c->stats.ms_d2h += ev_ms(c->d2h_ev[2 * k], c->d2h_ev[2 * k + 1]);
+  {
+    std::lock_guard<std::mutex> g(c->qmu);
+    const int64_t t = pp.pt.ticket;
+    if (pp.status != DNALN_OK && !c->first_err.count(t)) c->first_err[t] = pp.status;
+    if (pp.pt.last) {
+      auto fe = c->first_err.find(t);
+      const int st = fe == c->first_err.end() ? DNALN_OK : fe->second;
+      if (fe != c->first_err.end()) c->first_err.erase(fe);
+      *pp.pt.cigar_used = c->ticket_ops[t];
+      c->ticket_ops.erase(t);
+      c->results[t] = st;
+    }
+  }
+  if (pp.pt.last) c->qcv.notify_all();
+}
+
+// Runs part pt (inputs in slot k) and starts copying its results out. Returns the part's status.
+int compute_part(dnaln_ctx* c, int k, const MapPart& pt, const SlotBufs& sb, int64_t base, int64_t* used) {
+  *used = 0;
+  IndexRes* r = find_index(c, pt.index_id);
+  if (!r) return DNALN_ERR_NOT_FOUND;
+  if (int e = validate_map_params(c, &pt.p, *r)) return e;
+  const int64_t m = pt.b - pt.a;
+  dnaln_map_record* d_out = dbuf<dnaln_map_record>(c, kSlotNames[k][4], m);
+  uint32_t* d_cig = dbuf<uint32_t>(c, kSlotNames[k][5], pt.cig_bound);
+  if (!d_out || !d_cig) return DNALN_ERR_OOM;
+  CK(cudaStreamWaitEvent(c->st, c->in_ready[k], 0));
+  CK(cudaStreamWaitEvent(c->st, c->out_free[k], 0));  // the results of part j-2 have left the slot
+  BatchHints hint;
+  hint.seq_base = pt.lo;
+  hint.bases = pt.bases;
+  hint.max_len = pt.max_len;
+  hint.cigar_base = base;
+  if (int e = run_map(c, *r, sb.seq, sb.off, sb.len, sb.hash, m, pt.p, d_out, d_cig, pt.cig_bound, used, nullptr,
+                      hint))
+    return e;
+  c->stats.ms_h2d += ev_ms(c->h2d_ev[2 * k], c->h2d_ev[2 * k + 1]);  // complete: run_map waited for it
+  if (base + *used > pt.cigar_cap || (*used > 0 && !pt.cigar))
+    return fail(c, DNALN_ERR_CAPACITY, "CIGAR buffer holds %lld ops, batch needs at least %lld",
+                static_cast<long long>(pt.cigar_cap), static_cast<long long>(base + *used));
+  CK(cudaEventRecord(c->d2h_ev[2 * k], c->cp_out));
+  CK(cudaMemcpyAsync(pt.out + pt.a, d_out, m * sizeof(dnaln_map_record), cudaMemcpyDeviceToHost, c->cp_out));
+  if (*used > 0)
+    CK(cudaMemcpyAsync(pt.cigar + base, d_cig, *used * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->cp_out));
+  CK(cudaEventRecord(c->d2h_ev[2 * k + 1], c->cp_out));
+  CK(cudaEventRecord(c->out_free[k], c->cp_out));
+  return DNALN_OK;
+}
+
+// Drives queued parts through the two slots until the queue is empty.
+void drive_parts(dnaln_ctx* c) {
+  PendingPart pend[2];
+  SlotBufs sb[2];
+  MapPart pt;
+  if (!pop_part(c, pt)) return;
+  int k = 0;
+  int staged = stage_in(c, k, pt, sb[k]);
+  for (;;) {
+    MapPart nx;
+    const bool have_next = pop_part(c, nx);
+    int next_staged = DNALN_OK;
+    if (have_next) next_staged = stage_in(c, 1 - k, nx, sb[1 - k]);  // slot 1-k's inputs are free
+    int64_t base = 0;
+    bool failed = false;
+    {
+      std::lock_guard<std::mutex> g(c->qmu);
+      base = c->ticket_ops[pt.ticket];
+      failed = c->first_err.count(pt.ticket) != 0;
+    }
+    int64_t used = 0;
+    int st = staged;
+    if (st == DNALN_OK && failed) st = DNALN_ERR_INVALID_ARG;  // an earlier part of the ticket failed
+    if (st == DNALN_OK) st = compute_part(c, k, pt, sb[k], base, &used);
+    // the stream is idle (run_map synchronised it after waiting for out_free[k]): the part
+    // that used slot k before is fully copied out
+    finish_part(c, k, pend[k]);
+    if (st == DNALN_OK) {
+      std::lock_guard<std::mutex> g(c->qmu);
+      c->ticket_ops[pt.ticket] = base + used;
+    }
+    pend[k].pt = pt;
+    pend[k].status = st;
+    pend[k].active = true;
+    if (st != DNALN_OK) {
+      cudaStreamSynchronize(c->cp_out);
+      finish_part(c, 1 - k, pend[1 - k]);
+      finish_part(c, k, pend[k]);
+    } else if (pend[1 - k].active && cudaEventQuery(c->out_free[1 - k]) == cudaSuccess) {
+      finish_part(c, 1 - k, pend[1 - k]);
+    }
+    cudaGetLastError();
+    if (!have_next) break;
+    pt = nx;
+    staged = next_staged;
+    k = 1 - k;
+  }
+  cudaStreamSynchronize(c->cp_out);
+  finish_part(c, 1 - k, pend[1 - k]);  // older first
+  finish_part(c, k, pend[k]);
+}
+
+void map_worker(dnaln_ctx* c) {
+  cudaSetDevice(c->device);
+  std::unique_lock<std::mutex> ql(c->qmu);
+  for (;;) {
+    c->qcv.wait(ql, [&] { return c->stop || !c->queue.empty(); });
+    if (c->queue.empty()) break;  // stopping, nothing left
+    ql.unlock();
+    {
+      std::lock_guard<std::mutex> g(c->mu);
+      drive_parts(c);
+    }
+    ql.lock();
+  }
+}
 }  // namespace
 
 extern "C" {
@@ -632,6 +851,12 @@ int dnaln_gpu_ctx_create(int device, dnaln_ctx** out) {
 
 int dnaln_gpu_ctx_destroy(dnaln_ctx* c) {
   if (!c) return DNALN_OK;
+  {  // the worker finishes what is queued, then exits
+    std::lock_guard<std::mutex> g(c->qmu);
+    c->stop = true;
+  }
+  c->qcv.notify_all();
+  if (c->worker.joinable()) c->worker.join();
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
   for (auto& kv : c->idx) free_index(kv.second);
@@ -664,11 +889,15 @@ const char* dnaln_gpu_last_error(const dnaln_ctx* c) { return c ? c->err.c_str()
 
 int dnaln_gpu_set_stream(dnaln_ctx* c, void* stream) {
   if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
+  if (!c) return DNALN_ERR_INVALID_ARG;
   c->st = stream ? static_cast<cudaStream_t>(stream) : c->own;
   return DNALN_OK;
 }
 
 int dnaln_gpu_get_stats(const dnaln_ctx* c, dnaln_stats* out) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c || !out) return DNALN_ERR_INVALID_ARG;
   *out = c->stats;
   return DNALN_OK;
@@ -676,12 +905,16 @@ int dnaln_gpu_get_stats(const dnaln_ctx* c, dnaln_stats* out) {
 
 int dnaln_gpu_reset_stats(dnaln_ctx* c) {
   if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
+  if (!c) return DNALN_ERR_INVALID_ARG;
   c->stats = dnaln_stats{};
   c->ktimes.clear();
   return DNALN_OK;
 }
 
 int dnaln_gpu_set_kernel_trace(dnaln_ctx* c, int32_t on, const char* only) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c) return DNALN_ERR_INVALID_ARG;
   c->trace_only = only ? only : "";
   if (on && c->trace_ev.empty()) {
@@ -696,6 +929,8 @@ int dnaln_gpu_set_kernel_trace(dnaln_ctx* c, int32_t on, const char* only) {
 }
 
 int dnaln_gpu_kernel_times(const dnaln_ctx* c, dnaln_kernel_time* out, int32_t cap, int32_t* n_out) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c || !n_out || cap < 0 || (cap > 0 && !out)) return DNALN_ERR_INVALID_ARG;
   int32_t i = 0;
   for (const auto& kv : c->ktimes) {
@@ -713,6 +948,8 @@ int dnaln_gpu_kernel_times(const dnaln_ctx* c, dnaln_kernel_time* out, int32_t c
 }
 
 int dnaln_gpu_set_sub_batch(dnaln_ctx* c, int64_t reads) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c || reads < 0) return DNALN_ERR_INVALID_ARG;
   c->sub_batch = reads;
   return DNALN_OK;
@@ -722,6 +959,7 @@ int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
   if (!c || !name) return DNALN_ERR_INVALID_ARG;
   const std::string k = name;
   if (k == "sub_batch") return dnaln_gpu_set_sub_batch(c, value);
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (k == "warp_seed_only") {
     c->warp_seed_only = value != 0;
     return DNALN_OK;
@@ -749,6 +987,8 @@ int dnaln_gpu_host_free(dnaln_ctx* c, void* p) {
 
 int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases, const uint64_t* contig_off,
                           const uint32_t* contig_len, int32_t n_contigs, int32_t k, int32_t w, int32_t* index_id) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c || !genome || !contig_off || !contig_len || !index_id || n_contigs < 1)
     return fail(c, DNALN_ERR_INVALID_ARG, "null argument or no contigs");
   if (k < 4 || k > 28) return fail(c, DNALN_ERR_INVALID_ARG, "k must be in [4, 28] (got %d)", k);
@@ -823,6 +1063,8 @@ int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases,
 }
 
 int dnaln_gpu_index_stats(const dnaln_ctx* cc, int32_t id, uint64_t out6[6]) {
+  if (!cc) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(cc->mu);
   auto* c = const_cast<dnaln_ctx*>(cc);
   if (!c || !out6) return DNALN_ERR_INVALID_ARG;
   IndexRes* r = find_index(c, id);
@@ -838,6 +1080,8 @@ int dnaln_gpu_index_stats(const dnaln_ctx* cc, int32_t id, uint64_t out6[6]) {
 
 int dnaln_gpu_index_export(dnaln_ctx* c, int32_t id, uint64_t* keys, uint32_t* offsets, uint32_t* counts,
                            uint32_t* positions) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c) return DNALN_ERR_INVALID_ARG;
   if (int e = set_device(c)) return e;
   IndexRes* r = find_index(c, id);
@@ -856,6 +1100,8 @@ int dnaln_gpu_index_export(dnaln_ctx* c, int32_t id, uint64_t* keys, uint32_t* o
 
 int dnaln_gpu_index_free(dnaln_ctx* c, int32_t id) {
   if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
+  if (!c) return DNALN_ERR_INVALID_ARG;
   if (int e = set_device(c)) return e;
   IndexRes* r = find_index(c, id);
   if (!r) return DNALN_ERR_NOT_FOUND;
@@ -868,6 +1114,8 @@ int dnaln_gpu_index_free(dnaln_ctx* c, int32_t id) {
 int dnaln_gpu_sketch(dnaln_ctx* c, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,
                      const uint32_t* pos_offset, int64_t n, int32_t k, int32_t w, uint64_t* out_hash,
                      uint32_t* out_pos, uint32_t* out_strand, int32_t* out_count) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c || n < 0 || (n > 0 && (!codes || !seq_off || !seq_len || !out_hash || !out_pos || !out_strand || !out_count)))
     return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
   if (k < 1 || k > 31) return fail(c, DNALN_ERR_INVALID_ARG, "k must be in [1, 31] (got %d)", k);
@@ -904,6 +1152,8 @@ int dnaln_gpu_sketch(dnaln_ctx* c, const uint8_t* codes, const int64_t* seq_off,
 
 int dnaln_gpu_lookup(dnaln_ctx* c, int32_t id, const uint64_t* hashes, int64_t n, uint32_t* out_offset,
                      uint32_t* out_count) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c || n < 0 || (n > 0 && (!hashes || !out_offset || !out_count)))
     return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
   if (int e = set_device(c)) return e;
@@ -929,6 +1179,8 @@ int dnaln_gpu_lookup(dnaln_ctx* c, int32_t id, const uint64_t* hashes, int64_t n
 int dnaln_gpu_chain(dnaln_ctx* c, uint32_t* rpos, int32_t* qpos, uint32_t* strand, const int64_t* set_off,
                     int64_t n_sets, int32_t k, const dnaln_chain_params* p, int32_t* out_score, uint32_t* out_strand,
                     int32_t* out_n, int64_t* out_dmin, int64_t* out_dmax, uint32_t* out_rpos, int32_t* out_count) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c || !p || !set_off || n_sets < 0 || !out_count) return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
   if (p->lookback < 0 || p->band < 0 || p->band > (1 << 20))
     return fail(c, DNALN_ERR_INVALID_ARG, "chain lookback must be >= 0 and band in [0, 2^20]");
@@ -1009,6 +1261,8 @@ int dnaln_gpu_align(dnaln_ctx* c, const uint8_t* q, const int64_t* q_off, const 
                     const int64_t* t_off, const int32_t* t_len, int64_t n, int32_t traceback,
                     const dnaln_score_params* sp, dnaln_align_result* out, uint32_t* cigar, int64_t cigar_cap,
                     int64_t* cigar_used) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c || !sp || n < 0 || (n > 0 && (!q || !q_off || !q_len || !t || !t_off || !t_len || !out)))
     return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
   if (sp->bw < 0 || sp->bw > 1000 || sp->gap_ext < 0 || sp->gap_open < 0 || sp->mismatch < 0 || sp->ambig < 0)
@@ -1117,6 +1371,8 @@ int dnaln_gpu_map_batch_device(dnaln_ctx* c, int32_t id, const char* d_seq, cons
                                const int32_t* d_seq_len, const uint32_t* d_name_hash, int64_t n,
                                const dnaln_map_params* p, dnaln_map_record* d_out, uint32_t* d_cigar,
                                int64_t cigar_cap, int64_t* cigar_used) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (!c || n < 0 || !cigar_used || (n > 0 && (!d_seq || !d_seq_off || !d_seq_len || !d_name_hash || !d_out)))
     return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
   if (int e = set_device(c)) return e;
@@ -1130,136 +1386,87 @@ int dnaln_gpu_map_batch_device(dnaln_ctx* c, int32_t id, const char* d_seq, cons
   return e;
 }
 
+int dnaln_gpu_map_submit(dnaln_ctx* c, int32_t id, const char* seq, const int64_t* seq_off, const int32_t* seq_len,
+                         const uint32_t* name_hash, int64_t n, const dnaln_map_params* p, dnaln_map_record* out,
+                         uint32_t* cigar, int64_t cigar_cap, int64_t* cigar_used, int64_t* ticket) {
+  if (!c || n < 0 || !cigar_used || !ticket || !p || (n > 0 && (!seq || !seq_off || !seq_len || !name_hash || !out)))
+    return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
+  *ticket = 0;
+  *cigar_used = 0;
+  // the index-dependent checks run in the worker (the index table belongs to it while it
+  // drives the device); their failures come back from dnaln_gpu_map_wait
+  if (int e = validate_map_params_basic(c, p)) return e;
+  // parts of at most sub_batch reads, with their host-side facts (lengths are known here)
+  const int64_t S = c->sub_batch > 0 ? c->sub_batch : (n > 0 ? n : 1);
+  std::vector<MapPart> parts;
+  for (int64_t a = 0; a < n; a += S) {
+    MapPart pt;
+    pt.index_id = id;
+    pt.seq = seq;
+    pt.seq_off = seq_off;
+    pt.seq_len = seq_len;
+    pt.name_hash = name_hash;
+    pt.a = a;
+    pt.b = std::min(n, a + S);
+    pt.lo = seq_off[a];
+    pt.p = *p;
+    pt.out = out;
+    pt.cigar = cigar;
+    pt.cigar_cap = cigar_cap;
+    pt.cigar_used = cigar_used;
+    for (int64_t i = pt.a; i < pt.b; ++i) {
+      if (seq_len[i] < 0 || seq_off[i] < 0) return fail(c, DNALN_ERR_INVALID_ARG, "negative offset or length");
+      pt.lo = std::min(pt.lo, seq_off[i]);
+      pt.hi = std::max(pt.hi, seq_off[i] + seq_len[i]);
+      pt.bases += seq_len[i];
+      pt.max_len = std::max<int64_t>(pt.max_len, seq_len[i]);
+      pt.cig_bound += 2 * static_cast<int64_t>(seq_len[i]) + 3;  // walk ops (<= 2*len+1) + 2 clips
+    }
+    if (pt.hi < pt.lo) pt.hi = pt.lo;
+    parts.push_back(pt);
+  }
+  {
+    std::lock_guard<std::mutex> g(c->qmu);
+    const int64_t t = c->next_ticket++;
+    *ticket = t;
+    if (parts.empty()) {
+      c->results[t] = DNALN_OK;
+      return DNALN_OK;
+    }
+    parts.back().last = true;
+    for (MapPart& pt : parts) {
+      pt.ticket = t;
+      c->queue.push_back(pt);
+    }
+    c->ticket_ops[t] = 0;
+    if (!c->worker.joinable()) c->worker = std::thread(map_worker, c);
+  }
+  c->qcv.notify_all();
+  return DNALN_OK;
+}
+
+int dnaln_gpu_map_wait(dnaln_ctx* c, int64_t ticket) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::unique_lock<std::mutex> ql(c->qmu);
+  if (ticket <= 0 || ticket >= c->next_ticket) return fail(c, DNALN_ERR_INVALID_ARG, "unknown ticket %lld",
+                                                           static_cast<long long>(ticket));
+  c->qcv.wait(ql, [&] { return c->results.count(ticket) != 0 || c->stop; });
+  auto it = c->results.find(ticket);
+  if (it == c->results.end()) return fail(c, DNALN_ERR_INVALID_ARG, "ticket %lld was already waited for",
+                                          static_cast<long long>(ticket));
+  const int e = it->second;
+  c->results.erase(it);
+  return e;
+}
+
 int dnaln_gpu_map_batch(dnaln_ctx* c, int32_t id, const char* seq, const int64_t* seq_off, const int32_t* seq_len,
                         const uint32_t* name_hash, int64_t n, const dnaln_map_params* p, dnaln_map_record* out,
                         uint32_t* cigar, int64_t cigar_cap, int64_t* cigar_used) {
-  if (!c || n < 0 || !cigar_used || (n > 0 && (!seq || !seq_off || !seq_len || !name_hash || !out)))
-    return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
-  if (int e = set_device(c)) return e;
-  IndexRes* r = find_index(c, id);
-  if (!r) return DNALN_ERR_NOT_FOUND;
-  if (int e = validate_map_params(c, p, *r)) return e;
-  *cigar_used = 0;
-  if (n == 0) return DNALN_OK;
-
-  // Sub-batches of at most sub_batch reads go through two device slots: while one
-  // sub-batch computes, the next one's reads are copied in and the previous one's records
-  // and CIGARs are copied out, on the context's two copy streams.
-  struct Sub {
-    int64_t a, b, lo, hi, bases, max_len, cig_bound;
-  };
-  const int64_t S = c->sub_batch > 0 ? c->sub_batch : n;
-  std::vector<Sub> subs;
-  int64_t span = 0, rmax = 0, cmax = 0;
-  for (int64_t a = 0; a < n; a += S) {
-    Sub sb{a, std::min(n, a + S), seq_off[a], 0, 0, 0, 0};
-    for (int64_t i = sb.a; i < sb.b; ++i) {
-      if (seq_len[i] < 0 || seq_off[i] < 0) return fail(c, DNALN_ERR_INVALID_ARG, "negative offset or length");
-      sb.lo = std::min(sb.lo, seq_off[i]);
-      sb.hi = std::max(sb.hi, seq_off[i] + seq_len[i]);
-      sb.bases += seq_len[i];
-      sb.max_len = std::max<int64_t>(sb.max_len, seq_len[i]);
-      sb.cig_bound += 2 * static_cast<int64_t>(seq_len[i]) + 3;  // walk ops (<= 2*len+1) + 2 clips
-    }
-    span = std::max(span, sb.hi - sb.lo);
-    rmax = std::max(rmax, sb.b - sb.a);
-    cmax = std::max(cmax, sb.cig_bound);
-    subs.push_back(sb);
-  }
-  const int J = static_cast<int>(subs.size());
-  char* d_seq[2] = {};
-  int64_t* d_off[2] = {};
-  int32_t* d_len[2] = {};
-  uint32_t* d_hash[2] = {};
-  dnaln_map_record* d_out[2] = {};
-  uint32_t* d_cig[2] = {};
-  static const char* const kSlotNames[2][6] = {{"in_seq0", "in_off0", "in_len0", "in_hash0", "out_rec0", "out_cig0"},
-                                               {"in_seq1", "in_off1", "in_len1", "in_hash1", "out_rec1", "out_cig1"}};
-  for (int k = 0; k < 2 && k < J; ++k) {
-    d_seq[k] = dbuf<char>(c, kSlotNames[k][0], span);
-    d_off[k] = dbuf<int64_t>(c, kSlotNames[k][1], rmax);
-    d_len[k] = dbuf<int32_t>(c, kSlotNames[k][2], rmax);
-    d_hash[k] = dbuf<uint32_t>(c, kSlotNames[k][3], rmax);
-    d_out[k] = dbuf<dnaln_map_record>(c, kSlotNames[k][4], rmax);
-    d_cig[k] = dbuf<uint32_t>(c, kSlotNames[k][5], cmax);
-    if (!d_seq[k] || !d_off[k] || !d_len[k] || !d_hash[k] || !d_out[k] || !d_cig[k]) return DNALN_ERR_OOM;
-  }
-  cudaStream_t st = c->st;
-  bool h2d_rec[2] = {false, false}, d2h_rec[2] = {false, false};
-  const auto drain = [&]() {
-    cudaStreamSynchronize(c->cp_in);
-    cudaStreamSynchronize(c->cp_out);
-    for (int k = 0; k < 2; ++k) {
-      if (h2d_rec[k]) c->stats.ms_h2d += ev_ms(c->h2d_ev[2 * k], c->h2d_ev[2 * k + 1]);
-      if (d2h_rec[k]) c->stats.ms_d2h += ev_ms(c->d2h_ev[2 * k], c->d2h_ev[2 * k + 1]);
-      h2d_rec[k] = d2h_rec[k] = false;
-    }
-  };
-  const auto h2d = [&](int j) -> int {
-    const Sub& sb = subs[j];
-    const int k = j & 1;
-    const int64_t m = sb.b - sb.a;
-    if (h2d_rec[k]) c->stats.ms_h2d += ev_ms(c->h2d_ev[2 * k], c->h2d_ev[2 * k + 1]);  // done: its slot was used
-    CK(cudaEventRecord(c->h2d_ev[2 * k], c->cp_in));
-    if (sb.hi > sb.lo) CK(cudaMemcpyAsync(d_seq[k], seq + sb.lo, sb.hi - sb.lo, cudaMemcpyHostToDevice, c->cp_in));
-    CK(cudaMemcpyAsync(d_off[k], seq_off + sb.a, m * sizeof(int64_t), cudaMemcpyHostToDevice, c->cp_in));
-    CK(cudaMemcpyAsync(d_len[k], seq_len + sb.a, m * sizeof(int32_t), cudaMemcpyHostToDevice, c->cp_in));
-    CK(cudaMemcpyAsync(d_hash[k], name_hash + sb.a, m * sizeof(uint32_t), cudaMemcpyHostToDevice, c->cp_in));
-    CK(cudaEventRecord(c->h2d_ev[2 * k + 1], c->cp_in));
-    CK(cudaEventRecord(c->in_ready[k], c->cp_in));
-    h2d_rec[k] = true;
-    return DNALN_OK;
-  };
-  const auto d2h = [&](int j, int64_t base, int64_t used) -> int {
-    const Sub& sb = subs[j];
-    const int k = j & 1;
-    if (d2h_rec[k]) c->stats.ms_d2h += ev_ms(c->d2h_ev[2 * k], c->d2h_ev[2 * k + 1]);
-    CK(cudaEventRecord(c->d2h_ev[2 * k], c->cp_out));
-    CK(cudaMemcpyAsync(out + sb.a, d_out[k], (sb.b - sb.a) * sizeof(dnaln_map_record), cudaMemcpyDeviceToHost,
-                       c->cp_out));
-    if (used > 0)
-      CK(cudaMemcpyAsync(cigar + base, d_cig[k], used * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->cp_out));
-    CK(cudaEventRecord(c->d2h_ev[2 * k + 1], c->cp_out));
-    CK(cudaEventRecord(c->out_free[k], c->cp_out));
-    d2h_rec[k] = true;
-    return DNALN_OK;
-  };
-
-  int64_t base = 0;
-  int e = DNALN_OK;
-  for (int j = 0; j < 2 && j < J && e == DNALN_OK; ++j) e = h2d(j);
-  for (int j = 0; j < J && e == DNALN_OK; ++j) {
-    const Sub& sb = subs[j];
-    const int k = j & 1;
-    if (cudaStreamWaitEvent(st, c->in_ready[k], 0) != cudaSuccess ||
-        (j >= 2 && cudaStreamWaitEvent(st, c->out_free[k], 0) != cudaSuccess)) {
-      e = fail(c, DNALN_ERR_CUDA, "stream wait: %s", cudaGetErrorString(cudaGetLastError()));
-      break;
-    }
-    BatchHints hint;
-    hint.seq_base = sb.lo;
-    hint.bases = sb.bases;
-    hint.max_len = sb.max_len;
-    hint.cigar_base = base;
-    int64_t used = 0;
-    e = run_map(c, *r, d_seq[k], d_off[k], d_len[k], d_hash[k], sb.b - sb.a, *p, d_out[k], d_cig[k], cmax, &used,
-                nullptr, hint);
-    if (e != DNALN_OK) break;
-    // run_map returns with its stream idle, so slot k's inputs are free for sub-batch j + 2
-    if (j + 2 < J && (e = h2d(j + 2)) != DNALN_OK) break;
-    if (base + used > cigar_cap || (used > 0 && !cigar)) {
-      e = fail(c, DNALN_ERR_CAPACITY, "CIGAR buffer holds %lld ops, batch needs at least %lld",
-               static_cast<long long>(cigar_cap), static_cast<long long>(base + used));
-      break;
-    }
-    if ((e = d2h(j, base, used)) != DNALN_OK) break;
-    base += used;
-  }
-  drain();
-  if (e != DNALN_OK) return e;
-  if (cudaGetLastError() != cudaSuccess) return fail(c, DNALN_ERR_CUDA, "copy stream error");
-  *cigar_used = base;
-  return DNALN_OK;
+  int64_t ticket = 0;
+  if (int e = dnaln_gpu_map_submit(c, id, seq, seq_off, seq_len, name_hash, n, p, out, cigar, cigar_cap, cigar_used,
+                                   &ticket))
+    return e;
+  return dnaln_gpu_map_wait(c, ticket);
 }
 
 }  // extern "C"

@@ -140,8 +140,9 @@ void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_l
                       const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as, CandBuf cb, uint32_t* err);
 
 // One thread per read (seed_thread.cu): passes 1 and 2 of the reads the per-thread budgets
-// admit, writing codes of every read, candidates of the admitted ones, n_min and
-// n_anchor = 0; the others are appended to big_list (count in *big_n, zeroed by the caller)
+// admit, writing codes of every read, candidates of the admitted ones, n_min, n_anc_t (their
+// anchor counts, for statistics) and n_anchor = 0 (no scratch); the others are appended
+// to big_list (count in *big_n, zeroed by the caller)
 // for launch_seed_list / launch_chain_map. Returns false, launching nothing, when the
 // parameters are outside the path's range.
 bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp);
@@ -149,7 +150,7 @@ bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* s
                               const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes,
                               const DevIndex& ix, const SeedParams& sp, const ChainParamsDev& cp,
                               const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
-                              int32_t* big_list, int* big_n, uint32_t* err);
+                              int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err);
 
 // Stage entry points: sketch of code sequences, lookups, chaining of given anchor sets.
 void launch_sketch_codes(cudaStream_t st, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,

@@ -70,7 +70,8 @@ __global__ void __launch_bounds__(kTT)
                    const int32_t* __restrict__ seq_len, const int64_t* __restrict__ pofs, int64_t n,
                    uint8_t* __restrict__ codes, DevIndex ix, SeedParams sp, ChainParamsDev cp, CandParams cand,
                    CandBuf cb, int32_t* __restrict__ n_min, int64_t* __restrict__ n_anchor,
-                   int32_t* __restrict__ big_list, int* __restrict__ big_n, uint32_t* __restrict__ err) {
+                   int32_t* __restrict__ n_anc_t, int32_t* __restrict__ big_list, int* __restrict__ big_n,
+                   uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* const stg = reinterpret_cast<uint32_t*>(smem);  // region A (all columns, for the encode)
   const int T = threadIdx.x, lane = T & 31;
@@ -348,10 +349,12 @@ __global__ void __launch_bounds__(kTT)
   n_anchor[r] = 0;  // no anchor scratch: this read either finished here or is listed below
   if (big) {
     n_min[r] = 0;
+    n_anc_t[r] = 0;
     big_list[atomicAdd(big_n, 1)] = static_cast<int32_t>(r);
     return;
   }
   n_min[r] = nmin;
+  n_anc_t[r] = na;
   cb.n_cand[r] = nd;
 }
 
@@ -366,7 +369,7 @@ bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* s
                               const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes,
                               const DevIndex& ix, const SeedParams& sp, const ChainParamsDev& cp,
                               const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
-                              int32_t* big_list, int* big_n, uint32_t* err) {
+                              int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err) {
   if (!seed_thread_supported(sp, cp)) return false;
   if (n <= 0) return true;
   static bool attr_set[64] = {};  // per device
@@ -380,7 +383,8 @@ bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* s
   }
   const int64_t blocks = (n + kTT - 1) / kTT;
   k_seed_chain_t<kTW><<<static_cast<unsigned>(blocks), kTT, kThreadSmem, st>>>(
-      seq, seq_off, seq_base, seq_len, pofs, n, codes, ix, sp, cp, cand, cb, n_min, n_anchor, big_list, big_n, err);
+      seq, seq_off, seq_base, seq_len, pofs, n, codes, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list,
+      big_n, err);
   return true;
 }
 

@@ -116,7 +116,8 @@ typedef struct dnaln_kernel_time {
 int dnaln_gpu_set_kernel_trace(dnaln_ctx* ctx, int32_t on, const char* only);
 /* Writes min(cap, count) entries; *n_out = count of traced kernel names. */
 int dnaln_gpu_kernel_times(const dnaln_ctx* ctx, dnaln_kernel_time* out, int32_t cap, int32_t* n_out);
-/* Reads per sub-batch of dnaln_gpu_map_batch (default 65536; 0 = whole batch at once). */
+/* Reads per part of a host-buffer batch (default 0: the whole batch is one part; smaller
+ * parts let one synchronous call overlap its own copies, at some kernel efficiency). */
 int dnaln_gpu_set_sub_batch(dnaln_ctx* ctx, int64_t reads);
 /* Tuning switches (none changes any result):
  *   "sub_batch"      same as dnaln_gpu_set_sub_batch;
@@ -201,12 +202,22 @@ int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_off, const in
  * read name (src/common.hpp:136-140, dnaln_fnv1a below), the tie-break between equal
  * best candidates. Records go to out[r]; CIGARs to `cigar` (capacity cigar_cap ops;
  * the sum over reads of 2*len+3 always suffices; DNALN_ERR_CAPACITY if it is short).
- * The host-buffer call streams the batch through the device in sub-batches (see
- * dnaln_gpu_set_sub_batch), overlapping copies with compute; page-locked buffers
- * (dnaln_gpu_host_alloc) make the copies asynchronous. */
+ * Page-locked buffers (dnaln_gpu_host_alloc) make the copies asynchronous. */
 int dnaln_gpu_map_batch(dnaln_ctx* ctx, int32_t index_id, const char* seq, const int64_t* seq_off,
                         const int32_t* seq_len, const uint32_t* name_hash, int64_t n, const dnaln_map_params* p,
                         dnaln_map_record* out, uint32_t* cigar, int64_t cigar_cap, int64_t* cigar_used);
+/* The same call split in two (no reference counterpart; a streaming caller's form of
+ * Mapper::map): submit queues the batch and returns a ticket at once; a worker thread of
+ * the context maps queued batches in order, copying the next batch's reads in and the
+ * previous batch's results out while the current one computes. Every buffer of a batch
+ * must stay valid and unmodified until dnaln_gpu_map_wait returns for its ticket; wait
+ * returns the batch's status and sets *cigar_used. Each ticket is waited for once. Other
+ * calls on the context wait until the queue is empty. */
+int dnaln_gpu_map_submit(dnaln_ctx* ctx, int32_t index_id, const char* seq, const int64_t* seq_off,
+                         const int32_t* seq_len, const uint32_t* name_hash, int64_t n, const dnaln_map_params* p,
+                         dnaln_map_record* out, uint32_t* cigar, int64_t cigar_cap, int64_t* cigar_used,
+                         int64_t* ticket);
+int dnaln_gpu_map_wait(dnaln_ctx* ctx, int64_t ticket);
 
 /* Same pipeline with every buffer already in device memory (no host transfers); the
  * CIGAR count is returned through the host pointer cigar_used. */

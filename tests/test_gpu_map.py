@@ -141,6 +141,29 @@ def test_thread_and_warp_seed_paths_identical(ctx, request, wl):
     assert np.array_equal(mixed_path.cigar, warp_path.cigar)
 
 
+@pytest.mark.parametrize("sub_batch", [0, 3000])
+def test_submit_wait_matches_map_batch(ctx, repeat, sub_batch):
+    # several batches in flight through the worker (reads copied in while the previous batch
+    # computes), waited for out of order; each must equal the synchronous call
+    g, reads, _ = repeat
+    p = D.default_map_params()
+    iid = ctx.index_build(g)
+    try:
+        ctx.set_sub_batch(0)
+        spans = [(0, 7000), (7000, 7001), (7001, 7001), (7001, 20000), (3000, 9000)]
+        want = [ctx.map_batch(iid, reads.slice(a, b), p) for a, b in spans]
+        ctx.set_sub_batch(sub_batch)
+        tickets = [ctx.map_submit(iid, reads.slice(a, b), p) for a, b in spans]
+        for t, w in reversed(list(zip(tickets, want))):
+            got = ctx.map_wait(t)
+            assert np.array_equal(gpu_records(got), gpu_records(w))
+            assert np.array_equal(got.records["cigar_off"], w.records["cigar_off"])
+            assert np.array_equal(got.cigar, w.cigar)
+    finally:
+        ctx.set_sub_batch(0)
+        ctx.index_free(iid)
+
+
 @pytest.mark.parametrize("sub_batch", [0, 997, 4096])
 def test_sub_batch_pipeline_identical(ctx, repeat, sub_batch):
     # the host-buffer call streams sub-batches through two device slots; records and
@@ -174,7 +197,7 @@ def test_sub_batch_pipeline_identical(ctx, repeat, sub_batch):
             assert np.array_equal(got.cigar_of(i), whole.cigar_of(i))
         assert used.value == len(whole.cigar)
     finally:
-        ctx.set_sub_batch(65536)
+        ctx.set_sub_batch(0)
         ctx.index_free(iid)
 
 
