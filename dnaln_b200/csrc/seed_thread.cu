@@ -60,7 +60,8 @@ static_assert(2 * kTMaxAnc <= kWordsA, "anchor keys must fit a staging column");
 static_assert(2 * kTMaxMin <= kWordsB && kTMaxAnc + 4 * kTMaxChains <= kWordsB, "region B column too small");
 constexpr int kRegionA = kWordsA * kTPitch * 4;
 constexpr int kRegionB = kWordsB * kTT * 4;
-constexpr int kThreadSmem = kRegionA + kRegionB;
+constexpr int kTMaxBand = 256;  // chaining band the shared gap-cost table holds
+constexpr int kThreadSmem = kRegionA + kRegionB + (kTMaxBand + 1) * 4;
 
 __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return b < a ? b : a; }
 
@@ -74,17 +75,24 @@ __global__ void __launch_bounds__(kTT)
                    uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* const stg = reinterpret_cast<uint32_t*>(smem);  // region A (all columns, for the encode)
+  int32_t* const lut = reinterpret_cast<int32_t*>(smem + kRegionA + kRegionB);  // chaining gap costs
   const int T = threadIdx.x, lane = T & 31;
+  for (int d = T; d <= cp.band; d += kTT) lut[d] = cp.cost[d];
+  __syncthreads();
   uint32_t* const ca = stg + T;                                                   // this thread's A column
   uint32_t* const cbw = reinterpret_cast<uint32_t*>(smem + kRegionA) + T;         // this thread's B column
-  const auto key_ld = [&](int a) {
-    return static_cast<uint64_t>(ca[(2 * a + 1) * kTPitch]) << 32 | ca[2 * a * kTPitch];
-  };
+  // anchor a: word 2a = strand << 31 | rpos, word 2a+1 = qpos (>= 0 here); as one 64-bit
+  // key (word 2a high) it orders like (strand, rpos, qpos), the reference's anchor order
+  const auto a_hi = [&](int a) -> uint32_t& { return ca[2 * a * kTPitch]; };
+  const auto a_lo = [&](int a) -> uint32_t& { return ca[(2 * a + 1) * kTPitch]; };
+  const auto key_ld = [&](int a) { return static_cast<uint64_t>(a_hi(a)) << 32 | a_lo(a); };
   const auto key_st = [&](int a, uint64_t v) {
-    ca[2 * a * kTPitch] = static_cast<uint32_t>(v);
-    ca[(2 * a + 1) * kTPitch] = static_cast<uint32_t>(v >> 32);
+    a_hi(a) = static_cast<uint32_t>(v >> 32);
+    a_lo(a) = static_cast<uint32_t>(v);
   };
-  const auto fp_at = [&](int i) -> int32_t& { return reinterpret_cast<int32_t&>(cbw[i * kTT]); };
+  // DP word of anchor i: (prev + 1) | f << 8 | max(f[0..i]) << 20 (f <= k * 32 < 4096)
+  const auto fp_at = [&](int i) -> uint32_t& { return cbw[i * kTT]; };
+  const auto f_of = [](uint32_t w) { return static_cast<int>((w >> 8) & 0xFFFu); };
   const auto ch_at = [&](int field, int c) -> int32_t& {
     return reinterpret_cast<int32_t&>(cbw[(kTMaxAnc + field * kTMaxChains + c) * kTT]);
   };
@@ -221,7 +229,8 @@ __global__ void __launch_bounds__(kTT)
           const uint32_t v = __ldg(ix.positions + off + t);
           const uint32_t rv = (v & 1u) ^ mst;
           const int32_t qpos = rv ? len - pos - k : pos;
-          key_st(na, anchor_key(rv, v >> 1, qpos));
+          a_hi(na) = rv << 31 | v >> 1;
+          a_lo(na) = static_cast<uint32_t>(qpos);
           ++na;
         }
       }
@@ -249,31 +258,39 @@ __global__ void __launch_bounds__(kTT)
       }
       key_st(j + 1, x);
     }
-    // ---- DP (src/chain.cpp:22-45); region B becomes f << 8 | (prev + 1)
+    // ---- DP (src/chain.cpp:22-45); region B becomes the DP words
+    // A predecessor j' <= j scores at most max(f[0..j]) + k (gain <= k, cost >= 0), so once
+    // that is <= best no remaining candidate can win the strict '>': the scan stops there
+    // with the reference's result. On colinear chains this ends it after a step or two.
+    const uint32_t max_gap = static_cast<uint32_t>(cp.max_gap);
+    int pm = 0;
     for (int i = 0; i < na; ++i) {
-      const uint64_t ki = key_ld(i);
-      const uint32_t si = key_strand(ki), ri = key_rpos(ki);
-      const int32_t qi = key_qpos(ki);
+      const uint32_t hi_i = a_hi(i);
+      const int32_t qi = static_cast<int32_t>(a_lo(i));
       int best = k, bj = -1;
       const int lo = i - cp.lookback > 0 ? i - cp.lookback : 0;
       for (int j = i - 1; j >= lo; --j) {
-        const uint64_t kj = key_ld(j);
-        if (key_strand(kj) != si) break;
-        const int64_t dr = static_cast<int64_t>(ri) - key_rpos(kj);
-        if (dr > cp.max_gap) break;
-        const int32_t dq = qi - key_qpos(kj);
-        if (dr <= 0 || dq <= 0) continue;
-        const int64_t dd = dr > dq ? dr - dq : dq - dr;
+        const uint32_t wj = fp_at(j);
+        if (static_cast<int>(wj >> 20) + k <= best) break;
+        const uint32_t hi_j = a_hi(j);
+        if ((hi_i ^ hi_j) >> 31) break;  // strand change
+        const uint32_t dr = hi_i - hi_j;  // same strand, sorted: rpos_i - rpos_j >= 0
+        if (dr > max_gap) break;
+        const int32_t dq = qi - static_cast<int32_t>(a_lo(j));
+        if (dr == 0 || dq <= 0) continue;
+        const int32_t dri = static_cast<int32_t>(dr);  // <= max_gap < 2^29
+        const int32_t dd = dri > dq ? dri - dq : dq - dri;
         if (dd > cp.band) continue;
-        int g = dq < dr ? dq : static_cast<int>(dr);
+        int g = dq < dri ? dq : dri;
         if (g > k) g = k;
-        const int sc = (fp_at(j) >> 8) + g - __ldg(cp.cost + dd);
+        const int sc = f_of(wj) + g - lut[dd];
         if (sc > best) {
           best = sc;
           bj = j;
         }
       }
-      fp_at(i) = best << 8 | (bj + 1);
+      pm = best > pm ? best : pm;
+      fp_at(i) = static_cast<uint32_t>(bj + 1) | static_cast<uint32_t>(best) << 8 | static_cast<uint32_t>(pm) << 20;
     }
     // ---- chains (src/chain.cpp:47-68)
     uint32_t used = 0;
@@ -281,7 +298,7 @@ __global__ void __launch_bounds__(kTT)
     for (;;) {
       int end = -1, bf = INT_MIN;
       for (int i = 0; i < na; ++i) {
-        const int f = fp_at(i) >> 8;
+        const int f = f_of(fp_at(i));
         if (!((used >> i) & 1u) && f > bf) {
           bf = f;
           end = i;
@@ -293,23 +310,22 @@ __global__ void __launch_bounds__(kTT)
       while (i >= 0 && !((used >> i) & 1u)) {
         used |= 1u << i;
         ++cnt;
-        const uint64_t key = key_ld(i);
-        const int32_t d = static_cast<int32_t>(key_rpos(key)) - key_qpos(key);
+        const int32_t d = static_cast<int32_t>(a_hi(i) & 0x7FFFFFFFu) - static_cast<int32_t>(a_lo(i));
         dmin = d < dmin ? d : dmin;
         dmax = d > dmax ? d : dmax;
-        i = (fp_at(i) & 0xFF) - 1;
+        i = static_cast<int>(fp_at(i) & 0xFFu) - 1;
       }
-      const int score = bf - (i >= 0 ? (fp_at(i) >> 8) : 0);
+      const int score = bf - (i >= 0 ? f_of(fp_at(i)) : 0);
       if (score < cp.min_score || cnt < cp.min_anchors) continue;
       if (nch == kTMaxChains) {
         big = true;
         break;
       }
-      const uint64_t ke = key_ld(end);
+      const uint32_t he = a_hi(end);
       ch_at(0, nch) = score;
-      ch_at(1, nch) = static_cast<int32_t>(key_strand(ke));
+      ch_at(1, nch) = static_cast<int32_t>(he >> 31);
       ch_at(2, nch) = dmin + (dmax - dmin) / 2;
-      ch_at(3, nch) = static_cast<int32_t>(key_rpos(ke));
+      ch_at(3, nch) = static_cast<int32_t>(he & 0x7FFFFFFFu);
       ++nch;
     }
     // ---- candidate loci (src/mapper.cpp:40-62), chains by (score desc, extraction order)
@@ -362,7 +378,7 @@ __global__ void __launch_bounds__(kTT)
 
 bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp) {
   return sp.w == kTW && sp.k >= 4 && sp.k <= 15 && cp.max_gap >= 0 && cp.max_gap < (1 << 29) && cp.band >= 0 &&
-         cp.lookback >= 0;
+         cp.band <= kTMaxBand && cp.lookback >= 0;
 }
 
 bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
