@@ -335,9 +335,11 @@ __device__ bool window_has_n(const SwTask& tk, int W, const uint8_t* __restrict_
 
 // Two alignments per thread in biased 16-bit halves (A low, B high). Pairs it cannot take
 // (an N in a target window, or scores/lengths outside the 16-bit range) are listed in
-// fb (fb[0] = count, then local task indices) for k_sw_fb.
+// fb (fb[0] = count, then local task indices) for k_sw_fb. With traceback at W <= 33 the
+// launch bound asks for three resident blocks (<= 170 registers, no spills), which gives
+// the latency-bound recurrence 12 warps per SM instead of 8.
 template <int W, bool TB>
-__global__ void __launch_bounds__(kSwThreads) k_sw_u2(const SwTask* __restrict__ tasks, int base, int n,
+__global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1) k_sw_u2(const SwTask* __restrict__ tasks, int base, int n,
                                                       const int* __restrict__ n_dev, const uint8_t* __restrict__ qbase,
                                                       const uint8_t* __restrict__ tbase, SwParams p,
                                                       SwResult* __restrict__ res, uint32_t* __restrict__ dir,
@@ -384,7 +386,13 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_u2(const SwTask* __restrict__
   const uint32_t OE = pack2(p.oe), GE = pack2(p.ge), SB = pack2(kScoreBias);
   uint32_t best2 = kBias2;
   uint32_t best_a = kBias, best_b = kBias;
-  int bi_a = -1, bd_a = -1, bi_b = -1, bd_b = -1;
+  int bi_a = -1, bi_b = -1;
+  // With traceback, each half's best row is kept in shared memory ([d][thread] words) the
+  // moment it improves the best score, and its first maximal column is found once, after
+  // the last row: one max per cell instead of tracking the argmax per cell.
+  extern __shared__ uint32_t sw_rows[];
+  uint32_t* const row_a = sw_rows + threadIdx.x;
+  uint32_t* const row_b = sw_rows + W * kSwThreads + threadIdx.x;
   uint32_t ca = qcode(qa, qla, 0), cb = qcode(qb, qlb, 0);
   for (int i = 0; i < qmax; ++i) {
     // rows past a query's end are N rows for it: they cannot raise its best (values only
@@ -394,7 +402,6 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_u2(const SwTask* __restrict__
     const uint32_t t_next = tc2(static_cast<int64_t>(i) + W);
     const uint32_t ca_next = qcode(qa, qla, i + 1), cb_next = qcode(qb, qlb, i + 1);
     uint32_t f = kBias2, hleft = kBias2, hdiag = H[0], rmax = 0, dw = 0;
-    int rda = 0, rdb = 0;
 #pragma unroll
     for (int d = 0; d < W; ++d) {
       const uint32_t hup = H[d + 1], eup = E[d + 1];
@@ -416,31 +423,25 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_u2(const SwTask* __restrict__
           DP[(static_cast<size_t>(i) * WQ + (d >> 2)) * 32] = dw;
           dw = 0;
         }
-        if (d == 0) {
-          rmax = h;
-        } else {  // first strict maximum of the row, per half
-          const uint32_t nm = __vmaxu2(rmax, h);
-          const uint32_t up = nm ^ rmax;  // nonzero half where h beat the row maximum
-          rda = (up & 0xFFFFu) ? d : rda;
-          rdb = (up >> 16) ? d : rdb;
-          rmax = nm;
-        }
+        rmax = d == 0 ? h : __vmaxu2(rmax, h);
       } else {
         best2 = __vmaxu2(best2, h);
       }
       hleft = h;
       hdiag = hup;
     }
-    if constexpr (TB) {
+    if constexpr (TB) {  // a strictly better row (rows in order: the first strict maximum)
       if ((rmax & 0xFFFFu) > best_a) {
         best_a = rmax & 0xFFFFu;
         bi_a = i;
-        bd_a = rda;
+#pragma unroll
+        for (int d = 0; d < W; ++d) row_a[d * kSwThreads] = H[d];
       }
       if ((rmax >> 16) > best_b) {
         best_b = rmax >> 16;
         bi_b = i;
-        bd_b = rdb;
+#pragma unroll
+        for (int d = 0; d < W; ++d) row_b[d * kSwThreads] = H[d];
       }
     }
 #pragma unroll
@@ -449,12 +450,21 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_u2(const SwTask* __restrict__
     ca = ca_next;
     cb = cb_next;
   }
+  int bd_a = 0, bd_b = 0;
   if constexpr (!TB) {
     best_a = best2 & 0xFFFFu;
     best_b = best2 >> 16;
+  } else {  // first column of the best row holding the best value, per half
+    bd_a = bi_a >= 0 ? W : -1;
+    bd_b = bi_b >= 0 ? W : -1;
+#pragma unroll 1
+    for (int d = W - 1; d >= 0; --d) {
+      if (bi_a >= 0 && (row_a[d * kSwThreads] & 0xFFFFu) == best_a) bd_a = d;
+      if (bi_b >= 0 && (row_b[d * kSwThreads] >> 16) == best_b) bd_b = d;
+    }
   }
-  res[ta.slot] = stash(static_cast<int>(best_a) - static_cast<int>(kBias), TB ? bi_a : 0, TB ? bd_a : 0);
-  if (has_b) res[tb.slot] = stash(static_cast<int>(best_b) - static_cast<int>(kBias), TB ? bi_b : 0, TB ? bd_b : 0);
+  res[ta.slot] = stash(static_cast<int>(best_a) - static_cast<int>(kBias), TB ? bi_a : 0, bd_a);
+  if (has_b) res[tb.slot] = stash(static_cast<int>(best_b) - static_cast<int>(kBias), TB ? bi_b : 0, bd_b);
 }
 
 // The pairs k_sw_u2 listed, one alignment per thread, int32.
@@ -579,9 +589,18 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
   const KernelTrace& t = kt ? *kt : none;
   cudaMemsetAsync(fb, 0, sizeof(int), st);
   if (tb) {
+    constexpr int kRowBytes = 2 * W * kSwThreads * 4;  // the two saved best rows of each thread
+    if (kRowBytes > 48 * 1024) {
+      static bool attr_set[64] = {};
+      int dev = 0;
+      if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && !attr_set[dev] &&
+          cudaFuncSetAttribute(k_sw_u2<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowBytes) ==
+              cudaSuccess)
+        attr_set[dev] = true;
+    }
     t.begin(st, "k_sw_u2<tb>");
-    k_sw_u2<W, true><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max,
-                                                          fb);
+    k_sw_u2<W, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
+                                                                  rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<tb>");
     k_sw_fb<W, true><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
