@@ -47,6 +47,9 @@ constexpr int kTMaxMin = 32;              // minimizers per read
 constexpr int kTMaxAnc = 32;              // anchors per read (one bit each in a 32-bit mask)
 constexpr int kTMaxChains = 8;            // chains per read passing the score / anchor filters
 constexpr int kTW = 10;                   // window length of the compiled sketch
+constexpr int kEncGroup = 4;              // reads whose bytes a warp loads at once
+constexpr int kEncPer = kTMaxLen / 32;    // byte positions per lane and staged read
+constexpr int kProbe = 8;                 // minimizers probed with independent loads at once
 
 // Dynamic shared memory of a block: two regions of 32-bit words, each thread owning one
 // column of each (word w of thread T at w * pitch + T), so that after the cooperative
@@ -107,23 +110,51 @@ __global__ void __launch_bounds__(kTT)
     po = pofs[r];
   }
 
-  // ---- cooperative encode: codes of both strands to HBM, staged codes to shared memory
-  for (int j = 0; j < 32; ++j) {
-    if (r0 + j >= n) break;
-    const int lj = __shfl_sync(0xffffffffu, len, j);
-    const int64_t sj = __shfl_sync(0xffffffffu, soff, j);
-    const int64_t pj = __shfl_sync(0xffffffffu, po, j);
-    const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + sj;
-    uint8_t* fw = codes + 2 * pj;
-    uint8_t* rc = fw + lj;
-    uint8_t* st8 = reinterpret_cast<uint8_t*>(stg);
-    const int tj = (T & ~31) + j;
-    const bool stage = lj <= kTMaxLen;
-    for (int i = lane; i < lj; i += 32) {
-      const uint8_t c = static_cast<uint8_t>(nt4(s[i]));
-      fw[i] = c;
-      rc[lj - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
-      if (stage) st8[((i >> 2) * kTPitch + tj) * 4 + (i & 3)] = c;
+  // ---- cooperative encode: codes of both strands to HBM, staged codes to shared memory.
+  // Reads go in groups of kEncGroup; all byte loads of a group (coalesced across the lanes)
+  // are issued before any is used, so the group costs one memory latency, not one per byte
+  // position.
+  uint8_t* const st8 = reinterpret_cast<uint8_t*>(stg);
+  for (int j0 = 0; j0 < 32; j0 += kEncGroup) {
+    if (r0 + j0 >= n) break;
+    uint32_t by[kEncGroup][kEncPer];
+    int lg[kEncGroup];
+    int64_t sg[kEncGroup], pg[kEncGroup];
+#pragma unroll
+    for (int q = 0; q < kEncGroup; ++q) {
+      lg[q] = __shfl_sync(0xffffffffu, len, j0 + q);  // 0 past the batch
+      sg[q] = __shfl_sync(0xffffffffu, soff, j0 + q);
+      pg[q] = __shfl_sync(0xffffffffu, po, j0 + q);
+      const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + sg[q];
+#pragma unroll
+      for (int u = 0; u < kEncPer; ++u) {
+        const int i = lane + 32 * u;
+        by[q][u] = i < lg[q] ? s[i] : 0u;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kEncGroup; ++q) {
+      const int lj = lg[q];
+      const int tj = (T & ~31) + j0 + q;
+      uint8_t* fw = codes + 2 * pg[q];
+      uint8_t* rc = fw + lj;
+      const bool stage = lj <= kTMaxLen;
+#pragma unroll
+      for (int u = 0; u < kEncPer; ++u) {
+        const int i = lane + 32 * u;
+        if (i < lj) {
+          const uint8_t c = static_cast<uint8_t>(nt4(by[q][u]));
+          fw[i] = c;
+          rc[lj - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
+          if (stage) st8[((i >> 2) * kTPitch + tj) * 4 + (i & 3)] = c;
+        }
+      }
+      const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + sg[q];
+      for (int i = lane + 32 * kEncPer; i < lj; i += 32) {  // the rest of a read too long to stage
+        const uint8_t c = static_cast<uint8_t>(nt4(s[i]));
+        fw[i] = c;
+        rc[lj - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
+      }
     }
   }
   __syncwarp();
@@ -194,39 +225,69 @@ __global__ void __launch_bounds__(kTT)
   // ---- probe and anchors (src/mapper.cpp:16-40); region A becomes the anchor keys
   int na = 0;
   if (!big) {
-    for (int j0 = 0; j0 < nmin && !big; j0 += 4) {
-      uint2 m[4];
-      ulonglong2 b[4];
+    for (int j0 = 0; j0 < nmin && !big; j0 += kProbe) {
+      // kProbe keys walk the table (src/index.hpp:24-38) in lockstep rounds: each round
+      // loads the next bucket of every key still unresolved, as independent loads, so
+      // colliding keys cost the longest chain of the group, not the sum of the chains.
+      uint2 m[kProbe];
+      ulonglong2 bk[kProbe];
+      uint64_t slot[kProbe];
+      uint32_t pending = 0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < kProbe; ++q) {
         m[q] = make_uint2(0, 0);
-        b[q] = make_ulonglong2(kInvalidHash, 0);
+        bk[q] = make_ulonglong2(kInvalidHash, 0);
+        slot[q] = 0;
         if (j0 + q < nmin) {
           m[q] = make_uint2(cbw[2 * (j0 + q) * kTT], cbw[(2 * (j0 + q) + 1) * kTT]);
-          b[q] = __ldg(ix.table + (static_cast<uint64_t>(m[q].x) & ix.mask));
+          slot[q] = static_cast<uint64_t>(m[q].x) & ix.mask;
+          bk[q] = __ldg(ix.table + slot[q]);
+          pending |= 1u << q;
         }
       }
+      uint32_t off[kProbe], cnt[kProbe], v0[kProbe];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (j0 + q >= nmin || big) break;
-        const uint64_t h = m[q].x;
-        uint32_t off = 0, cnt = 0;
-        if (b[q].x == h) {
-          off = static_cast<uint32_t>(b[q].y);
-          cnt = static_cast<uint32_t>(b[q].y >> 32);
-        } else if (b[q].x != kInvalidHash) {
-          probe(ix, h, off, cnt, err);  // a collision in the first bucket: walk on
+      for (int q = 0; q < kProbe; ++q) off[q] = cnt[q] = 0;
+      for (uint64_t round = 0; pending; ++round) {
+        if (round > ix.mask) {  // the table is at most half full: an empty bucket ends every walk
+          atomicOr(err, kErrProbeLoop);
+          break;
         }
-        if (cnt > sp.max_occ) cnt = 0;
-        if (cnt == 0) continue;
-        if (na + static_cast<int>(cnt) > kTMaxAnc) {
+        uint32_t next = 0;
+#pragma unroll
+        for (int q = 0; q < kProbe; ++q) {
+          if ((pending >> q) & 1u) {
+            if (bk[q].x == static_cast<uint64_t>(m[q].x)) {
+              off[q] = static_cast<uint32_t>(bk[q].y);
+              cnt[q] = static_cast<uint32_t>(bk[q].y >> 32);
+            } else if (bk[q].x != kInvalidHash) {
+              slot[q] = (slot[q] + 1) & ix.mask;
+              next |= 1u << q;
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kProbe; ++q)
+          if ((next >> q) & 1u) bk[q] = __ldg(ix.table + slot[q]);
+        pending = next;
+      }
+#pragma unroll
+      for (int q = 0; q < kProbe; ++q) {
+        if (cnt[q] > sp.max_occ) cnt[q] = 0;
+        v0[q] = cnt[q] ? __ldg(ix.positions + off[q]) : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < kProbe; ++q) {
+        if (j0 + q >= nmin || big) break;
+        if (cnt[q] == 0) continue;
+        if (na + static_cast<int>(cnt[q]) > kTMaxAnc) {
           big = true;
           break;
         }
         const int32_t pos = static_cast<int32_t>(m[q].y & 0x7FFFFFFFu);
         const uint32_t mst = m[q].y >> 31;
-        for (uint32_t t = 0; t < cnt; ++t) {
-          const uint32_t v = __ldg(ix.positions + off + t);
+        for (uint32_t t = 0; t < cnt[q]; ++t) {
+          const uint32_t v = t == 0 ? v0[q] : __ldg(ix.positions + off[q] + t);
           const uint32_t rv = (v & 1u) ^ mst;
           const int32_t qpos = rv ? len - pos - k : pos;
           a_hi(na) = rv << 31 | v >> 1;
