@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--n-reads", type=int, default=None, help="override the workload's read count (testing)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    help="synthetic workload (dnaln_b200.synth.WORKLOADS); the default is the headline one")
+    ap.add_argument("--bw", type=int, default=16, help="SW band half-width (16, or 64 for the mixed-length workload)")
     return ap.parse_args()
 
 
@@ -99,11 +102,18 @@ class ClockSampler(threading.Thread):
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
-def workload_config(n_reads: int, world: int) -> dict:
-    return {"workload": f"{WORKLOAD}: 4.6 Mbp i.i.d. genome (P(G)=P(C)=0.254), {n_reads:,} x 150 bp reads "
-                        "(1% substitution, 0.1% indel), k=15 w=10 bw=16 A2 B4 O4 E2, batches of 262,144",
-            "reads_per_step": n_reads, "batch": BATCH, "genome_bp": 4_600_000,
-            "l2": "no flush: each step streams 150 MB of reads (> 126 MB L2) plus ~1 GB of scratch",
+def workload_config(n_reads: int, world: int, name: str = WORKLOAD, bw: int = 16, genome_bp: int = 4_600_000,
+                    mean_len: float = 150.0) -> dict:
+    if name == WORKLOAD:
+        desc = (f"{WORKLOAD}: 4.6 Mbp i.i.d. genome (P(G)=P(C)=0.254), {n_reads:,} x 150 bp reads "
+                f"(1% substitution, 0.1% indel), k=15 w=10 bw={bw} A2 B4 O4 E2, batches of 262,144")
+    else:
+        from dnaln_b200 import synth
+        desc = f"{name}: {synth.WORKLOADS[name][2]}, {n_reads:,} reads, k=15 w=10 bw={bw} A2 B4 O4 E2"
+    return {"workload": desc, "reads_per_step": n_reads, "batch": BATCH, "genome_bp": genome_bp,
+            "mean_read_len": round(mean_len, 1),
+            "l2": f"no flush: each step streams {n_reads * mean_len / 1e6:.0f} MB of reads plus the per-batch "
+                  "scratch (both well above the 126 MB L2)",
             "parallelism": f"dp{world} read shards, index replica per GPU"}
 
 
@@ -189,8 +199,8 @@ def run_reference(args) -> None:
     import oracle
     import dnaln_b200 as D
     from dnaln_b200 import synth
-    g, reads, _ = synth.workload(WORKLOAD, seed=args.seed, n_reads=args.n_reads)
-    p = D.default_map_params()
+    g, reads, _ = synth.workload(args.workload, seed=args.seed, n_reads=args.n_reads)
+    p = D.default_map_params(bw=args.bw)
     threads = len(os.sched_getaffinity(0))
     if oracle.REF_SO.exists():
         ref, kind = oracle.Reference(), "reference"
@@ -215,7 +225,8 @@ def run_reference(args) -> None:
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
-            "config": workload_config(len(sample), 1), "impl": "reference",
+            "config": workload_config(len(sample), 1, args.workload, args.bw, len(g.codes),
+                                      float(np.mean(sample.seq_len))), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind,
                              "sample": f"{len(sample):,} reads per step, Mapper::map, {cores} threads",
                              "cpu": _cpu_model()},
@@ -237,11 +248,13 @@ def run_ours(args) -> None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
 
-    g, reads, _ = synth.workload(WORKLOAD, seed=args.seed + 7919 * rank, n_reads=args.n_reads)
+    g, reads, _ = synth.workload(args.workload, seed=args.seed + 7919 * rank, n_reads=args.n_reads)
     n_reads = len(reads)
-    p = D.default_map_params()
+    p = D.default_map_params(bw=args.bw)
     ctx = D.Context(local)
+    t_ix = time.perf_counter()
     iid = ctx.index_build(g)
+    index_build_s = time.perf_counter() - t_ix
     L = N.lib()
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
@@ -381,7 +394,7 @@ def run_ours(args) -> None:
     mean_len = float(np.mean(reads.seq_len))
     launches, dom_ms = ktimes[dom]
     avg_launch_ms = dom_ms / launches
-    algo = kernel_bytes(dom, st, mean_len)
+    algo = kernel_bytes(dom, st, mean_len, args.bw)
     peak, peak_kind = measured_peaks()
     achieved = (algo / launches) / (avg_launch_ms / 1e3) / 1e9 if algo is not None else None
     traffic = None  # DRAM bytes per launch of this kernel from the committed ncu summary
@@ -402,7 +415,7 @@ def run_ours(args) -> None:
     out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, no dataset)",
-           "config": workload_config(n_reads, world),
+           "config": workload_config(n_reads, world, args.workload, args.bw, len(g.codes), mean_len),
            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                    "ms_per_step": ms_e2e / e2e_steps, "wall_s": wall_e2e},
            "gpu_launches": int(st["launches"]),
@@ -416,8 +429,11 @@ def run_ours(args) -> None:
            "sw_gcups": cells / (sw_ms / 1e3) / 1e9 if sw_ms > 0 else None,
            "sw_cells_per_step": cells / args.steps,
            "mapped_frac": st["mapped"] / max(st["reads"], 1),
-           "clocks": clk}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+           "clocks": clk,
+           "index": dict(build_s=index_build_s, where="dnaln_gpu_index_build",
+                         **{k: v for k, v in ctx.index_stats(iid).items() if k in ("n_keys", "device_bytes")}),
+           "candidates_per_read": st["candidates"] / max(st["reads"], 1)}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == WORKLOAD:
         out["cpu_baseline"] = cpu_baseline(g, reads, p)
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -15,6 +15,7 @@
 // the host only waits where it must size a buffer. The host-buffer entry point splits a
 // batch into sub-batches and overlaps their copies in and out with the compute (two
 // device slots, two copy streams); it knows the lengths, so it skips the first read-back.
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -321,6 +322,39 @@ int check_device_errors(dnaln_ctx* c, uint32_t bits) {
               !!(bits & kErrProbeLoop));
 }
 
+// SW tasks of a batch whose reads differ in length, longest first (a thread's two
+// alignments and a warp's 64 then have similar lengths, so no lane idles through a long
+// partner's rows). *sorted = tasks when there is nothing to gain.
+int sort_tasks_by_length(dnaln_ctx* c, const SwTask* tasks, int n_max, const int* n_dev, const char* tag,
+                         const SwTask** sorted) {
+  *sorted = tasks;
+  if (n_max < 2) return DNALN_OK;
+  const std::string t = tag;
+  DBUF(keys_in, uint32_t, (t + "_kin").c_str(), n_max);
+  DBUF(keys_out, uint32_t, (t + "_kout").c_str(), n_max);
+  DBUF(idx_in, int32_t, (t + "_iin").c_str(), n_max);
+  DBUF(idx_out, int32_t, (t + "_iout").c_str(), n_max);
+  DBUF(out, SwTask, (t + "_sorted").c_str(), n_max);
+  const KernelTrace kt = tracer(c);
+  kt.begin(c->st, "k_task_keys");
+  launch_task_keys(c->st, tasks, n_max, n_dev, keys_in, idx_in);
+  kt.end(c->st);
+  size_t tmp = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys_in, keys_out, idx_in, idx_out, n_max, 0, 17, c->st));
+  DBUF(tb, uint8_t, "cub_tmp_sort", tmp);
+  kt.begin(c->st, "cub_sort");
+  const cudaError_t e = cub::DeviceRadixSort::SortPairs(tb, tmp, keys_in, keys_out, idx_in, idx_out, n_max, 0, 17,
+                                                        c->st);
+  kt.end(c->st);
+  CK(e);
+  kt.begin(c->st, "k_task_gather");
+  launch_task_gather(c->st, tasks, n_max, n_dev, idx_out, out);
+  kt.end(c->st);
+  c->stats.launches += 2;
+  *sorted = out;
+  return DNALN_OK;
+}
+
 // Launches traceback SW over tasks [0, n_max) (count read on the device from n_dev),
 // chunked so the direction-bit scratch stays within dir_cap_bytes.
 int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks, int n_max, const int* n_dev,
@@ -519,7 +553,12 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   kt.begin(st, "k_score_tasks");
   launch_score_tasks(st, n, pofs, d_seq_len, cb, ix.dev, mc, sc_tasks, c->d_count, ctr);
   kt.end(st);
-  if (int e = launch_sw_chunked(c, false, bytes_ok, sc_tasks, static_cast<int>(n * MC), c->d_count, codes,
+  // reads of very different lengths: SW tasks longest first (lengths known on the host)
+  const bool by_length = static_cast<double>(max_len) > 1.25 * static_cast<double>(B) / static_cast<double>(n);
+  const SwTask* sc_run = sc_tasks;
+  if (by_length)
+    if (int e = sort_tasks_by_length(c, sc_tasks, static_cast<int>(n * MC), c->d_count, "sc", &sc_run)) return e;
+  if (int e = launch_sw_chunked(c, false, bytes_ok, sc_run, static_cast<int>(n * MC), c->d_count, codes,
                                 ix.dev.genome, swp, res_sc, static_cast<int>(max_len), nullptr, nullptr))
     return e;
   CK(cudaEventRecord(c->ev[kEvSc1], st));
@@ -538,7 +577,10 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   kt.begin(st, "k_cig_slots");
   k_cig_slots<<<nblk(n), 256, 0, st>>>(pofs, n, cig_slot);
   kt.end(st);
-  if (int e = launch_sw_chunked(c, true, bytes_ok, tb_tasks, static_cast<int>(n), c->d_count + 1, codes,
+  const SwTask* tb_run = tb_tasks;
+  if (by_length)
+    if (int e = sort_tasks_by_length(c, tb_tasks, static_cast<int>(n), c->d_count + 1, "tb", &tb_run)) return e;
+  if (int e = launch_sw_chunked(c, true, bytes_ok, tb_run, static_cast<int>(n), c->d_count + 1, codes,
                                 ix.dev.genome, swp, res_tb, static_cast<int>(max_len), cig_tb, cig_slot))
     return e;
   CK(cudaEventRecord(c->ev[kEvTb1], st));

@@ -258,4 +258,35 @@ void launch_align_gather(cudaStream_t st, int64_t n, const SwResult* res, const 
   if (n > 0) k_align_gather<<<blocks_for(n), kThreads, 0, st>>>(n, res, cig_src, src_off, dst_off, out, dst);
 }
 
+namespace {
+
+__global__ void k_task_keys(const SwTask* __restrict__ tasks, int n_max, const int* __restrict__ n_dev,
+                            uint32_t* __restrict__ keys, int32_t* __restrict__ idx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_max) return;
+  const int n = n_dev ? min(n_max, *n_dev) : n_max;
+  const int ql = i < n ? min(tasks[i].qlen, 0xFFFF) : 0;
+  keys[i] = i < n ? 0xFFFFu - static_cast<uint32_t>(ql) : 0x10000u;  // longest first, unused slots last
+  idx[i] = i;
+}
+
+__global__ void k_task_gather(const SwTask* __restrict__ tasks, int n_max, const int* __restrict__ n_dev,
+                              const int32_t* __restrict__ order, SwTask* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = n_dev ? min(n_max, *n_dev) : n_max;
+  if (i < n) out[i] = tasks[order[i]];
+}
+
+}  // namespace
+
+void launch_task_keys(cudaStream_t st, const SwTask* tasks, int n_max, const int* n_dev, uint32_t* keys,
+                      int32_t* idx) {
+  if (n_max > 0) k_task_keys<<<blocks_for(n_max), kThreads, 0, st>>>(tasks, n_max, n_dev, keys, idx);
+}
+
+void launch_task_gather(cudaStream_t st, const SwTask* tasks, int n_max, const int* n_dev, const int32_t* order,
+                        SwTask* out) {
+  if (n_max > 0) k_task_gather<<<blocks_for(n_max), kThreads, 0, st>>>(tasks, n_max, n_dev, order, out);
+}
+
 }  // namespace dnb

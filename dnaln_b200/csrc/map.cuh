@@ -45,4 +45,12 @@ void launch_align_gather(cudaStream_t st, int64_t n, const SwResult* res, const 
 // ops count per align result -> counts[i] (for the scan of dst offsets)
 void launch_align_counts(cudaStream_t st, int64_t n, const SwResult* res, int64_t* counts);
 
+// Length order of SW tasks (tasks of similar length share a thread and a warp): sort keys
+// (longest first; slots at or past the device count *n_dev last) and identity values.
+void launch_task_keys(cudaStream_t st, const SwTask* tasks, int n_max, const int* n_dev, uint32_t* keys,
+                      int32_t* idx);
+// out[i] = tasks[order[i]] for i below the device count.
+void launch_task_gather(cudaStream_t st, const SwTask* tasks, int n_max, const int* n_dev, const int32_t* order,
+                        SwTask* out);
+
 }  // namespace dnb

@@ -467,6 +467,207 @@ __global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1) k_sw_u2(c
   if (has_b) res[tb.slot] = stash(static_cast<int>(best_b) - static_cast<int>(kBias), TB ? bi_b : 0, bd_b);
 }
 
+// Wide bands, W = 32 * LANES + 1: LANES consecutive lanes of a warp share one pair of
+// alignments (A and B in the 16-bit halves, as in k_sw_u2), lane c holding band cells
+// [32c, 32c + 32) of the row in registers (the last lane also cell W - 1). Lane c works on
+// row t - c at step t, so its left neighbour finished the same row one step earlier: the
+// row's running F and H(left) arrive by one shuffle at the start of the step. The one value
+// a lane needs from its right neighbour — H and E of the previous row at the neighbour's
+// first cell (the E input of the lane's last cell) — is exactly what the neighbour
+// computes first in the same step, so a second shuffle after each lane's first cell
+// delivers it; every lane is busy on every step. Each lane tracks the first strict
+// maximum of its own cells (best-row checkpoint in shared memory, as k_sw_u2), and the
+// lanes of a pair combine (value, then earliest row, then smallest column) at the end:
+// the first strict maximum of the whole band in row-major order. Pairs k_sw_u2 would
+// hand to the int32 kernel are listed in fb the same way.
+template <int LANES, bool TB>
+__global__ void __launch_bounds__(kSwThreads, TB ? 3 : 1)
+    k_sw_wide(const SwTask* __restrict__ tasks, int base, int n, const int* __restrict__ n_dev,
+              const uint8_t* __restrict__ qbase, const uint8_t* __restrict__ tbase, SwParams p,
+              SwResult* __restrict__ res, uint32_t* __restrict__ dir, int rows_max, int* __restrict__ fb) {
+  constexpr int W = 32 * LANES + 1, WQ = (W + 3) / 4, CH = 32;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int c = lane % LANES;  // chunk of this lane
+  const int lt = (blockIdx.x * blockDim.x + threadIdx.x) / LANES;  // pair index within this launch
+  const int nn = n_dev ? min(n, *n_dev) : n;
+  const int warp_first = (blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / LANES;
+  if (base + 2 * warp_first >= nn) return;  // the whole warp is past the tasks (warp-uniform)
+  const int ia = base + 2 * lt, ib = ia + 1;
+  const bool live = ia < nn, has_b = ib < nn;
+  SwTask ta{}, tb{};
+  if (live) ta = tasks[ia];
+  if (has_b) tb = tasks[ib];
+  else tb = ta, tb.qlen = 0;
+  const int qmax = live ? max(ta.qlen, tb.qlen) : 0;
+  const bool fits = qmax * p.match + 2 * (p.oe + p.ge + p.mismatch + p.ambig) < 16000 &&
+                    p.match + kScoreBias <= 127 && p.mismatch <= kScoreBias && p.ambig <= kScoreBias;
+  bool skip = !live;
+  if (live && (!fits || window_has_n(ta, W, tbase) || (has_b && window_has_n(tb, W, tbase)))) {
+    skip = true;
+    if (c == 0) {
+      const int k = atomicAdd(fb, has_b ? 2 : 1);
+      fb[1 + k] = 2 * lt;
+      if (has_b) fb[2 + k] = 2 * lt + 1;
+    }
+  }
+  const int steps = __reduce_max_sync(FULL, skip ? 0 : qmax + LANES - 1);
+  uint32_t* DP = TB ? pair_base(dir, 2 * lt, rows_max, WQ) : nullptr;
+  const uint8_t* __restrict__ qa = qbase + ta.q_off;
+  const uint8_t* __restrict__ qb = qbase + tb.q_off;
+  const int qla = ta.qlen, qlb = tb.qlen;
+  auto tc2 = [&](int64_t j) {
+    const uint32_t a = tcode(tbase, ta, j), b = has_b ? tcode(tbase, tb, j) : 0u;
+    return sel2(a > 3 ? 0u : a, b > 3 ? 0u : b);
+  };
+  auto qcode = [&](const uint8_t* __restrict__ q, int ql, int i) {
+    return i >= 0 && i < ql ? min(static_cast<uint32_t>(q[i]), 4u) : 4u;
+  };
+  const int d0 = CH * c;  // band column of local cell 0
+  uint32_t H[CH + 2], E[CH + 2], T[CH + 1];
+#pragma unroll
+  for (int k = 0; k < CH + 2; ++k) {
+    H[k] = kBias2;
+    E[k] = kBias2;
+  }
+#pragma unroll
+  for (int k = 0; k <= CH; ++k) T[k] = skip ? 0u : tc2(d0 + k);  // row 0
+  const uint32_t OE = pack2(p.oe), GE = pack2(p.ge), SB = pack2(kScoreBias);
+  uint32_t best2 = kBias2, best_a = kBias, best_b = kBias;
+  int bi_a = -1, bi_b = -1;
+  extern __shared__ uint32_t sw_rows[];
+  uint32_t* const row_a = sw_rows + threadIdx.x;
+  uint32_t* const row_b = sw_rows + (CH + 1) * kSwThreads + threadIdx.x;
+  uint32_t hout = kBias2, fout = kBias2;  // this lane's last cell of its previous row
+  for (int t = 0; t < steps; ++t) {
+    const int i = t - c;
+    const bool act = !skip && i >= 0 && i < qmax;
+    // row i's F and H(left) at column d0 - 1, from the left lane (its step t - 1)
+    uint32_t hleft = __shfl_up_sync(FULL, hout, 1), f = __shfl_up_sync(FULL, fout, 1);
+    if (c == 0) hleft = f = kBias2;
+    const uint32_t ca = qcode(qa, qla, i), cb = qcode(qb, qlb, i);
+    const uint32_t plo = prof_biased(p, ca), phi = prof_biased(p, cb);
+    const uint32_t t_next = act ? tc2(static_cast<int64_t>(i) + 1 + d0 + CH) : 0u;
+    uint32_t hdiag = H[0], rmax = 0, dw = 0;
+    // local cell 0, then hand (H, E) of it to the left lane: the E input of its last cell
+    uint32_t h0, e0;
+    {
+      const uint32_t hup = H[1], eup = E[1];
+      const uint32_t hd = hdiag + prmt(plo, phi, T[0]) - SB;
+      const uint32_t eo = hup - OE, ee = eup - GE, fo = hleft - OE, fe = f - GE;
+      e0 = __vmaxu2(eo, ee);
+      f = __vmaxu2(fo, fe);
+      const uint32_t m1 = __vmaxu2(hd, e0);
+      h0 = __vimax3_u16x2(m1, f, kBias2);
+      if constexpr (TB)
+        dw = ((__vminu2(m1 - hd, kOne2) * 2u + __vminu2(h0 - m1, kOne2)) * 2u + __vminu2(e0 - eo, kOne2)) * 2u +
+             __vminu2(f - fo, kOne2);
+      rmax = h0;
+      hleft = h0;
+      hdiag = hup;
+    }
+    // a lane that has not reached row 0 passes row -1's values (zero)
+    uint32_t nh = __shfl_down_sync(FULL, i >= 0 ? h0 : kBias2, 1);
+    uint32_t ne = __shfl_down_sync(FULL, i >= 0 ? e0 : kBias2, 1);
+    if (c == LANES - 1) {
+      nh = H[CH];
+      ne = E[CH];
+    }
+    if (act) {
+      H[0] = h0;
+      E[0] = e0;
+    }
+#pragma unroll
+    for (int k = 1; k <= CH; ++k) {
+      if (k == CH && c != LANES - 1) break;  // the extra cell W - 1 belongs to the last lane
+      const uint32_t hup = k == CH - 1 ? nh : (k == CH ? kBias2 : H[k + 1]);
+      const uint32_t eup = k == CH - 1 ? ne : (k == CH ? kBias2 : E[k + 1]);
+      const uint32_t hd = hdiag + prmt(plo, phi, T[k]) - SB;
+      const uint32_t eo = hup - OE, ee = eup - GE, fo = hleft - OE, fe = f - GE;
+      const uint32_t e = __vmaxu2(eo, ee);
+      f = __vmaxu2(fo, fe);
+      const uint32_t m1 = __vmaxu2(hd, e);
+      const uint32_t h = __vimax3_u16x2(m1, f, kBias2);
+      if (act) {
+        H[k] = h;
+        E[k] = e;
+      }
+      if constexpr (TB) {
+        const uint32_t code = ((__vminu2(m1 - hd, kOne2) * 2u + __vminu2(h - m1, kOne2)) * 2u +
+                               __vminu2(e - eo, kOne2)) * 2u + __vminu2(f - fo, kOne2);
+        dw = dw * 16u + code;
+        if ((k & 3) == 3) {
+          if (act) DP[(static_cast<size_t>(i) * WQ + ((d0 + k) >> 2)) * 32] = dw;
+          dw = 0;
+        } else if (k == CH) {  // cell W - 1 opens the last, partial word
+          dw <<= 12;
+          if (act) DP[(static_cast<size_t>(i) * WQ + ((d0 + k) >> 2)) * 32] = dw;
+        }
+        rmax = __vmaxu2(rmax, h);
+      } else {
+        best2 = __vmaxu2(best2, h);
+      }
+      hleft = h;
+      hdiag = hup;
+    }
+    if constexpr (!TB) best2 = __vmaxu2(best2, h0);
+    hout = hleft;
+    fout = f;
+    if (act) {
+      if constexpr (TB) {  // a strictly better row of this lane's cells
+        if ((rmax & 0xFFFFu) > best_a) {
+          best_a = rmax & 0xFFFFu;
+          bi_a = i;
+#pragma unroll
+          for (int k = 0; k <= CH; ++k) row_a[k * kSwThreads] = H[k];
+        }
+        if ((rmax >> 16) > best_b) {
+          best_b = rmax >> 16;
+          bi_b = i;
+#pragma unroll
+          for (int k = 0; k <= CH; ++k) row_b[k * kSwThreads] = H[k];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < CH; ++k) T[k] = T[k + 1];
+      T[CH] = t_next;
+    }
+  }
+  // combine the lanes of the pair: larger value, then earlier row, then smaller column
+  uint64_t key_a, key_b;
+  const int ncell = c == LANES - 1 ? CH + 1 : CH;
+  if constexpr (TB) {
+    int bd_a = 0xFFF, bd_b = 0xFFF;
+#pragma unroll 1
+    for (int k = ncell - 1; k >= 0; --k) {
+      if (bi_a >= 0 && (row_a[k * kSwThreads] & 0xFFFFu) == best_a) bd_a = d0 + k;
+      if (bi_b >= 0 && (row_b[k * kSwThreads] >> 16) == best_b) bd_b = d0 + k;
+    }
+    key_a = static_cast<uint64_t>(best_a) << 40 | static_cast<uint64_t>(0xFFFFFu - static_cast<uint32_t>(bi_a + 1)) << 12 |
+            (0xFFFu - static_cast<uint32_t>(bd_a));
+    key_b = static_cast<uint64_t>(best_b) << 40 | static_cast<uint64_t>(0xFFFFFu - static_cast<uint32_t>(bi_b + 1)) << 12 |
+            (0xFFFu - static_cast<uint32_t>(bd_b));
+  } else {
+    key_a = static_cast<uint64_t>(best2 & 0xFFFFu) << 40;
+    key_b = static_cast<uint64_t>(best2 >> 16) << 40;
+  }
+#pragma unroll
+  for (int o = 1; o < LANES; o <<= 1) {
+    const uint64_t xa = __shfl_xor_sync(FULL, key_a, o), xb = __shfl_xor_sync(FULL, key_b, o);
+    key_a = xa > key_a ? xa : key_a;
+    key_b = xb > key_b ? xb : key_b;
+  }
+  if (c != 0 || skip) return;
+  const auto unpack = [](uint64_t key) {
+    const int best = static_cast<int>(key >> 40) - static_cast<int>(kBias);
+    const int bi = static_cast<int>(0xFFFFFu - static_cast<uint32_t>((key >> 12) & 0xFFFFFu)) - 1;
+    const int bd = static_cast<int>(0xFFFu - static_cast<uint32_t>(key & 0xFFFu));
+    return TB ? stash(best, bi, bd) : stash(best, 0, 0);
+  };
+  res[ta.slot] = unpack(key_a);
+  if (has_b) res[tb.slot] = unpack(key_b);
+}
+
 // The pairs k_sw_u2 listed, one alignment per thread, int32.
 template <int W, bool TB>
 __global__ void __launch_bounds__(kSwThreads) k_sw_fb(const SwTask* __restrict__ tasks, int base,
@@ -620,13 +821,48 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
   }
 }
 
+template <int LANES>
+void launch_wide(cudaStream_t st, bool tb, const SwTask* tasks, int base, int count, int n, const int* n_dev,
+                 const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res, uint32_t* dir,
+                 int rows_max, uint32_t* cig, const int64_t* cig_off, int* fb, uint32_t* err, const KernelTrace* kt) {
+  constexpr int W = 32 * LANES + 1;
+  const int pairs = (count + 1) / 2;
+  const int blocks_pairs = static_cast<int>((static_cast<int64_t>(pairs) * LANES + kSwThreads - 1) / kSwThreads);
+  const int blocks_tasks = (count + kSwThreads - 1) / kSwThreads;
+  const KernelTrace none;
+  const KernelTrace& t = kt ? *kt : none;
+  cudaMemsetAsync(fb, 0, sizeof(int), st);
+  if (tb) {
+    constexpr int kRowBytes = 2 * 33 * kSwThreads * 4;  // the two saved best rows of each lane
+    t.begin(st, "k_sw_wide<tb>");
+    k_sw_wide<LANES, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res,
+                                                                        dir, rows_max, fb);
+    t.end(st);
+    t.begin(st, "k_sw_fb<tb>");
+    k_sw_fb<W, true><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    t.end(st);
+    t.begin(st, "k_sw_walk");
+    k_sw_walk<W><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, count, n, n_dev, qbase, tbase, p, res, dir,
+                                                      rows_max, cig, cig_off, err);
+    t.end(st);
+  } else {
+    t.begin(st, "k_sw_wide<score>");
+    k_sw_wide<LANES, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
+                                                                 rows_max, fb);
+    t.end(st);
+    t.begin(st, "k_sw_fb<score>");
+    k_sw_fb<W, false><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    t.end(st);
+  }
+}
+
 }  // namespace
 
 bool sw_bytes_ok(const dnaln_score_params& s) {
   return s.match <= 127 && s.mismatch <= 128 && s.ambig <= 128 && s.match >= -128;
 }
 
-bool sw_band_in_registers(int W) { return W == 11 || W == 17 || W == 33 || W == 43 || W == 65; }
+bool sw_band_in_registers(int W) { return W == 11 || W == 17 || W == 33 || W == 43 || W == 65 || W == 129; }
 
 bool sw_uses_generic(int W, bool bytes_ok) { return !(bytes_ok && sw_band_in_registers(W)); }
 
@@ -673,6 +909,10 @@ bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int
       DNB_SW_U2(33)
       DNB_SW_U2(43)
       DNB_SW_U2(65)
+      case 129:
+        launch_wide<4>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, fb,
+                       err, kt);
+        return true;
       default: break;
     }
 #undef DNB_SW_U2

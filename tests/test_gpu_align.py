@@ -71,6 +71,22 @@ def test_other_band_widths(ctx, port, bw):
         check_same(ctx.align(qs, ts, tb, D.ScoreParams(*sc)), port.align(qs, ts, tb, sc), tb)
 
 
+@pytest.mark.parametrize("scheme", SCHEMES)
+def test_wide_band_lanes(ctx, port, scheme):
+    # bw 64 (W = 129) runs four lanes per pair of alignments; odd task counts, mixed lengths
+    # up to 1000 and N bases (the int32 list) included
+    sc = scheme[:5] + (64,)
+    rng = np.random.default_rng(sum(scheme))
+    qs, ts = random_tasks(rng, 1001, 64, max_len=1000)
+    for q in qs[::37]:
+        q[rng.integers(len(q))] = 4 if len(q) else 0
+    for t in ts[::53]:
+        if len(t):
+            t[rng.integers(len(t))] = 4
+    for tb in (False, True):
+        check_same(ctx.align(qs, ts, tb, D.ScoreParams(*sc)), port.align(qs, ts, tb, sc), tb)
+
+
 def test_large_scores_outside_byte_profile(ctx, port):
     # scores that do not fit the signed-byte substitution profile use the generic path
     sc = (200, 300, 5, 2, 150, 16)
