@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD,
                     help="synthetic workload (dnaln_b200.synth.WORKLOADS); the default is the headline one")
     ap.add_argument("--bw", type=int, default=16, help="SW band half-width (16, or 64 for the mixed-length workload)")
+    ap.add_argument("--serve-requests", type=int, default=1500, help="requests per rate point (--workload serve)")
+    ap.add_argument("--serve-lanes", type=int, default=3)
+    ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.5, 0.8],
+                    help="offered loads as fractions of the measured capacity (--workload serve)")
     return ap.parse_args()
 
 
@@ -199,6 +203,9 @@ def run_reference(args) -> None:
     import oracle
     import dnaln_b200 as D
     from dnaln_b200 import synth
+    if args.workload == SERVE:
+        run_reference_serve(args)
+        return
     g, reads, _ = synth.workload(args.workload, seed=args.seed, n_reads=args.n_reads)
     p = D.default_map_params(bw=args.bw)
     threads = len(os.sched_getaffinity(0))
@@ -231,6 +238,42 @@ def run_reference(args) -> None:
                              "sample": f"{len(sample):,} reads per step, Mapper::map, {cores} threads",
                              "cpu": _cpu_model()},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_serve(args) -> None:
+    """The reference's CPU mapper on the serving workload's requests, back to back, all
+    host threads: requests are mapped in arrival order, each split over the threads."""
+    import oracle
+    import dnaln_b200 as D
+    pools = ServePools(args.seed)
+    p = D.default_map_params(bw=args.bw)
+    threads = len(os.sched_getaffinity(0))
+    if not oracle.REF_SO.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference build (oracle/_ref) is missing"}))
+        return
+    ref = oracle.Reference()
+    rgs = [ref.genome(g) for g in pools.genomes]
+    reqs = pools.stream(args.serve_requests, args.seed + 100)
+    sample, tot = [], 0
+    for r in reqs:  # a bounded sample of the stream: ~20 s of CPU work
+        sample.append(r)
+        tot += r[2]
+        if tot >= 400_000:
+            break
+    dt = 0.0
+    for gi, a, m in sample:
+        dt += ref.time_map(rgs[gi], pools.pools[gi].slice(a, a + m), p, threads)
+    value = tot / dt
+    line = {"metric": "reads/s (served)", "value": value, "unit": "reads/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": 1e3 * dt, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic (seeded generator)",
+            "config": {"workload": "serve (reference CPU mapper, requests back to back)", "requests": len(sample),
+                       "reads": tot}, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": "reference",
+                             "sample": f"first {len(sample)} requests of the stream ({tot:,} reads), Mapper::map, "
+                                       f"{threads} threads", "cpu": _cpu_model()},
+            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -442,9 +485,174 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+# ---- serving: a Poisson request stream over two resident indexes ------------------------
+SERVE = "serve"
+SERVE_POOL = 400_000       # reads generated per genome; a request is a contiguous slice of a pool
+SERVE_MAX_REQ = 50_000     # request sizes log-uniform in [1, 50,000] reads
+SERVE_CIGAR_PER_READ = 16  # CIGAR capacity per read of a request's output (DNALN_ERR_CAPACITY if short)
+
+
+class ServePools:
+    """The two genomes of the serving workload (4.6 Mbp and 120 Mbp), a pool of reads of
+    length uniform in [100, 300] on each, and a seeded request stream over them."""
+
+    def __init__(self, seed: int, pool: int = SERVE_POOL):
+        from dnaln_b200 import synth
+        self.genomes = [synth.make_genome(synth.GENOME_4M6, seed), synth.make_genome(synth.GENOME_120M, seed + 1)]
+        spec = synth.ReadsSpec(n_reads=pool, len_min=100, len_max=300, len_dist=2)
+        self.pools = [synth.make_reads(g, spec, seed + 10 + i)[0] for i, g in enumerate(self.genomes)]
+        self.arrays = [(rb.seq, np.ascontiguousarray(rb.seq_off[:-1]), np.ascontiguousarray(rb.seq_len),
+                        rb.name_hash()) for rb in self.pools]
+
+    def stream(self, n_req: int, seed: int):
+        """(genome, first read, size) per request: genome 50/50, size log-uniform."""
+        rng = np.random.default_rng(seed)
+        g = rng.integers(0, 2, n_req)
+        size = np.minimum(SERVE_MAX_REQ, np.floor(np.exp(rng.uniform(0, np.log(SERVE_MAX_REQ + 1), n_req)))).astype(
+            np.int64)
+        size = np.maximum(size, 1)
+        start = np.array([rng.integers(0, len(self.pools[gi]) - sz + 1) for gi, sz in zip(g, size)], np.int64)
+        return list(zip(g.tolist(), start.tolist(), size.tolist()))
+
+
+def replay(srv, pools: ServePools, iids, reqs, rate: float | None, p) -> dict:
+    """Submits reqs at Poisson arrival times of `rate` requests/s (None: all at once) from
+    one producer thread, waits for all; latencies are the server's (submit to completion)."""
+    from dnaln_b200 import _native as N
+    L = N.lib()
+    n_tot = sum(r[2] for r in reqs)
+    rec = np.zeros(n_tot, dtype=__import__("dnaln_b200").MAP_RECORD_DTYPE)
+    cig = np.zeros(n_tot * SERVE_CIGAR_PER_READ, np.uint32)
+    used = [C.c_int64() for _ in reqs]
+    ids = [C.c_int64() for _ in reqs]
+    rng = np.random.default_rng(12345)
+    arrivals = np.zeros(len(reqs)) if rate is None else np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+    base = np.concatenate([[0], np.cumsum([r[2] for r in reqs])])
+    errors = []
+
+    def produce():
+        t0 = time.perf_counter()
+        for i, (gi, a, m) in enumerate(reqs):
+            while True:
+                dt = arrivals[i] - (time.perf_counter() - t0)
+                if dt <= 0:
+                    break
+                if dt > 0.002:
+                    time.sleep(dt - 0.001)
+            seq, off, ln, nh = pools.arrays[gi]
+            rc = L.dnaln_serve_submit(srv._h, iids[gi], seq.ctypes.data, off.ctypes.data + 8 * a,
+                                      ln.ctypes.data + 4 * a, nh.ctypes.data + 4 * a, m, C.byref(p),
+                                      rec.ctypes.data + 40 * int(base[i]),
+                                      cig.ctypes.data + 4 * SERVE_CIGAR_PER_READ * int(base[i]),
+                                      SERVE_CIGAR_PER_READ * m, C.byref(used[i]), C.byref(ids[i]))
+            if rc:
+                errors.append(L.dnaln_serve_last_error(srv._h).decode())
+                ids[i].value = 0
+
+    srv.reset_stats()
+    w0 = time.perf_counter()
+    th = threading.Thread(target=produce)
+    th.start()
+    lat = []
+    for i in range(len(reqs)):
+        while ids[i].value == 0 and th.is_alive():
+            time.sleep(0.0002)
+        if ids[i].value == 0:
+            continue
+        x = C.c_double()
+        rc = L.dnaln_serve_wait(srv._h, ids[i].value, C.byref(x))
+        if rc:
+            errors.append(L.dnaln_serve_last_error(srv._h).decode())
+        lat.append(x.value)
+    th.join()
+    wall = time.perf_counter() - w0
+    if errors:
+        raise RuntimeError(f"serving failed: {errors[0]}")
+    st = srv.stats()
+    lat = np.array(lat)
+    return {"offered_req_per_s": rate, "requests": len(reqs), "reads": n_tot, "wall_s": wall,
+            "reads_per_s": n_tot / wall, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max()), "batches": st["batches"],
+            "mean_batch_reads": st["mean_batch_reads"], "max_queue_depth": st["max_queue_depth"],
+            "lane_ms": {k[3:]: st[k] for k in ("ms_form", "ms_gather", "ms_device", "ms_scatter", "ms_complete")}}
+
+
+def run_serve(args) -> None:
+    """The serving workload: both indexes resident, Poisson arrivals at a swept rate,
+    requests of log-uniform 1..50,000 reads (length uniform in [100, 300]) to either genome.
+    The continuously batching server (3 lanes, requests coalesced) is measured against
+    serving the same stream with the plain per-batch kernels (one lane, one request per batch)."""
+    import torch
+    import dnaln_b200 as D
+    from dnaln_b200.serve import Server
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    pools = ServePools(args.seed)
+    ctx = D.Context(local)
+    t_ix = time.perf_counter()
+    iids = [ctx.index_build(g) for g in pools.genomes]
+    build_s = time.perf_counter() - t_ix
+    p = D.default_map_params(bw=args.bw)
+    n_req = args.serve_requests
+    warm = pools.stream(64, args.seed + 99)
+    reqs = pools.stream(n_req, args.seed + 100)
+    mean_reads = float(np.mean([r[2] for r in reqs]))
+    clocks = ClockSampler(local)
+    clocks.start()
+    modes = {"batched": dict(lanes=args.serve_lanes, coalesce=True),
+             "plain": dict(lanes=1, coalesce=False, max_batch_reads=BATCH)}
+    points = {}
+    for name, kw in modes.items():
+        with Server(ctx, **kw) as srv:
+            replay(srv, pools, iids, warm, None, p)        # warm-up: the lanes' staging and scratch
+            replay(srv, pools, iids, reqs, None, p)        # grow to the stream's batch sizes
+            sat = replay(srv, pools, iids, reqs, None, p)  # all requests at once: capacity
+            cap_req = sat["requests"] / sat["wall_s"]
+            pts = [dict(sat, load="saturation")]
+            for frac in args.serve_loads:
+                r = replay(srv, pools, iids, reqs, frac * cap_req, p)
+                r["load"] = frac
+                pts.append(r)
+            points[name] = pts
+    clk = clocks.result()
+    # offered loads of the plain server, replayed on the batched one: same absolute rates
+    with Server(ctx, **modes["batched"]) as srv:
+        replay(srv, pools, iids, reqs, None, p)
+        plain_cap = points["plain"][0]["requests"] / points["plain"][0]["wall_s"]
+        same = [dict(replay(srv, pools, iids, reqs, f * plain_cap, p), load=f"{f} x plain capacity")
+                for f in args.serve_loads]
+    points["batched_at_plain_rates"] = same
+    head = points["batched"][0]
+    out = {"metric": "reads/s (served)", "value": head["reads_per_s"], "unit": "reads/s", "n_gpus": 1,
+           "steps": len(args.serve_loads) + 1, "warmup": 1, "ms_per_step": 1e3 * head["wall_s"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+           "data": "synthetic (seeded generator, no dataset)",
+           "config": {"workload": "serve: 4.6 Mbp + 120 Mbp indexes resident, Poisson arrivals, requests of "
+                                  "log-uniform 1-50,000 reads of length U[100, 300] to either genome 50/50, "
+                                  f"k=15 w=10 bw={args.bw}",
+                      "requests_per_point": n_req, "mean_reads_per_request": mean_reads,
+                      "l2": "no flush: each point streams its requests' reads (GBs) through the lanes",
+                      "parallelism": "1 GPU, request server lanes"},
+           "e2e": {"value": head["reads_per_s"], "unit": "reads/s",
+                   "h2d_bytes_per_step": int(head["reads"] * (200 + 16)), "d2h_bytes_per_step": int(head["reads"] * 40),
+                   "note": "host buffers in, records and CIGARs out: the served path is end to end"},
+           "latency": {k: [{kk: v[kk] for kk in ("load", "offered_req_per_s", "reads_per_s", "p50_ms", "p99_ms",
+                                                 "mean_ms", "max_ms", "batches", "mean_batch_reads",
+                                                 "max_queue_depth", "lane_ms")} for v in pts]
+                       for k, pts in points.items()},
+           "batched_vs_plain_capacity": head["reads_per_s"] / points["plain"][0]["reads_per_s"],
+           "index_build_s": build_s, "clocks": clk}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == SERVE and args.impl != "reference":
+        run_serve(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

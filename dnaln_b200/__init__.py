@@ -10,6 +10,8 @@ follow dnaln's C++ API):
 * :meth:`Context.align`       — ``Aligner::align`` (src/align.hpp:62-68)
 * :meth:`Context.map_batch`   — ``Mapper::map`` (src/mapper.cpp:75-223)
 * :func:`sam_format`          — ``Mapper::append_sam`` (src/mapper.cpp:231-270)
+* :class:`dnaln_b200.serve.Server` — request server with continuous batching (no
+  reference counterpart)
 
 Every call goes to the CUDA library; there is no CPU fallback. Errors raise
 :class:`DnalnError` carrying the C status code and message.
@@ -268,6 +270,12 @@ class Context:
 
     def index_free(self, iid: int) -> None:
         self._check(self._lib.dnaln_gpu_index_free(self._h, iid))
+
+    def index_attach(self, src: "Context", iid: int) -> int:
+        """Shares index `iid` of context `src` (same device) with this context, no copy."""
+        out = C.c_int32()
+        self._check(self._lib.dnaln_gpu_index_attach(self._h, src.handle, iid, C.byref(out)))
+        return out.value
 
     # -- stages -------------------------------------------------------------------------
     def sketch(self, seqs: list[np.ndarray], k: int, w: int, pos_offset: list[int] | None = None):

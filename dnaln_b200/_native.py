@@ -57,6 +57,19 @@ class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 48), ("launches", C.c_int64), ("ms", C.c_double)]
 
 
+class ServeParams(C.Structure):
+    _fields_ = [("lanes", C.c_int32), ("coalesce", C.c_int32), ("max_batch_reads", C.c_int64),
+                ("hbm_budget_bytes", C.c_int64)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("requests", "reads", "bases", "batches")] + \
+               [(n, C.c_double) for n in ("p50_ms", "p99_ms", "max_ms", "mean_ms", "mean_batch_reads")] + \
+               [("max_queue_depth", C.c_int64), ("budget_bytes", C.c_int64), ("lane_budget_bytes", C.c_int64),
+                ("lanes", C.c_int32), ("pad_", C.c_int32)] + \
+               [(n, C.c_double) for n in ("ms_form", "ms_gather", "ms_device", "ms_scatter", "ms_complete")]
+
+
 class SynthGenomeSpec(C.Structure):
     _fields_ = [("n_contigs", C.c_int32), ("contig_len", C.c_uint32), ("gc", C.c_double),
                 ("n_repeat_units", C.c_int32), ("repeat_unit_len", C.c_int32), ("repeat_frac", C.c_double),
@@ -105,6 +118,16 @@ SIGNATURES = {
     "dnaln_gpu_index_stats": (C.c_int, [P, i32, P]),
     "dnaln_gpu_index_export": (C.c_int, [P, i32, P, P, P, P]),
     "dnaln_gpu_index_free": (C.c_int, [P, i32]),
+    "dnaln_gpu_index_attach": (C.c_int, [P, P, i32, C.POINTER(i32)]),
+    "dnaln_gpu_ctx_device": (C.c_int, [P, C.POINTER(i32)]),
+    "dnaln_serve_create": (C.c_int, [P, C.POINTER(ServeParams), C.POINTER(P)]),
+    "dnaln_serve_submit": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64, C.POINTER(i64),
+                                     C.POINTER(i64)]),
+    "dnaln_serve_wait": (C.c_int, [P, i64, C.POINTER(dbl)]),
+    "dnaln_serve_get_stats": (C.c_int, [P, C.POINTER(ServeStats)]),
+    "dnaln_serve_reset_stats": (C.c_int, [P]),
+    "dnaln_serve_last_error": (C.c_char_p, [P]),
+    "dnaln_serve_destroy": (C.c_int, [P]),
     "dnaln_gpu_sketch": (C.c_int, [P, P, P, P, P, i64, i32, i32, P, P, P, P]),
     "dnaln_gpu_lookup": (C.c_int, [P, i32, P, i64, P, P]),
     "dnaln_gpu_chain": (C.c_int, [P, P, P, P, P, i64, i32, C.POINTER(ChainParams), P, P, P, P, P, P, P]),

@@ -20,7 +20,8 @@ ROOT = PKG.parent
 BUILD = PKG / "_build"
 LIB = PKG / "libdnaln_b200.so"
 
-CUDA_SOURCES = ["csrc/sw.cu", "csrc/seed.cu", "csrc/seed_thread.cu", "csrc/map.cu", "csrc/capi.cu", "csrc/noalloc.cu"]
+CUDA_SOURCES = ["csrc/sw.cu", "csrc/seed.cu", "csrc/seed_thread.cu", "csrc/map.cu", "csrc/capi.cu", "csrc/noalloc.cu",
+                "csrc/serve.cu"]
 HOST_SOURCES = ["host/index_host.cpp", "host/sam.cpp", "host/synth.cpp"]
 HEADERS = ["csrc/common.cuh", "csrc/sw.cuh", "csrc/seed.cuh", "csrc/map.cuh", "host/index_host.hpp"]
 PUBLIC_HEADERS = ["dnaln_b200.h", "dnaln_synth.h"]

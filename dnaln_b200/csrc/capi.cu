@@ -26,6 +26,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -47,8 +48,23 @@ struct DevBuf {
   size_t cap = 0;
 };
 
-struct IndexRes {
+// Device memory of one resident index. Contexts that share the index (index_attach) hold
+// it through a shared pointer; the last holder to release it frees the memory.
+struct IndexMem {
   DevBuf table, positions, genome, coff, clen, nruns;
+  IndexMem() = default;
+  IndexMem(const IndexMem&) = delete;
+  IndexMem& operator=(const IndexMem&) = delete;
+  ~IndexMem() {
+    for (DevBuf* b : {&table, &positions, &genome, &coff, &clen, &nruns})
+      if (b->p) cudaFree(b->p);
+  }
+  size_t bytes() const { return table.cap + positions.cap + genome.cap + coff.cap + clen.cap + nruns.cap; }
+};
+
+struct IndexRes {
+  std::shared_ptr<IndexMem> mem;
+  int device = 0;
   uint64_t n_keys = 0, n_pos = 0, n_buckets = 0, n_bases = 0;
   uint32_t max_count = 0;
   int32_t n_contigs = 0, k = 0, w = 0;
@@ -663,10 +679,8 @@ int dalloc(dnaln_ctx* c, DevBuf& b, size_t bytes) {
   return DNALN_OK;
 }
 
-void free_index(IndexRes& r) {
-  for (DevBuf* b : {&r.table, &r.positions, &r.genome, &r.coff, &r.clen, &r.nruns})
-    if (b->p) cudaFree(b->p);
-}
+// Drops this holder's reference; the memory goes with the last one.
+void free_index(IndexRes& r) { r.mem.reset(); }
 
 
 // ---- the worker behind dnaln_gpu_map_submit ----------------------------------------------
@@ -929,6 +943,12 @@ int dnaln_gpu_ctx_destroy(dnaln_ctx* c) {
 
 const char* dnaln_gpu_last_error(const dnaln_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
+int dnaln_gpu_ctx_device(const dnaln_ctx* c, int32_t* device) {
+  if (!c || !device) return DNALN_ERR_INVALID_ARG;
+  *device = c->device;
+  return DNALN_OK;
+}
+
 int dnaln_gpu_set_stream(dnaln_ctx* c, void* stream) {
   if (!c) return DNALN_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> ctx_lock(c->mu);
@@ -1043,6 +1063,9 @@ int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases,
   HostIndex h;
   build_index_host(genome, contig_off, contig_len, n_contigs, k, w, h);
   IndexRes r;
+  r.mem = std::make_shared<IndexMem>();
+  r.device = c->device;
+  IndexMem& m = *r.mem;
   r.n_keys = h.n_keys;
   r.n_pos = h.pos.size();
   r.n_buckets = h.keys.size();
@@ -1067,9 +1090,9 @@ int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases,
     i = j;
   }
   int e = DNALN_OK;
-  if ((e = dalloc(c, r.nruns, runs.size() * sizeof(uint2))) || (e = dalloc(c, r.table, table.size() * sizeof(ulonglong2))) ||
-      (e = dalloc(c, r.positions, h.pos.size() * sizeof(uint32_t))) || (e = dalloc(c, r.genome, n_bases)) ||
-      (e = dalloc(c, r.coff, n_contigs * sizeof(uint64_t))) || (e = dalloc(c, r.clen, n_contigs * sizeof(uint32_t)))) {
+  if ((e = dalloc(c, m.nruns, runs.size() * sizeof(uint2))) || (e = dalloc(c, m.table, table.size() * sizeof(ulonglong2))) ||
+      (e = dalloc(c, m.positions, h.pos.size() * sizeof(uint32_t))) || (e = dalloc(c, m.genome, n_bases)) ||
+      (e = dalloc(c, m.coff, n_contigs * sizeof(uint64_t))) || (e = dalloc(c, m.clen, n_contigs * sizeof(uint32_t)))) {
     free_index(r);
     return e;
   }
@@ -1077,22 +1100,22 @@ int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases,
   auto up = [&](DevBuf& b, const void* src, size_t bytes) {
     if (x == cudaSuccess && bytes) x = cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
   };
-  up(r.table, table.data(), table.size() * sizeof(ulonglong2));
-  up(r.positions, h.pos.data(), h.pos.size() * sizeof(uint32_t));
-  up(r.genome, genome, n_bases);
-  up(r.coff, contig_off, n_contigs * sizeof(uint64_t));
-  up(r.clen, contig_len, n_contigs * sizeof(uint32_t));
-  up(r.nruns, runs.data(), runs.size() * sizeof(uint2));
+  up(m.table, table.data(), table.size() * sizeof(ulonglong2));
+  up(m.positions, h.pos.data(), h.pos.size() * sizeof(uint32_t));
+  up(m.genome, genome, n_bases);
+  up(m.coff, contig_off, n_contigs * sizeof(uint64_t));
+  up(m.clen, contig_len, n_contigs * sizeof(uint32_t));
+  up(m.nruns, runs.data(), runs.size() * sizeof(uint2));
   if (x != cudaSuccess) {
     free_index(r);
     return fail(c, DNALN_ERR_CUDA, "index upload: %s", cudaGetErrorString(x));
   }
-  r.dev.table = static_cast<const ulonglong2*>(r.table.p);
-  r.dev.positions = static_cast<const uint32_t*>(r.positions.p);
-  r.dev.genome = static_cast<const uint8_t*>(r.genome.p);
-  r.dev.contig_off = static_cast<const uint64_t*>(r.coff.p);
-  r.dev.contig_len = static_cast<const uint32_t*>(r.clen.p);
-  r.dev.n_runs = static_cast<const uint2*>(r.nruns.p);
+  r.dev.table = static_cast<const ulonglong2*>(m.table.p);
+  r.dev.positions = static_cast<const uint32_t*>(m.positions.p);
+  r.dev.genome = static_cast<const uint8_t*>(m.genome.p);
+  r.dev.contig_off = static_cast<const uint64_t*>(m.coff.p);
+  r.dev.contig_len = static_cast<const uint32_t*>(m.clen.p);
+  r.dev.n_runs = static_cast<const uint2*>(m.nruns.p);
   r.dev.n_n_runs = static_cast<int32_t>(runs.size());
   r.dev.mask = h.mask;
   r.dev.n_contigs = n_contigs;
@@ -1116,7 +1139,7 @@ int dnaln_gpu_index_stats(const dnaln_ctx* cc, int32_t id, uint64_t out6[6]) {
   out6[2] = r->max_count;
   out6[3] = r->n_buckets * 16 + r->n_pos * 4;  // src/index.hpp:46
   out6[4] = r->n_buckets;
-  out6[5] = r->table.cap + r->positions.cap + r->genome.cap + r->coff.cap + r->clen.cap + r->nruns.cap;
+  out6[5] = r->mem->bytes();
   return DNALN_OK;
 }
 
@@ -1129,14 +1152,14 @@ int dnaln_gpu_index_export(dnaln_ctx* c, int32_t id, uint64_t* keys, uint32_t* o
   IndexRes* r = find_index(c, id);
   if (!r) return DNALN_ERR_NOT_FOUND;
   std::vector<ulonglong2> t(r->n_buckets);
-  CK(cudaMemcpy(t.data(), r->table.p, t.size() * sizeof(ulonglong2), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(t.data(), r->mem->table.p, t.size() * sizeof(ulonglong2), cudaMemcpyDeviceToHost));
   for (size_t i = 0; i < t.size(); ++i) {
     if (keys) keys[i] = t[i].x;
     if (offsets) offsets[i] = static_cast<uint32_t>(t[i].y);
     if (counts) counts[i] = static_cast<uint32_t>(t[i].y >> 32);
   }
   if (positions && r->n_pos)
-    CK(cudaMemcpy(positions, r->positions.p, r->n_pos * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(positions, r->mem->positions.p, r->n_pos * sizeof(uint32_t), cudaMemcpyDeviceToHost));
   return DNALN_OK;
 }
 
@@ -1150,6 +1173,24 @@ int dnaln_gpu_index_free(dnaln_ctx* c, int32_t id) {
   cudaStreamSynchronize(c->st);
   free_index(*r);
   c->idx.erase(id);
+  return DNALN_OK;
+}
+
+int dnaln_gpu_index_attach(dnaln_ctx* dst, dnaln_ctx* src, int32_t src_id, int32_t* dst_id) {
+  if (!dst || !src || !dst_id) return dst ? fail(dst, DNALN_ERR_INVALID_ARG, "null argument") : DNALN_ERR_INVALID_ARG;
+  if (dst == src) return fail(dst, DNALN_ERR_INVALID_ARG, "a context cannot attach its own index");
+  // both locks, in address order, so that two attaches in opposite directions cannot deadlock
+  std::unique_lock<std::mutex> l1(dst < src ? dst->mu : src->mu, std::defer_lock);
+  std::unique_lock<std::mutex> l2(dst < src ? src->mu : dst->mu, std::defer_lock);
+  std::lock(l1, l2);
+  if (src->device != dst->device)
+    return fail(dst, DNALN_ERR_INVALID_ARG, "index %d lives on device %d, this context on device %d", src_id,
+                src->device, dst->device);
+  auto it = src->idx.find(src_id);
+  if (it == src->idx.end()) return fail(dst, DNALN_ERR_NOT_FOUND, "unknown index id %d", src_id);
+  const int32_t id = dst->next_id++;
+  dst->idx[id] = it->second;  // shares the device memory (shared pointer), copies the descriptors
+  *dst_id = id;
   return DNALN_OK;
 }
 

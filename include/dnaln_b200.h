@@ -97,6 +97,8 @@ const char* dnaln_gpu_version(void);
 int dnaln_gpu_ctx_create(int device, dnaln_ctx** out);
 int dnaln_gpu_ctx_destroy(dnaln_ctx* ctx);
 const char* dnaln_gpu_last_error(const dnaln_ctx* ctx);
+/* The CUDA device the context runs on. */
+int dnaln_gpu_ctx_device(const dnaln_ctx* ctx, int32_t* device);
 /* Launch on `stream` (a cudaStream_t) instead of the context's own stream; NULL restores it. */
 int dnaln_gpu_set_stream(dnaln_ctx* ctx, void* stream);
 int dnaln_gpu_get_stats(const dnaln_ctx* ctx, dnaln_stats* out);
@@ -143,6 +145,12 @@ int dnaln_gpu_index_stats(const dnaln_ctx* ctx, int32_t index_id, uint64_t out6[
 int dnaln_gpu_index_export(dnaln_ctx* ctx, int32_t index_id, uint64_t* keys, uint32_t* offsets, uint32_t* counts,
                            uint32_t* positions);
 int dnaln_gpu_index_free(dnaln_ctx* ctx, int32_t index_id);
+/* Makes index src_id of context src (same device) usable by context dst under the new id
+ * *dst_id, without copying it: several contexts (one per host thread, or the lanes of a
+ * server below) map against one resident copy. The memory is freed when the last context
+ * holding the index frees it or is destroyed. No reference counterpart: the reference
+ * builds one MinimizerIndex per process (src/main.cpp:33-35). */
+int dnaln_gpu_index_attach(dnaln_ctx* dst, dnaln_ctx* src, int32_t src_id, int32_t* dst_id);
 
 /* ---- per-stage entry points (batched forms of the reference's per-read calls) ------- */
 
@@ -225,6 +233,55 @@ int dnaln_gpu_map_batch_device(dnaln_ctx* ctx, int32_t index_id, const char* d_s
                                const int32_t* d_seq_len, const uint32_t* d_name_hash, int64_t n,
                                const dnaln_map_params* p, dnaln_map_record* d_out, uint32_t* d_cigar,
                                int64_t cigar_cap, int64_t* cigar_used);
+
+/* ---- serving: continuous batching over resident indexes -------------------------------
+ * No reference counterpart: the reference maps one FASTQ per process against one index
+ * (src/main.cpp:33-61). A server keeps the indexes of its home context resident and maps
+ * requests (read sets of any size, each against one index) submitted from any number of
+ * producer threads. Each of its worker lanes is a context of its own (stream, scratch)
+ * sharing the home context's indexes (dnaln_gpu_index_attach). A lane that frees up takes
+ * the oldest waiting request and, with coalesce = 1, fills its next batch with the reads
+ * of the waiting requests for the same index and parameters in arrival order, splitting
+ * large requests across batches; requests that arrive while others are on the GPU join
+ * the next batch, and the lanes' batches overlap on the device. A batch takes reads while
+ * its estimated device footprint fits the lane's share of the HBM budget. Every request's
+ * records and CIGARs are those dnaln_gpu_map_batch gives for it alone (mapping is per
+ * read, so batch composition cannot change a result). */
+typedef struct dnaln_server dnaln_server;
+typedef struct {
+  int32_t lanes;             /* concurrent batches on the device (0 = 3) */
+  int32_t coalesce;          /* 1 = requests share batches; 0 = each batch holds one request's reads */
+  int64_t max_batch_reads;   /* reads per batch (0 = 262,144) */
+  int64_t hbm_budget_bytes;  /* device memory for the batches in flight, all lanes together
+                                (0 = free device memory at creation minus 2 GiB) */
+} dnaln_serve_params;
+typedef struct {
+  uint64_t requests, reads, bases, batches;  /* completed since creation or the last reset */
+  double p50_ms, p99_ms, max_ms, mean_ms;    /* request latency, submit to completion */
+  double mean_batch_reads;
+  int64_t max_queue_depth;                   /* requests waiting for a lane, at most */
+  int64_t budget_bytes, lane_budget_bytes;
+  int32_t lanes, pad_;
+  /* lane time, summed over lanes: forming batches, gathering reads into the staging
+   * buffers, on the device (copies in, mapping, copies out), scattering results, and
+   * completing requests (CIGAR layout) */
+  double ms_form, ms_gather, ms_device, ms_scatter, ms_complete;
+} dnaln_serve_stats;
+int dnaln_serve_create(dnaln_ctx* home, const dnaln_serve_params* sp, dnaln_server** out);
+/* Same arguments as dnaln_gpu_map_submit; index_id is an index of the home context. The
+ * buffers must stay valid until dnaln_serve_wait returns for *request. */
+int dnaln_serve_submit(dnaln_server* s, int32_t index_id, const char* seq, const int64_t* seq_off,
+                       const int32_t* seq_len, const uint32_t* name_hash, int64_t n, const dnaln_map_params* p,
+                       dnaln_map_record* out, uint32_t* cigar, int64_t cigar_cap, int64_t* cigar_used,
+                       int64_t* request);
+/* Blocks until the request is complete; returns its status, *latency_ms (may be NULL) =
+ * submit-to-completion time. Each request is waited for once. */
+int dnaln_serve_wait(dnaln_server* s, int64_t request, double* latency_ms);
+int dnaln_serve_get_stats(dnaln_server* s, dnaln_serve_stats* out);
+int dnaln_serve_reset_stats(dnaln_server* s);
+const char* dnaln_serve_last_error(const dnaln_server* s);
+/* Finishes every submitted request, then releases the lanes. */
+int dnaln_serve_destroy(dnaln_server* s);
 
 /* FNV-1a of a read name (src/common.hpp:136-140), and of n names concatenated in
  * names[name_off[i] .. name_off[i+1]) into out[i]. */
