@@ -370,6 +370,23 @@ def run_ours(args) -> None:
     ctx.set_kernel_trace(False)
     value = world * n_reads * args.steps / (ms / 1e3)
 
+    # ---- the plain per-batch form of the same step: every read through the warp-per-read
+    # seeding and chaining kernels (no length buckets), SW tasks in read order ----------
+    ctx.set_option("warp_seed_only", 1)
+    ctx.set_option("length_order", 0)
+    step_device()
+    barrier()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for _ in range(args.steps):
+        step_device()
+    g1.record(stream)
+    barrier()
+    ms_plain = max_over_ranks(g0.elapsed_time(g1))
+    ctx.set_option("warp_seed_only", 0)
+    ctx.set_option("length_order", 1)
+    plain_value = world * n_reads * args.steps / (ms_plain / 1e3)
+
     # ---- end to end through the host-buffer C call (e2e) ----------------------------
     host = []
     for part in parts:
@@ -462,6 +479,9 @@ def run_ours(args) -> None:
            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                    "ms_per_step": ms_e2e / e2e_steps, "wall_s": wall_e2e},
            "gpu_launches": int(st["launches"]),
+           "plain": {"value": plain_value, "ms_per_step": ms_plain / args.steps,
+                     "what": "same step, every read through the warp-per-read kernels, SW tasks in read order"},
+           "batched_vs_plain": value / plain_value,
            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak if achieved is not None else None, "traffic": traffic,
                         "peak_kind": peak_kind,

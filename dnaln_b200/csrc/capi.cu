@@ -139,6 +139,7 @@ struct dnaln_ctx {
   std::thread worker;
   bool stop = false;
   bool warp_seed_only = false;  // option: every read through the warp-per-read seeding kernels
+  bool length_order = true;     // option: SW tasks of mixed-length batches run longest first
   // kernel trace: event pairs of the current batch, totals per kernel name
   bool trace_on = false, trace_open = false;
   std::string trace_only;  // non-empty: trace only the kernel of this name
@@ -570,7 +571,8 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   launch_score_tasks(st, n, pofs, d_seq_len, cb, ix.dev, mc, sc_tasks, c->d_count, ctr);
   kt.end(st);
   // reads of very different lengths: SW tasks longest first (lengths known on the host)
-  const bool by_length = static_cast<double>(max_len) > 1.25 * static_cast<double>(B) / static_cast<double>(n);
+  const bool by_length =
+      c->length_order && static_cast<double>(max_len) > 1.25 * static_cast<double>(B) / static_cast<double>(n);
   const SwTask* sc_run = sc_tasks;
   if (by_length)
     if (int e = sort_tasks_by_length(c, sc_tasks, static_cast<int>(n * MC), c->d_count, "sc", &sc_run)) return e;
@@ -1024,6 +1026,10 @@ int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
   std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (k == "warp_seed_only") {
     c->warp_seed_only = value != 0;
+    return DNALN_OK;
+  }
+  if (k == "length_order") {
+    c->length_order = value != 0;
     return DNALN_OK;
   }
   if (k == "dir_cap_bytes") {

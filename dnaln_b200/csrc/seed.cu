@@ -40,7 +40,7 @@ namespace {
 constexpr int kSeedWarps = 8;
 constexpr int kRing = 512;  // >= 32 + max w (255)
 constexpr int kChainWarps = 4;
-constexpr int kSmCap = 128;  // anchors per read held in shared memory
+constexpr int kSmCap = 256;  // anchors per read held in shared memory
 
 struct SketchSmem {
   uint64_t hash[kRing];
@@ -259,19 +259,16 @@ struct ChainArrays {
   uint8_t* used;
 };
 
-// Sorts the n anchor keys, runs the DP, extracts chains into as.ch_*[c0 + j] and leaves
-// their final order in ord[0, m) (low 32 bits = j). Returns m in every lane.
-__device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const AnchorScratch& as, int64_t c0) {
+// The chaining DP for any lookback, in rounds of 32 predecessors (src/chain.cpp:22-45).
+// Per round one redux over score * 32 + (31 - lane): the largest score, ties to the
+// smallest lane = the nearest j; earlier (nearer) rounds win ties across rounds through
+// the strict '>' below — the reference's scan order.
+__device__ void chain_dp_rounds(const ChainArrays& a, int n, const ChainParamsDev& cp) {
   const int lane = threadIdx.x & 31;
-  warp_sort_u64(a.keys, n);
-  // DP (src/chain.cpp:22-45)
   for (int i = 0; i < n; ++i) {
     const uint64_t ki = a.keys[i];
     const uint32_t si = key_strand(ki);
     const int64_t ri = key_rpos(ki), qi = key_qpos(ki);
-    // Per round of 32 predecessors one redux over score * 32 + (31 - lane): the largest
-    // score, ties to the smallest lane = the nearest j; earlier (nearer) rounds win ties
-    // across rounds through the strict '>' below — the reference's scan order.
     int best_sc = 0, best_j = -1;
     for (int r0 = 0; r0 < cp.lookback; r0 += 32) {
       const int t = r0 + lane, j = i - 1 - t;
@@ -312,6 +309,70 @@ __device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const 
     }
     __syncwarp();
   }
+}
+
+// Sorts the n anchor keys, runs the DP, extracts chains into as.ch_*[c0 + j] and leaves
+// their final order in ord[0, m) (low 32 bits = j). Returns m in every lane.
+__device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const AnchorScratch& as, int64_t c0) {
+  const int lane = threadIdx.x & 31;
+  warp_sort_u64(a.keys, n);
+  // DP (src/chain.cpp:22-45) over a window of the 64 nearest predecessors kept in
+  // registers: for row i, lane t holds the key and f of anchors i-1-t (window 0) and
+  // i-33-t (window 1); after the row both windows move up one lane and row i enters at
+  // lane 0, so f never makes a round trip through memory on the DP's serial path. One
+  // redux per row takes the max of score * 64 + (63 - distance): the largest score, ties
+  // to the nearest predecessor (the reference scans j downward with a strict '>').
+  // A predecessor is considered only while the scan would not have stopped before it:
+  // anchors are sorted by (strand, rpos), so a strand change or dr > max_gap at j holds
+  // for every farther j too, and each lane can test its own j.
+  const unsigned FULL = 0xffffffffu;
+  if (cp.lookback > 64) {
+    chain_dp_rounds(a, n, cp);
+  } else {
+  uint64_t kw0 = 0, kw1 = 0;
+  int fw0 = 0, fw1 = 0;
+  uint64_t ki = n > 0 ? a.keys[0] : 0;
+  for (int i = 0; i < n; ++i) {
+    const uint64_t knext = i + 1 < n ? a.keys[i + 1] : 0;
+    const uint32_t si = key_strand(ki);
+    const int64_t ri = key_rpos(ki), qi = key_qpos(ki);
+    const auto score_of = [&](uint64_t kj, int fj, int t) {
+      if (t >= cp.lookback || t >= i || key_strand(kj) != si) return INT_MIN;
+      const int64_t dr = ri - key_rpos(kj), dq = qi - key_qpos(kj);
+      if (dr > cp.max_gap || dr <= 0 || dq <= 0) return INT_MIN;
+      const int64_t dd = dr > dq ? dr - dq : dq - dr;
+      if (dd > cp.band) return INT_MIN;
+      const int64_t g = dq < dr ? (dq < cp.k ? dq : cp.k) : (dr < cp.k ? dr : cp.k);
+      return (fj + static_cast<int>(g) - cp.cost[dd]) * 64 + (63 - t);
+    };
+    const int c0 = score_of(kw0, fw0, lane), c1 = score_of(kw1, fw1, 32 + lane);
+    const int m = __reduce_max_sync(FULL, c0 > c1 ? c0 : c1);
+    int fi = cp.k, pi = -1;
+    if (m != INT_MIN && (m >> 6) > cp.k) {
+      fi = m >> 6;
+      pi = i - 1 - (63 - (m & 63));
+    }
+    if (lane == 0) {
+      a.f[i] = fi;
+      a.prev[i] = pi;
+    }
+    // move the windows up one lane; row i enters window 0 at lane 0
+    const uint64_t out_k = __shfl_sync(FULL, kw0, 31);
+    const int out_f = __shfl_sync(FULL, fw0, 31);
+    kw1 = __shfl_up_sync(FULL, kw1, 1);
+    fw1 = __shfl_up_sync(FULL, fw1, 1);
+    kw0 = __shfl_up_sync(FULL, kw0, 1);
+    fw0 = __shfl_up_sync(FULL, fw0, 1);
+    if (lane == 0) {
+      kw1 = out_k;
+      fw1 = out_f;
+      kw0 = ki;
+      fw0 = fi;
+    }
+    ki = knext;
+  }
+  }
+  __syncwarp();
   // extraction order: f descending, index ascending (src/chain.cpp:49-50)
   for (int i = lane; i < n; i += 32) {
     a.ord[i] = static_cast<uint64_t>(desc32(a.f[i])) << 32 | static_cast<uint32_t>(i);

@@ -125,6 +125,8 @@ int dnaln_gpu_set_sub_batch(dnaln_ctx* ctx, int64_t reads);
  *   "sub_batch"      same as dnaln_gpu_set_sub_batch;
  *   "warp_seed_only" 1 = seed and chain every read one warp per read (default 0: short
  *                    reads one thread per read, the others one warp per read);
+ *   "length_order"   1 = SW tasks of a batch whose reads differ in length run longest
+ *                    first (default); 0 = in read order;
  *   "dir_cap_bytes"  traceback direction-code scratch per launch (default 1 GiB). */
 int dnaln_gpu_set_option(dnaln_ctx* ctx, const char* name, int64_t value);
 /* Page-locked host buffers for fast transfers (pass to the *_batch calls). */
