@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD,
                     help="synthetic workload (dnaln_b200.synth.WORKLOADS); the default is the headline one")
     ap.add_argument("--bw", type=int, default=16, help="SW band half-width (16, or 64 for the mixed-length workload)")
+    ap.add_argument("--cigar-per-read", type=int, default=0,
+                    help="CIGAR capacity per read of the output buffers (0 = the 2*len+3 bound)")
     ap.add_argument("--serve-requests", type=int, default=1500, help="requests per rate point (--workload serve)")
     ap.add_argument("--serve-lanes", type=int, default=3)
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.5, 0.8],
@@ -134,21 +136,29 @@ TASK_BYTES = 48 + 32  # SW task descriptor in, result out
 
 def kernel_bytes(kernel: str, st: dict, mean_len: float, bw: int = 16) -> float | None:
     """Algorithmic HBM bytes of all launches of one kernel, from the batch counters in st
-    (reads, minimizers, anchors, candidates, SW tasks). None for kernels not modelled."""
+    (reads, minimizers, anchors, candidates, SW tasks; the warp_* counters cover the reads
+    listed for the warp-per-read kernels). None for kernels not modelled."""
     n = st["reads"]
     mins = st["minimizers"] if st.get("minimizers") else 0.18 * mean_len * n
     W = 2 * bw + 1
+    cand_per_read = st["candidates"] / max(n, 1)
+    dir_row = max((W + 3) // 4 * 2, (W + 7) // 8 * 4)  # direction-code bytes per query row
     if kernel == "k_seed_chain_t":  # ASCII in, codes of both strands out, 16-B bucket per minimizer,
         # 4-B occurrence per anchor, 21-B candidate out, 36 B of per-read offsets / lengths / counts
-        return n * mean_len * (1 + 2) + mins * 16 + st["anchors"] * 4 + st["candidates"] * 21 + n * 36
+        return n * mean_len * (1 + 2) + mins * 16 + (st["anchors"] - st["warp_anchors"]) * 4 + \
+            st["candidates"] * 21 + n * 36
     if kernel == "k_seed":        # ASCII in, codes of both strands out, 20-B minimizer slot out + 16-B bucket
         return n * mean_len * (1 + 2) + mins * (20 + 16) + n * 24
-    if kernel == "k_chain_map":   # minimizer slots in, 4-B occurrence per anchor, 21-B candidate out
-        return mins * 20 + st["anchors"] * 4 + st["candidates"] * 21 + n * 28
-    if kernel == "k_sw_u2<tb>":   # query + window in, direction words out (W/4 words of 2 B per row), task/result
+    if kernel == "k_seed<list>":  # listed reads: ASCII in (codes already written), slots out + buckets
+        return st["warp_bases"] + st["warp_minimizers"] * (20 + 16) + st["warp_reads"] * 24
+    if kernel in ("k_chain_map", "k_chain_map<list>"):  # minimizer slots in, 4-B occurrence per anchor,
+        # 21-B candidate out, 28 B of per-read offsets / counts
+        r = st["warp_reads"]
+        return st["warp_minimizers"] * 20 + st["warp_anchors"] * 4 + r * cand_per_read * 21 + r * 28
+    if kernel in ("k_sw_u2<tb>", "k_sw_wide<tb>"):  # query + window in, direction codes out, task/result
         t = st["sw_tasks_tb"]
-        return t * (mean_len + (mean_len + 2 * bw) + mean_len * ((W + 3) // 4) * 2 + TASK_BYTES)
-    if kernel == "k_sw_u2<score>":
+        return t * (mean_len + (mean_len + 2 * bw) + mean_len * dir_row + TASK_BYTES)
+    if kernel in ("k_sw_u2<score>", "k_sw_wide<score>"):
         t = st["sw_tasks_score"]
         return t * (mean_len + (mean_len + 2 * bw) + TASK_BYTES)
     if kernel == "k_sw_walk":     # one direction word per step (~len steps), query/window bytes on the path, CIGAR
@@ -310,7 +320,7 @@ def run_ours(args) -> None:
     for part in parts:
         n = len(part)
         lens = part.seq_len
-        cap = int(np.sum(2 * lens.astype(np.int64) + 3))
+        cap = int(np.sum(2 * lens.astype(np.int64) + 3)) if not args.cigar_per_read else n * args.cigar_per_read
         dev.append(dict(
             n=n, cap=cap,
             seq=torch.from_numpy(part.seq).cuda(),
@@ -392,7 +402,7 @@ def run_ours(args) -> None:
     for part in parts:
         n = len(part)
         lens = part.seq_len
-        cap = int(np.sum(2 * lens.astype(np.int64) + 3))
+        cap = int(np.sum(2 * lens.astype(np.int64) + 3)) if not args.cigar_per_read else n * args.cigar_per_read
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
         host.append(dict(n=n, cap=cap, seq=pin(part.seq), off=pin(part.seq_off[:-1]), len=pin(lens),
                          hash=pin(part.name_hash().view(np.int32)),
@@ -496,7 +506,7 @@ def run_ours(args) -> None:
            "index": dict(build_s=index_build_s, where="dnaln_gpu_index_build",
                          **{k: v for k, v in ctx.index_stats(iid).items() if k in ("n_keys", "device_bytes")}),
            "candidates_per_read": st["candidates"] / max(st["reads"], 1)}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == WORKLOAD:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(g, reads, p)
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -50,7 +50,9 @@ class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("reads", "mapped", "anchors", "candidates", "cells", "sw_tasks_score",
                                           "sw_tasks_tb", "minimizers")] + \
                [(n, C.c_double) for n in ("ms_seed", "ms_chain", "ms_sw_score", "ms_sw_tb", "ms_post", "ms_h2d",
-                                          "ms_d2h", "ms_total")] + [("launches", C.c_uint64)]
+                                          "ms_d2h", "ms_total")] + \
+               [(n, C.c_uint64) for n in ("launches", "warp_reads", "warp_minimizers", "warp_anchors",
+                                          "warp_bases")]
 
 
 class KernelTime(C.Structure):

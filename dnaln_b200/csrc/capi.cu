@@ -324,6 +324,17 @@ __global__ void k_len64(const int32_t* __restrict__ len, int64_t n, int64_t* __r
   if ((threadIdx.x & 31) == 0 && l > 0) atomicMax(max_len, static_cast<unsigned long long>(l));
 }
 
+// *out += sum of vals[list[x]] for x < *list_n (minimizers of the reads listed for the
+// warp path): a warp sum, then one atomic per warp.
+__global__ void k_list_sum(const int32_t* __restrict__ vals, const int32_t* __restrict__ list,
+                           const int* __restrict__ list_n, unsigned long long* __restrict__ out) {
+  const int m = *list_n;
+  long long acc = 0;
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < m; x += gridDim.x * blockDim.x) acc += vals[list[x]];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, static_cast<unsigned long long>(acc));
+}
+
 __global__ void k_cig_slots(const int64_t* __restrict__ pofs, int64_t n, int64_t* __restrict__ out) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) out[i] = 2 * pofs[i] + i;
@@ -449,8 +460,9 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   DBUF(pofs, int64_t, "pofs", n + 1);
   // info: [0] longest read, [1..3] cells, mapped, candidates (map.cuh), [4] minimizers,
   // [5] anchors of the thread path
-  DBUF(info, unsigned long long, "info", 6);
-  CK(cudaMemsetAsync(info, 0, 6 * sizeof(unsigned long long), st));
+  // [6] minimizers and [7] bases of the reads listed for the warp path
+  DBUF(info, unsigned long long, "info", 8);
+  CK(cudaMemsetAsync(info, 0, 8 * sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
   CK(cudaMemsetAsync(c->d_count, 0, 3 * sizeof(int), st));
   unsigned long long* ctr = info + 1;  // cells, mapped, candidates (map.cuh)
@@ -523,17 +535,26 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
     CK(cub::DeviceReduce::Sum(nullptr, tmp, n_min, total, n, st));
     DBUF(t, uint8_t, "cub_tmp_red", tmp);
     CK(cub::DeviceReduce::Sum(t, tmp, n_min, total, n, st));
-    if (thread_path) CK(cub::DeviceReduce::Sum(t, tmp, n_anc_t, total + 1, n, st));
+    if (thread_path) {
+      CK(cub::DeviceReduce::Sum(t, tmp, n_anc_t, total + 1, n, st));
+      kt.begin(st, "k_list_sum");
+      k_list_sum<<<nblk(std::min<int64_t>(n, 148 * 256)), 256, 0, st>>>(n_min, big_list, big_n, info + 6);
+      k_list_sum<<<nblk(std::min<int64_t>(n, 148 * 256)), 256, 0, st>>>(d_seq_len, big_list, big_n, info + 7);
+      kt.end(st);
+    }
   }
   CK(cudaMemcpyAsync(c->h_info, anchor_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(c->h_info + 1, info + 4, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(c->h_info + 3, big_n, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 4, info + 6, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   const int64_t A = c->h_info[0];
   const int64_t n_minimizers = c->h_info[1];
   const int64_t n_anchors_thread = c->h_info[2];
   int n_big = 0;
   std::memcpy(&n_big, c->h_info + 3, sizeof n_big);
+  const int64_t n_minimizers_warp = thread_path ? c->h_info[4] : n_minimizers;
+  const int64_t n_bases_warp = thread_path ? c->h_info[5] : B;
 
   // pass 2 of the warp path: anchors, chains, candidates
   AnchorScratch as;
@@ -646,13 +667,17 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   s.reads += static_cast<uint64_t>(n);
   s.anchors += static_cast<uint64_t>(A + n_anchors_thread);
   s.minimizers += static_cast<uint64_t>(n_minimizers);
+  s.warp_reads += static_cast<uint64_t>(thread_path ? n_big : n);
+  s.warp_minimizers += static_cast<uint64_t>(n_minimizers_warp);
+  s.warp_anchors += static_cast<uint64_t>(A);
+  s.warp_bases += static_cast<uint64_t>(n_bases_warp);
   s.sw_tasks_score += static_cast<uint64_t>(counts[0]);
   s.sw_tasks_tb += static_cast<uint64_t>(counts[1]);
   s.cells += n_cells;
   s.mapped += n_mapped;
   s.candidates += n_cands;
   // k_len64, k_score_tasks, k_choose, k_cig_slots, k_records, k_cigar_gather, plus pass 1 / 2
-  s.launches += 6 + (thread_path ? 2 + (n_big > 0 ? 1 : 0) : 2);
+  s.launches += 6 + (thread_path ? 4 + (n_big > 0 ? 1 : 0) : 2);
   s.ms_seed += ev_ms(c, kEvSeed0, kEvSeed1);
   s.ms_chain += ev_ms(c, kEvChain0, kEvChain1);
   s.ms_sw_score += ev_ms(c, kEvSc0, kEvSc1);

@@ -329,24 +329,29 @@ __device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const 
   if (cp.lookback > 64) {
     chain_dp_rounds(a, n, cp);
   } else {
-  uint64_t kw0 = 0, kw1 = 0;
-  int fw0 = 0, fw1 = 0;
+  // window registers: rpos, qpos, strand and f of anchors i-1-lane and i-33-lane
+  int rw0 = 0, qw0 = 0, fw0 = 0, rw1 = 0, qw1 = 0, fw1 = 0;
+  uint32_t sw0 = 0, sw1 = 0;
+  const bool two = cp.lookback > 32;  // window 1 holds predecessors only beyond 32
   uint64_t ki = n > 0 ? a.keys[0] : 0;
   for (int i = 0; i < n; ++i) {
     const uint64_t knext = i + 1 < n ? a.keys[i + 1] : 0;
     const uint32_t si = key_strand(ki);
-    const int64_t ri = key_rpos(ki), qi = key_qpos(ki);
-    const auto score_of = [&](uint64_t kj, int fj, int t) {
-      if (t >= cp.lookback || t >= i || key_strand(kj) != si) return INT_MIN;
-      const int64_t dr = ri - key_rpos(kj), dq = qi - key_qpos(kj);
-      if (dr > cp.max_gap || dr <= 0 || dq <= 0) return INT_MIN;
-      const int64_t dd = dr > dq ? dr - dq : dq - dr;
-      if (dd > cp.band) return INT_MIN;
-      const int64_t g = dq < dr ? (dq < cp.k ? dq : cp.k) : (dr < cp.k ? dr : cp.k);
-      return (fj + static_cast<int>(g) - cp.cost[dd]) * 64 + (63 - t);
+    const int ri = static_cast<int>(key_rpos(ki)), qi = key_qpos(ki);
+    // rpos < 2^31 and |qpos| < 2^30, so dr and dq fit 32 bits; dd is formed in unsigned
+    // arithmetic and used only when dr and dq passed the range tests
+    const auto score_of = [&](int rj, int qj, uint32_t sj, int fj, int t) -> int {
+      const int dr = ri - rj, dq = qi - qj;
+      const int dd = static_cast<int>(dr > dq ? static_cast<uint32_t>(dr) - static_cast<uint32_t>(dq)
+                                              : static_cast<uint32_t>(dq) - static_cast<uint32_t>(dr));
+      if (t >= cp.lookback || t >= i || sj != si || dr > cp.max_gap || dr <= 0 || dq <= 0 || dd > cp.band)
+        return INT_MIN;
+      const int g = min(min(dq, dr), cp.k);
+      return (fj + g - cp.cost[dd]) * 64 + (63 - t);
     };
-    const int c0 = score_of(kw0, fw0, lane), c1 = score_of(kw1, fw1, 32 + lane);
-    const int m = __reduce_max_sync(FULL, c0 > c1 ? c0 : c1);
+    int c = score_of(rw0, qw0, sw0, fw0, lane);
+    if (two && i > 32) c = max(c, score_of(rw1, qw1, sw1, fw1, 32 + lane));
+    const int m = __reduce_max_sync(FULL, c);
     int fi = cp.k, pi = -1;
     if (m != INT_MIN && (m >> 6) > cp.k) {
       fi = m >> 6;
@@ -357,17 +362,30 @@ __device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const 
       a.prev[i] = pi;
     }
     // move the windows up one lane; row i enters window 0 at lane 0
-    const uint64_t out_k = __shfl_sync(FULL, kw0, 31);
-    const int out_f = __shfl_sync(FULL, fw0, 31);
-    kw1 = __shfl_up_sync(FULL, kw1, 1);
-    fw1 = __shfl_up_sync(FULL, fw1, 1);
-    kw0 = __shfl_up_sync(FULL, kw0, 1);
+    if (two) {
+      const int out_r = __shfl_sync(FULL, rw0, 31), out_q = __shfl_sync(FULL, qw0, 31);
+      const int out_f = __shfl_sync(FULL, fw0, 31);
+      const uint32_t out_s = __shfl_sync(FULL, sw0, 31);
+      rw1 = __shfl_up_sync(FULL, rw1, 1);
+      qw1 = __shfl_up_sync(FULL, qw1, 1);
+      fw1 = __shfl_up_sync(FULL, fw1, 1);
+      sw1 = __shfl_up_sync(FULL, sw1, 1);
+      if (lane == 0) {
+        rw1 = out_r;
+        qw1 = out_q;
+        fw1 = out_f;
+        sw1 = out_s;
+      }
+    }
+    rw0 = __shfl_up_sync(FULL, rw0, 1);
+    qw0 = __shfl_up_sync(FULL, qw0, 1);
     fw0 = __shfl_up_sync(FULL, fw0, 1);
+    sw0 = __shfl_up_sync(FULL, sw0, 1);
     if (lane == 0) {
-      kw1 = out_k;
-      fw1 = out_f;
-      kw0 = ki;
+      rw0 = ri;
+      qw0 = qi;
       fw0 = fi;
+      sw0 = si;
     }
     ki = knext;
   }

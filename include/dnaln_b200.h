@@ -90,6 +90,9 @@ typedef struct {
   double ms_post;     /* choose, MAPQ, records, CIGAR compaction */
   double ms_h2d, ms_d2h, ms_total;
   uint64_t launches;  /* kernels of this library launched (library scans excluded) */
+  /* reads seeded and chained one warp per read (long reads, or past the per-thread
+   * budget), their minimizers, anchors and bases */
+  uint64_t warp_reads, warp_minimizers, warp_anchors, warp_bases;
 } dnaln_stats;
 
 /* ---- context ---------------------------------------------------------------------- */

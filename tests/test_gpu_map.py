@@ -233,3 +233,24 @@ def test_full_size_workload_against_reference(ctx, ref):
             assert_same_as(ref.map(rg, part, p, nthreads=NTHREADS), res, len(part))
     finally:
         ctx.index_free(iid)
+
+
+@pytest.mark.slow
+def test_repeat_120mbp_workload_against_reference(ctx, ref):
+    # the 120 Mbp genome (8 contigs, repeat families, N runs; 1.28 GB index resident in HBM),
+    # 500,000 of its 150 bp reads in batches of 262,144: multi-candidate ranking, ties, MAPQ
+    g, reads, _ = synth.workload("repeat-120Mbp-10M-150bp", seed=2, n_reads=500_000)
+    p = D.default_map_params()
+    iid = ctx.index_build(g)
+    try:
+        assert ctx.index_stats(iid)["device_bytes"] > 1 << 30
+        rg = ref.genome(g)
+        multi = 0
+        for a in range(0, len(reads), 262_144):
+            part = reads.slice(a, min(len(reads), a + 262_144))
+            exp = ref.map(rg, part, p, nthreads=NTHREADS)
+            multi += int((exp[0][:, 6] > 1).sum())
+            assert_same_as(exp, ctx.map_batch(iid, part, p), len(part))
+        assert multi > 10_000
+    finally:
+        ctx.index_free(iid)
