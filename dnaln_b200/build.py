@@ -21,9 +21,9 @@ BUILD = PKG / "_build"
 LIB = PKG / "libdnaln_b200.so"
 
 CUDA_SOURCES = ["csrc/sw.cu", "csrc/seed.cu", "csrc/seed_thread.cu", "csrc/map.cu", "csrc/capi.cu", "csrc/noalloc.cu",
-                "csrc/serve.cu"]
-HOST_SOURCES = ["host/index_host.cpp", "host/sam.cpp", "host/synth.cpp"]
-HEADERS = ["csrc/common.cuh", "csrc/sw.cuh", "csrc/seed.cuh", "csrc/map.cuh", "host/index_host.hpp"]
+                "csrc/serve.cu", "csrc/index_build.cu"]
+HOST_SOURCES = ["host/sam.cpp", "host/synth.cpp"]
+HEADERS = ["csrc/common.cuh", "csrc/sw.cuh", "csrc/seed.cuh", "csrc/map.cuh", "csrc/index_build.cuh"]
 PUBLIC_HEADERS = ["dnaln_b200.h", "dnaln_synth.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -34,7 +34,7 @@
 
 #include "common.cuh"
 #include "dnaln_b200.h"
-#include "index_host.hpp"
+#include "index_build.cuh"
 #include "map.cuh"
 #include "seed.cuh"
 #include "sw.cuh"
@@ -1091,64 +1091,51 @@ int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases,
     if (contig_off[i] + contig_len[i] > n_bases || (i > 0 && contig_off[i] < contig_off[i - 1]))
       return fail(c, DNALN_ERR_INVALID_ARG, "contig %d is outside the genome or out of order", i);
   if (int e = set_device(c)) return e;
-  HostIndex h;
-  build_index_host(genome, contig_off, contig_len, n_contigs, k, w, h);
+  // the genome and contig table go up first; the index is then built where it will live
   IndexRes r;
   r.mem = std::make_shared<IndexMem>();
   r.device = c->device;
   IndexMem& m = *r.mem;
-  r.n_keys = h.n_keys;
-  r.n_pos = h.pos.size();
-  r.n_buckets = h.keys.size();
-  r.n_bases = n_bases;
-  r.max_count = h.max_count;
-  r.n_contigs = n_contigs;
-  r.k = k;
-  r.w = w;
-  std::vector<ulonglong2> table(h.keys.size());
-  for (size_t i = 0; i < table.size(); ++i)
-    table[i] = make_ulonglong2(h.keys[i], static_cast<uint64_t>(h.offs[i]) | static_cast<uint64_t>(h.cnts[i]) << 32);
-  // maximal runs of non-ACGT codes: SW tasks whose window avoids them skip the N scan
-  std::vector<uint2> runs;
-  for (uint64_t i = 0; i < n_bases;) {
-    if (genome[i] <= 3) {
-      ++i;
-      continue;
-    }
-    uint64_t j = i;
-    while (j < n_bases && genome[j] > 3) ++j;
-    runs.push_back(make_uint2(static_cast<uint32_t>(i), static_cast<uint32_t>(j)));
-    i = j;
-  }
   int e = DNALN_OK;
-  if ((e = dalloc(c, m.nruns, runs.size() * sizeof(uint2))) || (e = dalloc(c, m.table, table.size() * sizeof(ulonglong2))) ||
-      (e = dalloc(c, m.positions, h.pos.size() * sizeof(uint32_t))) || (e = dalloc(c, m.genome, n_bases)) ||
-      (e = dalloc(c, m.coff, n_contigs * sizeof(uint64_t))) || (e = dalloc(c, m.clen, n_contigs * sizeof(uint32_t)))) {
-    free_index(r);
+  if ((e = dalloc(c, m.genome, n_bases)) || (e = dalloc(c, m.coff, n_contigs * sizeof(uint64_t))) ||
+      (e = dalloc(c, m.clen, n_contigs * sizeof(uint32_t))))
     return e;
-  }
   cudaError_t x = cudaSuccess;
-  auto up = [&](DevBuf& b, const void* src, size_t bytes) {
-    if (x == cudaSuccess && bytes) x = cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice);
+  auto up = [&](DevBuf& b, const void* src, size_t bytes) {  // ordered before the build on c->st
+    if (x == cudaSuccess && bytes) x = cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, c->st);
   };
-  up(m.table, table.data(), table.size() * sizeof(ulonglong2));
-  up(m.positions, h.pos.data(), h.pos.size() * sizeof(uint32_t));
   up(m.genome, genome, n_bases);
   up(m.coff, contig_off, n_contigs * sizeof(uint64_t));
   up(m.clen, contig_len, n_contigs * sizeof(uint32_t));
-  up(m.nruns, runs.data(), runs.size() * sizeof(uint2));
-  if (x != cudaSuccess) {
-    free_index(r);
-    return fail(c, DNALN_ERR_CUDA, "index upload: %s", cudaGetErrorString(x));
+  if (x != cudaSuccess) return fail(c, DNALN_ERR_CUDA, "index upload: %s", cudaGetErrorString(x));
+  DeviceIndexBuild b;
+  char why[256] = {};
+  e = build_index_on_device(c->st, static_cast<const uint8_t*>(m.genome.p), n_bases, contig_off, contig_len, n_contigs,
+                            k, w, &b, why, sizeof why);
+  // the built arrays belong to the index from here on (freed with it on every path)
+  m.table = DevBuf{b.table, b.n_buckets * sizeof(ulonglong2)};
+  m.positions = DevBuf{b.positions, b.n_pos * sizeof(uint32_t)};
+  m.nruns = DevBuf{b.n_runs, static_cast<size_t>(b.n_n_runs) * sizeof(uint2)};
+  if (e != DNALN_OK) {
+    cudaStreamSynchronize(c->st);
+    return fail(c, e, "%s", why);
   }
+  r.n_keys = b.n_keys;
+  r.n_pos = b.n_pos;
+  r.n_buckets = b.n_buckets;
+  r.n_bases = n_bases;
+  r.max_count = b.max_count;
+  r.n_contigs = n_contigs;
+  r.k = k;
+  r.w = w;
   r.dev.table = static_cast<const ulonglong2*>(m.table.p);
   r.dev.positions = static_cast<const uint32_t*>(m.positions.p);
   r.dev.genome = static_cast<const uint8_t*>(m.genome.p);
   r.dev.contig_off = static_cast<const uint64_t*>(m.coff.p);
   r.dev.contig_len = static_cast<const uint32_t*>(m.clen.p);
   r.dev.n_runs = static_cast<const uint2*>(m.nruns.p);
-  r.dev.n_n_runs = static_cast<int32_t>(runs.size());
-  r.dev.mask = h.mask;
+  r.dev.n_n_runs = b.n_n_runs;
+  r.dev.mask = b.mask;
   r.dev.n_contigs = n_contigs;
   r.dev.k = k;
   r.dev.w = w;

@@ -66,6 +66,55 @@ def test_index_layout_matches_port(ctx, port, small_genome):
         ctx.index_free(iid)
 
 
+def _ragged_genome(rng):
+    # contigs of 0, 3, 40, 2,000, 30,000 and 120,000 bases, N runs inside and at the contig
+    # edges, one contig all N
+    lens = [0, 3, 40, 2000, 30000, 500, 120000]
+    parts = []
+    for i, n in enumerate(lens):
+        c = random_codes(rng, n, 0.002)
+        if n >= 40:
+            c[:7] = 4
+            c[-5:] = 4
+        if i == 5:
+            c[:] = 4
+        parts.append(c)
+    off = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.uint64)
+    return D.Genome(np.concatenate(parts).astype(np.uint8), off, np.array(lens, np.uint32))
+
+
+@pytest.mark.parametrize("k,w", [(15, 10), (4, 1), (28, 255), (12, 5), (21, 40)])
+def test_index_build_on_device_matches_port(ctx, port, k, w):
+    # the device build (sketch of every contig, stable sort, rank-ordered bucket placement)
+    # must give the reference's table bucket for bucket, for ragged contigs, N runs and the
+    # extreme k / w (even k: palindromic k-mers)
+    g = _ragged_genome(np.random.default_rng(k * 1000 + w))
+    iid = ctx.index_build(g, k, w)
+    try:
+        keys, offs, cnts, pos = ctx.index_export(iid)
+        pk, po, pc, pp = port.index(g, k, w).export()
+        assert np.array_equal(keys, pk) and np.array_equal(offs, po) and np.array_equal(cnts, pc)
+        assert np.array_equal(pos, pp)
+        st = ctx.index_stats(iid)
+        ps = port.index(g, k, w).stats()
+        for kk in ("n_keys", "n_positions", "max_count", "memory_bytes"):
+            assert st[kk] == ps[kk], kk
+    finally:
+        ctx.index_free(iid)
+
+
+def test_index_build_all_n_and_tiny(ctx, port):
+    for codes, lens in [(np.full(1000, 4, np.uint8), [1000]), (np.array([0, 1, 2], np.uint8), [3])]:
+        g = D.Genome(codes, np.array([0], np.uint64), np.array(lens, np.uint32))
+        iid = ctx.index_build(g, 15, 10)
+        try:
+            keys, offs, cnts, pos = ctx.index_export(iid)
+            assert ctx.index_stats(iid)["n_keys"] == 0 and len(pos) == 0
+            assert np.array_equal(keys, port.index(g, 15, 10).export()[0])
+        finally:
+            ctx.index_free(iid)
+
+
 def test_lookup_every_minimizer_and_absent(ctx, ref, small_genome):
     g = small_genome
     iid = ctx.index_build(g, 15, 10)
