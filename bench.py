@@ -287,6 +287,82 @@ def run_reference_serve(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def text_pipeline(ctx, iid, reads, g, p, steps: int) -> dict:
+    """The workload from FASTQ text in memory to SAM text in memory, through the C ABI with
+    no copies in between: dnaln_parse_reads on all host threads, the host-buffer mapping
+    call on the parsed arrays in batches of 262,144 (submit / wait, so one batch's copies
+    overlap the next one's kernels), dnaln_sam_format_mt on all host threads into one
+    reused buffer. Wall clock per step, the three parts one after another."""
+    import tempfile
+
+    import dnaln_b200 as D
+    from dnaln_b200 import _native as N
+    from dnaln_b200 import synth
+    L = N.lib()
+    with tempfile.NamedTemporaryFile(suffix=".fq") as f:
+        synth.write_fastq(reads, f.name)
+        text = np.fromfile(f.name, np.uint8)
+    threads = len(os.sched_getaffinity(0))
+    n_all = len(reads)
+    spans = [(a, min(n_all, a + BATCH)) for a in range(0, n_all, BATCH)]
+    lens_all = reads.seq_len.astype(np.int64)
+    caps = [int(np.sum(2 * lens_all[a:b] + 3)) for a, b in spans]
+    recs = [np.zeros(b - a, D.MAP_RECORD_DTYPE) for a, b in spans]
+    cigs = [np.zeros(c, np.uint32) for c in caps]
+    used = [C.c_int64() for _ in spans]
+    cn, co = g.name_buffers()
+    sam = np.zeros(int(np.sum(2 * lens_all)) + 200 * n_all + (1 << 20), np.uint8)
+    err = C.create_string_buffer(256)
+    t_parse = t_map = t_sam = 0.0
+    sam_bytes = 0
+    for step in range(steps + 1):  # the first step warms the page cache and the buffers
+        t0 = time.perf_counter()
+        h = C.c_void_p()
+        rc = L.dnaln_parse_reads(text.ctypes.data, len(text), threads, C.byref(h), C.addressof(err), 256)
+        if rc:
+            raise RuntimeError(err.value.decode())
+        n = C.c_int64()
+        v = [C.c_void_p() for _ in range(8)]
+        L.dnaln_reads_view(h, C.byref(n), *[C.byref(x) for x in v])
+        seq, so, sl, nm, no, ql, qo, nh = [x.value for x in v]
+        t1 = time.perf_counter()
+        tickets = []
+        for k, (a, b) in enumerate(spans):
+            t = C.c_int64()
+            rc = L.dnaln_gpu_map_submit(ctx.handle, iid, seq, so + 8 * a, sl + 4 * a, nh + 4 * a, b - a, C.byref(p),
+                                        recs[k].ctypes.data, cigs[k].ctypes.data, caps[k], C.byref(used[k]),
+                                        C.byref(t))
+            if rc:
+                raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
+            tickets.append(t.value)
+        for t in tickets:
+            if L.dnaln_gpu_map_wait(ctx.handle, t):
+                raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
+        t2 = time.perf_counter()
+        out_at = 0
+        for k, (a, b) in enumerate(spans):
+            u = C.c_int64()
+            rc = L.dnaln_sam_format_mt(seq, so + 8 * a, sl + 4 * a, nm, no + 8 * a, ql, qo + 8 * a, recs[k].ctypes.data,
+                                       cigs[k].ctypes.data, b - a, cn.ctypes.data, co.ctypes.data, threads,
+                                       sam.ctypes.data + out_at, len(sam) - out_at, C.byref(u))
+            if rc:
+                raise RuntimeError(f"SAM formatting failed ({rc})")
+            out_at += u.value
+        t3 = time.perf_counter()
+        L.dnaln_reads_free(h)
+        if step:
+            t_parse += t1 - t0
+            t_map += t2 - t1
+            t_sam += t3 - t2
+            sam_bytes = out_at
+    total = t_parse + t_map + t_sam
+    return {"value": steps * n_all / total, "unit": METRIC, "host_threads": threads,
+            "ms_per_step": {"parse": 1e3 * t_parse / steps, "map": 1e3 * t_map / steps, "sam": 1e3 * t_sam / steps},
+            "text_bytes_in": int(len(text)), "sam_bytes_out": int(sam_bytes),
+            "what": "FASTQ text in memory -> dnaln_parse_reads -> dnaln_gpu_map_submit/wait on the parsed "
+                    "(pageable) arrays -> dnaln_sam_format_mt -> SAM text in memory; wall clock, parts in sequence"}
+
+
 def run_ours(args) -> None:
     import torch
     import dnaln_b200 as D
@@ -458,6 +534,11 @@ def run_ours(args) -> None:
     h2d = sum(h["h2d"] for h in host)
     d2h = sum(40 * h["n"] for h in host) + 4 * sum(e2e_used.values())
 
+    # ---- end to end from FASTQ text to SAM text (host parse and format included) -------
+    e2e_text = None
+    if args.workload == WORKLOAD and rank == 0 and world == 1:
+        e2e_text = text_pipeline(ctx, iid, reads, g, p, max(2, min(args.steps, 5)))
+
     # ---- roofline of the dominant kernel ----------------------------------------------
     stage_ms = {"seed": st["ms_seed"], "chain": st["ms_chain"], "sw_score": st["ms_sw_score"], "sw_tb": st["ms_sw_tb"],
                 "post": st["ms_post"]}
@@ -506,6 +587,8 @@ def run_ours(args) -> None:
            "index": dict(build_s=index_build_s, where="dnaln_gpu_index_build",
                          **{k: v for k, v in ctx.index_stats(iid).items() if k in ("n_keys", "device_bytes")}),
            "candidates_per_read": st["candidates"] / max(st["reads"], 1)}
+    if e2e_text:
+        out["e2e_text"] = e2e_text
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(g, reads, p)
     if rank == 0:

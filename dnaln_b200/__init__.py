@@ -27,7 +27,7 @@ from . import _native as N
 from ._native import (ALIGN_RESULT_DTYPE, MAP_RECORD_DTYPE, ChainParams, MapParams, ScoreParams, Stats, lib, ptr)
 
 __all__ = ["Context", "Genome", "ReadBatch", "DnalnError", "ScoreParams", "ChainParams", "MapParams",
-           "default_map_params", "sam_format", "fnv1a", "lib", "MAP_RECORD_DTYPE", "ALIGN_RESULT_DTYPE",
+           "default_map_params", "sam_format", "parse_reads", "fnv1a", "lib", "MAP_RECORD_DTYPE", "ALIGN_RESULT_DTYPE",
            "cigar_to_string"]
 
 CIGAR_OPS = "MIDNSHP=X"
@@ -98,6 +98,7 @@ class ReadBatch:
     names: np.ndarray     # uint8
     name_off: np.ndarray  # int64, n+1
     qual: np.ndarray | None = None  # uint8, same offsets as seq (None = '*')
+    qual_off: np.ndarray | None = None  # int64, n+1: qualities with offsets of their own (mixed FASTA/FASTQ)
 
     def __post_init__(self):
         self.seq = np.ascontiguousarray(self.seq, dtype=np.uint8)
@@ -140,9 +141,11 @@ class ReadBatch:
     def slice(self, a: int, b: int) -> "ReadBatch":
         so = self.seq_off[a:b + 1] - self.seq_off[a]
         no = self.name_off[a:b + 1] - self.name_off[a]
-        q = None if self.qual is None else self.qual[self.seq_off[a]:self.seq_off[b]].copy()
+        qo = self.seq_off if self.qual_off is None else self.qual_off
+        q = None if self.qual is None else self.qual[qo[a]:qo[b]].copy()
+        qn = None if self.qual_off is None else self.qual_off[a:b + 1] - self.qual_off[a]
         return ReadBatch(self.seq[self.seq_off[a]:self.seq_off[b]].copy(), so,
-                         self.names[self.name_off[a]:self.name_off[b]].copy(), no, q)
+                         self.names[self.name_off[a]:self.name_off[b]].copy(), no, q, qn)
 
 
 @dataclass
@@ -393,8 +396,47 @@ class MapTicket:
     ticket: int = 0
 
 
-def sam_format(reads: ReadBatch, res: MapResult, genome: Genome) -> bytes:
-    """SAM body lines of a mapped batch (Mapper::append_sam, src/mapper.cpp:231-270)."""
+def parse_reads(text: bytes, threads: int = 0) -> ReadBatch:
+    """FASTA/FASTQ text -> ReadBatch (SeqReader::next, src/seqio.cpp:59-80), on `threads`
+    host threads (0 = all) for four-line FASTQ; raises DnalnError on malformed FASTQ."""
+    buf = np.frombuffer(text, np.uint8) if len(text) else np.zeros(1, np.uint8)
+    h = C.c_void_p()
+    err = C.create_string_buffer(256)
+    rc = lib().dnaln_parse_reads(ptr(buf), len(text), threads, C.byref(h), C.addressof(err), 256)
+    if rc != N.OK:
+        raise DnalnError(rc, err.value.decode(errors="replace"))
+    try:
+        n = C.c_int64()
+        v = [C.c_void_p() for _ in range(8)]
+        lib().dnaln_reads_view(h, C.byref(n), *[C.byref(x) for x in v])
+        m = n.value
+
+        def arr(p, dt, cnt):
+            if cnt == 0 or not p.value:
+                return np.zeros(cnt, dt)
+            return np.ctypeslib.as_array(C.cast(p, C.POINTER(np.ctypeslib.as_ctypes_type(dt))), (cnt,)).copy()
+        so = arr(v[1], np.int64, m + 1)
+        no = arr(v[4], np.int64, m + 1)
+        seq = arr(v[0], np.uint8, int(so[-1]) if m else 0)
+        names = arr(v[3], np.uint8, int(no[-1]) if m else 0)
+        qual = None
+        qo = None
+        if v[5].value:
+            qo = arr(v[6], np.int64, m + 1)
+            qual = arr(v[5], np.uint8, int(qo[-1]) if m else 0)
+            if np.array_equal(qo, so):
+                qo = None
+        rb = ReadBatch(seq if len(seq) else np.zeros(1, np.uint8), so, names if len(names) else np.zeros(1, np.uint8),
+                       no, qual, qo)
+        rb._hash = arr(v[7], np.uint32, m)
+        return rb
+    finally:
+        lib().dnaln_reads_free(h)
+
+
+def sam_format(reads: ReadBatch, res: MapResult, genome: Genome, threads: int = 1) -> bytes:
+    """SAM body lines of a mapped batch (Mapper::append_sam, src/mapper.cpp:231-270), on
+    `threads` host threads (0 = all)."""
     n = len(reads)
     if n == 0:
         return b""
@@ -407,8 +449,19 @@ def sam_format(reads: ReadBatch, res: MapResult, genome: Genome) -> bytes:
     recs = np.ascontiguousarray(res.records)
     cig = np.ascontiguousarray(res.cigar, dtype=np.uint32) if len(res.cigar) else np.zeros(1, np.uint32)
     args = [ptr(reads.seq), ptr(off), ptr(lens), ptr(reads.names), ptr(reads.name_off),
-            ptr(qual) if qual is not None else None, ptr(reads.seq_off) if qual is not None else None,
+            ptr(qual) if qual is not None else None,
+            (ptr(reads.qual_off) if reads.qual_off is not None else ptr(reads.seq_off)) if qual is not None else None,
             ptr(recs), ptr(cig), n, ptr(cn), ptr(co)]
+    if threads != 1:
+        est = int(2 * np.sum(lens.astype(np.int64)) + 512 * n + 4096)
+        out = np.zeros(est, np.uint8)
+        rc = lib().dnaln_sam_format_mt(*args, threads, ptr(out), est, C.byref(used))
+        if rc == N.ERR_CAPACITY:
+            out = np.zeros(used.value + 1, np.uint8)
+            rc = lib().dnaln_sam_format_mt(*args, threads, ptr(out), used.value + 1, C.byref(used))
+        if rc != N.OK:
+            raise DnalnError(rc, "SAM formatting failed")
+        return out[:used.value].tobytes()
     lib().dnaln_sam_format(*args, None, 0, C.byref(used))
     out = np.zeros(used.value + 1, np.uint8)
     rc = lib().dnaln_sam_format(*args, ptr(out), used.value + 1, C.byref(used))

@@ -142,6 +142,10 @@ SIGNATURES = {
     "dnaln_fnv1a": (u32, [C.c_char_p, i64]),
     "dnaln_fnv1a_batch": (None, [P, P, i64, P]),
     "dnaln_sam_format": (C.c_int, [P, P, P, P, P, P, P, P, P, i64, P, P, P, i64, C.POINTER(i64)]),
+    "dnaln_sam_format_mt": (C.c_int, [P, P, P, P, P, P, P, P, P, i64, P, P, i32, P, i64, C.POINTER(i64)]),
+    "dnaln_parse_reads": (C.c_int, [P, i64, i32, C.POINTER(P), P, i64]),
+    "dnaln_reads_view": (C.c_int, [P, C.POINTER(i64)] + [C.POINTER(P)] * 8),
+    "dnaln_reads_free": (None, [P]),
     "dnaln_synth_genome": (C.c_int, [u64, C.POINTER(SynthGenomeSpec), P]),
     "dnaln_synth_reads_bytes": (i64, [u64, C.POINTER(SynthReadsSpec)]),
     "dnaln_synth_reads": (C.c_int, [u64, P, P, P, i32, C.POINTER(SynthReadsSpec), P, i64, P, P, i64, P, P, P, P]),

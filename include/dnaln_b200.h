@@ -304,6 +304,28 @@ int dnaln_sam_format(const char* seq, const int64_t* seq_off, const int32_t* seq
                      const dnaln_map_record* rec, const uint32_t* cigar, int64_t n, const char* cnames,
                      const int64_t* cname_off, char* out, int64_t cap, int64_t* used);
 
+/* dnaln_sam_format on `threads` host threads (0 = all hardware threads): each formats a
+ * contiguous range of records, the ranges are concatenated in order; the same bytes. */
+int dnaln_sam_format_mt(const char* seq, const int64_t* seq_off, const int32_t* seq_len, const char* names,
+                        const int64_t* name_off, const char* qual, const int64_t* qual_off,
+                        const dnaln_map_record* rec, const uint32_t* cigar, int64_t n, const char* cnames,
+                        const int64_t* cname_off, int32_t threads, char* out, int64_t cap, int64_t* used);
+
+/* SeqReader::next (src/seqio.cpp:59-80) over FASTA/FASTQ text already in memory (gzip
+ * decoding stays with the caller): records in the layout the mapping calls take, on
+ * `threads` host threads (0 = all) when the text is plain four-line FASTQ, else as the
+ * reference reads it, line by line. Malformed FASTQ fails with DNALN_ERR_INVALID_ARG and
+ * the reference's message in err (capacity err_cap), where the reference would exit. */
+typedef struct dnaln_reads dnaln_reads;
+int dnaln_parse_reads(const char* text, int64_t len, int32_t threads, dnaln_reads** out, char* err, int64_t err_cap);
+/* Views of a parse: n records; sequences, names and qualities concatenated with n + 1
+ * offsets each (qual NULL when no record is FASTQ); name_hash[i] = FNV-1a of name i. Valid
+ * until dnaln_reads_free. */
+int dnaln_reads_view(const dnaln_reads* r, int64_t* n, const char** seq, const int64_t** seq_off,
+                     const int32_t** seq_len, const char** names, const int64_t** name_off, const char** qual,
+                     const int64_t** qual_off, const uint32_t** name_hash);
+void dnaln_reads_free(dnaln_reads* r);
+
 #ifdef __cplusplus
 }
 #endif

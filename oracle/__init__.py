@@ -226,7 +226,19 @@ class Reference:
                               C.POINTER(i64)]
         L.ref_fnv1a.restype = u32
         L.ref_fnv1a.argtypes = [P, i64]
+        L.ref_read_records.restype = C.c_int
+        L.ref_read_records.argtypes = [C.c_char_p, P, P, P, P, P, P, P]
         self.L = L
+
+    def read_records(self, path: str):
+        """read_all_records of a FASTA/FASTQ file: (seq, seq_off, names, name_off, qual, qual_off)."""
+        sz = np.zeros(4, np.int64)
+        self.L.ref_read_records(path.encode(), _p(sz), None, None, None, None, None, None)
+        n, sb, nb, qb = map(int, sz)
+        seq, names, qual = np.zeros(max(sb, 1), np.uint8), np.zeros(max(nb, 1), np.uint8), np.zeros(max(qb, 1), np.uint8)
+        so, no, qo = np.zeros(n + 1, np.int64), np.zeros(n + 1, np.int64), np.zeros(n + 1, np.int64)
+        self.L.ref_read_records(path.encode(), _p(sz), _p(seq), _p(so), _p(names), _p(no), _p(qual), _p(qo))
+        return seq[:sb], so, names[:nb], no, qual[:qb], qo
 
     def sketch(self, seq: np.ndarray, k: int, w: int, offset: int = 0):
         seq = np.ascontiguousarray(seq, np.uint8)

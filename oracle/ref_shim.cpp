@@ -10,6 +10,7 @@
 //   ref_chain         -> dnaln::Chainer::run                (src/chain.hpp:41)
 //   ref_align         -> dnaln::ScalarAligner / SimdAligner (src/align.hpp:70-104)
 //   ref_map           -> dnaln::Mapper::map + append_sam    (src/mapper.hpp:51-58)
+//   ref_read_records  -> dnaln::read_all_records            (src/seqio.hpp:47)
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -268,6 +269,39 @@ int64_t ref_map(void* gp, const char* seq, const int64_t* seq_off, const int32_t
     if (static_cast<int64_t>(body.size()) <= sam_cap) std::memcpy(sam, body.data(), body.size());
   }
   return total;
+}
+
+// read_all_records of a FASTA/FASTQ file (src/seqio.cpp:89-96). sizes4 = {records, sequence
+// bytes, name bytes, quality bytes}; with non-null buffers the records are also written
+// out, concatenated, with n + 1 offsets each. Well-formed input only: the reference exits
+// on malformed records.
+int ref_read_records(const char* path, int64_t* sizes4, char* seq, int64_t* seq_off, char* names, int64_t* name_off,
+                     char* qual, int64_t* qual_off) {
+  const std::vector<SeqRecord> v = read_all_records(path);
+  int64_t sb = 0, nb = 0, qb = 0;
+  for (size_t i = 0; i < v.size(); ++i) {
+    if (seq) {
+      seq_off[i] = sb;
+      name_off[i] = nb;
+      qual_off[i] = qb;
+      std::memcpy(seq + sb, v[i].seq.data(), v[i].seq.size());
+      std::memcpy(names + nb, v[i].name.data(), v[i].name.size());
+      std::memcpy(qual + qb, v[i].qual.data(), v[i].qual.size());
+    }
+    sb += static_cast<int64_t>(v[i].seq.size());
+    nb += static_cast<int64_t>(v[i].name.size());
+    qb += static_cast<int64_t>(v[i].qual.size());
+  }
+  if (seq) {
+    seq_off[v.size()] = sb;
+    name_off[v.size()] = nb;
+    qual_off[v.size()] = qb;
+  }
+  sizes4[0] = static_cast<int64_t>(v.size());
+  sizes4[1] = sb;
+  sizes4[2] = nb;
+  sizes4[3] = qb;
+  return 0;
 }
 
 // fnv1a of the reference (src/common.hpp:136-140), for tie-break checks.
