@@ -140,6 +140,7 @@ struct dnaln_ctx {
   bool stop = false;
   bool warp_seed_only = false;  // option: every read through the warp-per-read seeding kernels
   bool length_order = true;     // option: SW tasks of mixed-length batches run longest first
+  bool long_thread = true;      // option: listed long reads one thread each before the warp kernels
   // kernel trace: event pairs of the current batch, totals per kernel name
   bool trace_on = false, trace_open = false;
   std::string trace_only;  // non-empty: trace only the kernel of this name
@@ -464,7 +465,7 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   DBUF(info, unsigned long long, "info", 8);
   CK(cudaMemsetAsync(info, 0, 8 * sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
-  CK(cudaMemsetAsync(c->d_count, 0, 3 * sizeof(int), st));
+  CK(cudaMemsetAsync(c->d_count, 0, 4 * sizeof(int), st));
   unsigned long long* ctr = info + 1;  // cells, mapped, candidates (map.cuh)
   kt.begin(st, "k_len64");
   k_len64<<<nblk(n + 1), 256, 0, st>>>(d_seq_len, n, len64, info);
@@ -509,6 +510,12 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   DBUF(big_list, int32_t, "big_list", n);
   DBUF(n_anc_t, int32_t, "n_anc_t", n);
   int* big_n = c->d_count + 2;
+  // reads of mixed lengths: SW tasks (and the long reads of the seeding) longest first
+  const bool by_length =
+      c->length_order && static_cast<double>(max_len) > 1.25 * static_cast<double>(B) / static_cast<double>(n);
+  // the reads left for the warp kernels: those the thread kernels listed
+  int32_t* warp_list = big_list;
+  int* warp_n = big_n;
   CK(cudaEventRecord(c->ev[kEvSeed0], st));
   if (thread_path) {
     kt.begin(st, "k_seed_chain_t");
@@ -516,9 +523,41 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
                                              sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list, big_n, c->d_err);
     kt.end(st);
     if (!ok) return fail(c, DNALN_ERR_CUDA, "thread-per-read seeding kernel could not be configured");
+    if (c->long_thread && seed_long_supported(sp, cp) && max_len > seed_thread_max_len()) {
+      // long reads one thread each, in length order; what exceeds its bounds goes on
+      const int64_t lt = seed_long_threads(n);
+      DBUF(lscr, uint32_t, "long_scratch", seed_long_scratch_words(lt));
+      DBUF(big2, int32_t, "big2_list", n);
+      const int32_t* order = big_list;
+      if (by_length && n > 1) {
+        DBUF(lk_in, uint32_t, "long_kin", n);
+        DBUF(lk_out, uint32_t, "long_kout", n);
+        DBUF(lv_in, int32_t, "long_vin", n);
+        DBUF(lv_out, int32_t, "long_vout", n);
+        kt.begin(st, "k_long_keys");
+        launch_long_order(st, big_list, big_n, static_cast<int>(n), d_seq_len, lk_in, lv_in);
+        kt.end(st);
+        size_t tmp = 0;
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, lk_in, lk_out, lv_in, lv_out, static_cast<int>(n), 0, 32, st));
+        DBUF(tb, uint8_t, "cub_tmp_lsort", tmp);
+        kt.begin(st, "cub_sort");
+        CK(cub::DeviceRadixSort::SortPairs(tb, tmp, lk_in, lk_out, lv_in, lv_out, static_cast<int>(n), 0, 32, st));
+        kt.end(st);
+        order = lv_out;
+        c->stats.launches += 1;
+      }
+      kt.begin(st, "k_seed_chain_tl");
+      if (!launch_seed_chain_long(st, d_seq_len, pofs, codes, order, big_n, lt, ix.dev, sp, cp, cand, cb, n_min,
+                                  n_anchor, n_anc_t, lscr, big2, c->d_count + 3, seed_thread_max_len(), c->d_err))
+        return fail(c, DNALN_ERR_CUDA, "long-read seeding kernel could not be configured");
+      kt.end(st);
+      warp_list = big2;
+      warp_n = c->d_count + 3;
+      c->stats.launches += 1;
+    }
     kt.begin(st, "k_seed<list>");
-    launch_seed_list(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, big_list, big_n, codes, ix.dev, sp, mb,
-                     n_min, n_anchor, c->d_err);
+    launch_seed_list(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, warp_list, warp_n, codes, ix.dev, sp,
+                     mb, n_min, n_anchor, c->d_err);
     kt.end(st);
   } else {
     kt.begin(st, "k_seed");
@@ -538,21 +577,23 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
     if (thread_path) {
       CK(cub::DeviceReduce::Sum(t, tmp, n_anc_t, total + 1, n, st));
       kt.begin(st, "k_list_sum");
-      k_list_sum<<<nblk(std::min<int64_t>(n, 148 * 256)), 256, 0, st>>>(n_min, big_list, big_n, info + 6);
-      k_list_sum<<<nblk(std::min<int64_t>(n, 148 * 256)), 256, 0, st>>>(d_seq_len, big_list, big_n, info + 7);
+      k_list_sum<<<nblk(std::min<int64_t>(n, 148 * 256)), 256, 0, st>>>(n_min, warp_list, warp_n, info + 6);
+      k_list_sum<<<nblk(std::min<int64_t>(n, 148 * 256)), 256, 0, st>>>(d_seq_len, warp_list, warp_n, info + 7);
       kt.end(st);
     }
   }
   CK(cudaMemcpyAsync(c->h_info, anchor_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(c->h_info + 1, info + 4, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(c->h_info + 3, big_n, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 3, warp_n, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(c->h_info + 6, big_n, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(c->h_info + 4, info + 6, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   const int64_t A = c->h_info[0];
   const int64_t n_minimizers = c->h_info[1];
   const int64_t n_anchors_thread = c->h_info[2];
-  int n_big = 0;
+  int n_big = 0, n_listed = 0;  // reads for the warp kernels; reads the short thread kernel listed
   std::memcpy(&n_big, c->h_info + 3, sizeof n_big);
+  std::memcpy(&n_listed, c->h_info + 6, sizeof n_listed);
   const int64_t n_minimizers_warp = thread_path ? c->h_info[4] : n_minimizers;
   const int64_t n_bases_warp = thread_path ? c->h_info[5] : B;
 
@@ -574,7 +615,7 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   CK(cudaEventRecord(c->ev[kEvChain0], st));
   if (!thread_path || n_big > 0) {
     kt.begin(st, thread_path ? "k_chain_map<list>" : "k_chain_map");
-    launch_chain_map(st, pofs, d_seq_len, thread_path ? n_big : n, thread_path ? big_list : nullptr, n_min, anchor_off,
+    launch_chain_map(st, pofs, d_seq_len, thread_path ? n_big : n, thread_path ? warp_list : nullptr, n_min, anchor_off,
                      mb, ix.dev, cp, cand, as, cb, c->d_err);
     kt.end(st);
   }
@@ -592,8 +633,6 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   launch_score_tasks(st, n, pofs, d_seq_len, cb, ix.dev, mc, sc_tasks, c->d_count, ctr);
   kt.end(st);
   // reads of very different lengths: SW tasks longest first (lengths known on the host)
-  const bool by_length =
-      c->length_order && static_cast<double>(max_len) > 1.25 * static_cast<double>(B) / static_cast<double>(n);
   const SwTask* sc_run = sc_tasks;
   if (by_length)
     if (int e = sort_tasks_by_length(c, sc_tasks, static_cast<int>(n * MC), c->d_count, "sc", &sc_run)) return e;
@@ -671,6 +710,7 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   s.warp_minimizers += static_cast<uint64_t>(n_minimizers_warp);
   s.warp_anchors += static_cast<uint64_t>(A);
   s.warp_bases += static_cast<uint64_t>(n_bases_warp);
+  s.long_reads += static_cast<uint64_t>(thread_path && warp_list != big_list ? n_listed - n_big : 0);
   s.sw_tasks_score += static_cast<uint64_t>(counts[0]);
   s.sw_tasks_tb += static_cast<uint64_t>(counts[1]);
   s.cells += n_cells;
@@ -1051,6 +1091,10 @@ int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
   std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (k == "warp_seed_only") {
     c->warp_seed_only = value != 0;
+    return DNALN_OK;
+  }
+  if (k == "long_thread") {
+    c->long_thread = value != 0;
     return DNALN_OK;
   }
   if (k == "length_order") {

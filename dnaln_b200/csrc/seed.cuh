@@ -146,11 +146,30 @@ void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_l
 // for launch_seed_list / launch_chain_map. Returns false, launching nothing, when the
 // parameters are outside the path's range.
 bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp);
+int seed_thread_max_len();  // the longest read the short thread kernel stages
 bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
                               const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes,
                               const DevIndex& ix, const SeedParams& sp, const ChainParamsDev& cp,
                               const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
                               int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err);
+
+// Long reads, one thread each (seed_long.cu): the reads of list[0, *list_n) longer than
+// min_len (typically those the short kernel listed) with their state in `scratch`
+// (seed_long_scratch_words(threads) words); the others, and reads past its bounds, go to
+// next_list (count *next_n) for the warp kernels.
+// threads = seed_long_threads(upper bound of the list length).
+bool seed_long_supported(const SeedParams& sp, const ChainParamsDev& cp);
+int64_t seed_long_threads(int64_t n_max);
+size_t seed_long_scratch_words(int64_t threads);
+bool launch_seed_chain_long(cudaStream_t st, const int32_t* seq_len, const int64_t* pofs, const uint8_t* codes,
+                            const int32_t* list, const int* list_n, int64_t threads, const DevIndex& ix,
+                            const SeedParams& sp, const ChainParamsDev& cp, const CandParams& cand, CandBuf cb,
+                            int32_t* n_min, int64_t* n_anchor, int32_t* n_anc_t, uint32_t* scratch,
+                            int32_t* next_list, int* next_n, int min_len, uint32_t* err);
+// Sort keys (longest first; slots at or past *list_n last) and values (read ids) of a list
+// whose length is only known on the device; n_max = the list buffer's size.
+void launch_long_order(cudaStream_t st, const int32_t* list, const int* list_n, int n_max, const int32_t* seq_len,
+                       uint32_t* keys, int32_t* vals);
 
 // Stage entry points: sketch of code sequences, lookups, chaining of given anchor sets.
 void launch_sketch_codes(cudaStream_t st, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,

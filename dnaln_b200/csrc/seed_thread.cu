@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(kTT)
       const uint32_t he = a_hi(end);
       ch_at(0, nch) = score;
       ch_at(1, nch) = static_cast<int32_t>(he >> 31);
-      ch_at(2, nch) = dmin + (dmax - dmin) / 2;
+      ch_at(2, nch) = static_cast<int32_t>(dmin + (static_cast<int64_t>(dmax) - dmin) / 2);  // no int32 overflow
       ch_at(3, nch) = static_cast<int32_t>(he & 0x7FFFFFFFu);
       ++nch;
     }
@@ -436,6 +436,8 @@ __global__ void __launch_bounds__(kTT)
 }
 
 }  // namespace
+
+int seed_thread_max_len() { return kTMaxLen; }
 
 bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp) {
   return sp.w == kTW && sp.k >= 4 && sp.k <= 15 && cp.max_gap >= 0 && cp.max_gap < (1 << 29) && cp.band >= 0 &&

@@ -93,6 +93,7 @@ typedef struct {
   /* reads seeded and chained one warp per read (long reads, or past the per-thread
    * budget), their minimizers, anchors and bases */
   uint64_t warp_reads, warp_minimizers, warp_anchors, warp_bases;
+  uint64_t long_reads; /* reads seeded and chained by the long-read thread kernel */
 } dnaln_stats;
 
 /* ---- context ---------------------------------------------------------------------- */
@@ -128,6 +129,8 @@ int dnaln_gpu_set_sub_batch(dnaln_ctx* ctx, int64_t reads);
  *   "sub_batch"      same as dnaln_gpu_set_sub_batch;
  *   "warp_seed_only" 1 = seed and chain every read one warp per read (default 0: short
  *                    reads one thread per read, the others one warp per read);
+ *   "long_thread"    1 = reads the short thread kernel lists go one thread each through
+ *                    the long-read kernel first (default); 0 = straight to the warp kernels;
  *   "length_order"   1 = SW tasks of a batch whose reads differ in length run longest
  *                    first (default); 0 = in read order;
  *   "dir_cap_bytes"  traceback direction-code scratch per launch (default 1 GiB). */

@@ -123,22 +123,32 @@ def test_batch_invariance(ctx, repeat):
 
 @pytest.mark.parametrize("wl", ["repeat", "mixed", "small"])
 def test_thread_and_warp_seed_paths_identical(ctx, request, wl):
-    # short reads are seeded and chained one thread per read, the others (long, or past a
-    # per-thread budget) one warp per read; forcing every read through the warp kernels
-    # must give the same records and CIGARs
+    # short reads are seeded and chained one thread per read, long ones one thread per read
+    # with state in global memory, the rest (past either kernel's bounds) one warp per
+    # read; turning the long-read kernel off, or forcing every read through the warp
+    # kernels, must give the same records and CIGARs
     g, reads, _ = request.getfixturevalue(wl)
     p = D.default_map_params()
     iid = ctx.index_build(g)
     try:
+        ctx.reset_stats()
         mixed_path = ctx.map_batch(iid, reads, p)
+        st = ctx.stats()
+        ctx.set_option("long_thread", 0)
+        no_long = ctx.map_batch(iid, reads, p)
+        ctx.set_option("long_thread", 1)
         ctx.set_option("warp_seed_only", 1)
         warp_path = ctx.map_batch(iid, reads, p)
     finally:
         ctx.set_option("warp_seed_only", 0)
+        ctx.set_option("long_thread", 1)
         ctx.index_free(iid)
-    assert np.array_equal(gpu_records(mixed_path), gpu_records(warp_path))
-    assert np.array_equal(mixed_path.records["cigar_len"], warp_path.records["cigar_len"])
-    assert np.array_equal(mixed_path.cigar, warp_path.cigar)
+    if wl == "mixed":  # long reads took the long-read thread kernel
+        assert st["long_reads"] > 0
+    for other in (no_long, warp_path):
+        assert np.array_equal(gpu_records(mixed_path), gpu_records(other))
+        assert np.array_equal(mixed_path.records["cigar_len"], other.records["cigar_len"])
+        assert np.array_equal(mixed_path.cigar, other.cigar)
 
 
 @pytest.mark.parametrize("sub_batch", [0, 3000])
