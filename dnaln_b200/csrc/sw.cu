@@ -683,6 +683,148 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_fb(const SwTask* __restrict__
   res[tk.slot] = sw_one_reg<W, TB>(tk, qbase, tbase, p, TB ? pair_base(dir, lt, rows_max, WQ) : nullptr, lt & 1);
 }
 
+// The tasks k_sw_u2 / k_sw_wide listed (an N in the target window, or outside the biased
+// 16-bit range) for bands of W = 32 * LANES + 1 columns, one alignment per LANES lanes in
+// int32: lane c holds band columns [32c, 32c + 32) (the last lane also column W - 1) and
+// computes row t - c at step t — k_sw_wide's skewed wavefront, exchanging the left lane's
+// last (H, F) and the right lane's first (H, E) by shuffles. Scores come from the 5-entry
+// profile (N scored as the reference scores it), direction codes go to the task's half of
+// the pair words, the best cell is the first strict maximum in row-major order: the same
+// results and codes as sw_one_reg, which runs one alignment per thread and, at W = 129,
+// spills its band to local memory.
+template <int LANES, bool TB>
+__global__ void __launch_bounds__(kSwThreads)
+    k_sw_fb_lanes(const SwTask* __restrict__ tasks, int base, const uint8_t* __restrict__ qbase,
+                  const uint8_t* __restrict__ tbase, SwParams p, SwResult* __restrict__ res,
+                  uint32_t* __restrict__ dir, int rows_max, const int* __restrict__ fb) {
+  constexpr int W = 32 * LANES + 1, WQ = (W + 3) / 4, CH = 32;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int c = lane % LANES;
+  const int j = (blockIdx.x * blockDim.x + threadIdx.x) / LANES;  // entry of the fallback list
+  const int nfb = fb[0];
+  if ((blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / LANES >= nfb) return;  // warp-uniform
+  const bool live = j < nfb;
+  const int lt = live ? fb[1 + j] : 0;
+  SwTask tk{};
+  if (live) tk = tasks[base + lt];
+  const int ql = live ? tk.qlen : 0;
+  const int steps = __reduce_max_sync(FULL, live ? ql + LANES - 1 : 0);
+  const uint8_t* __restrict__ q = qbase + tk.q_off;
+  uint32_t* DP = TB ? pair_base(dir, lt, rows_max, WQ) : nullptr;
+  const int half = lt & 1;
+  const int d0 = CH * c;
+  int H[CH + 2], E[CH + 2];
+  uint32_t T[CH + 1];
+#pragma unroll
+  for (int k = 0; k < CH + 2; ++k) {
+    H[k] = 0;
+    E[k] = 0;
+  }
+#pragma unroll
+  for (int k = 0; k <= CH; ++k) T[k] = live ? sel1(tcode(tbase, tk, d0 + k)) : sel1(4u);
+  int best = 0, bi = -1, bd = -1;
+  int hout = 0, fout = 0;  // this lane's last cell of its previous row
+  for (int t = 0; t < steps; ++t) {
+    const int i = t - c;
+    const bool act = live && i >= 0 && i < ql;
+    int hleft = __shfl_up_sync(FULL, hout, 1), f = __shfl_up_sync(FULL, fout, 1);
+    if (c == 0) hleft = f = 0;
+    const uint32_t qc = act ? min(static_cast<uint32_t>(q[i]), 4u) : 4u;
+    const uint32_t plo = prof_lo(p, qc), phi = p.prof_n;
+    const uint32_t t_next = act ? sel1(tcode(tbase, tk, static_cast<int64_t>(i) + 1 + d0 + CH)) : sel1(4u);
+    int hdiag = H[0], rmax = 0, rk = 0;
+    uint32_t dw = 0;
+    int h0, e0;
+    {
+      const int hup = H[1], eup = E[1];
+      const int hd = hdiag + static_cast<int>(prmt(plo, phi, T[0]));
+      const int eo = hup - p.oe, ee = eup - p.ge, fo = hleft - p.oe, fe = f - p.ge;
+      e0 = max(eo, ee);
+      f = max(fo, fe);
+      const int m1 = max(hd, e0);
+      h0 = max(max(m1, f), 0);
+      if constexpr (TB) dw = dir_code32(hd >= e0, m1 >= f, eo >= ee, fo >= fe);
+      rmax = h0;
+      hleft = h0;
+      hdiag = hup;
+    }
+    // a lane that has not reached row 0 passes row -1's values (zero)
+    int nh = __shfl_down_sync(FULL, i >= 0 ? h0 : 0, 1);
+    int ne = __shfl_down_sync(FULL, i >= 0 ? e0 : 0, 1);
+    if (c == LANES - 1) {
+      nh = H[CH];
+      ne = E[CH];
+    }
+    if (act) {
+      H[0] = h0;
+      E[0] = e0;
+    }
+#pragma unroll
+    for (int k = 1; k <= CH; ++k) {
+      if (k == CH && c != LANES - 1) break;  // the extra cell W - 1 belongs to the last lane
+      const int hup = k == CH - 1 ? nh : (k == CH ? 0 : H[k + 1]);
+      const int eup = k == CH - 1 ? ne : (k == CH ? 0 : E[k + 1]);
+      const int hd = hdiag + static_cast<int>(prmt(plo, phi, T[k]));
+      const int eo = hup - p.oe, ee = eup - p.ge, fo = hleft - p.oe, fe = f - p.ge;
+      const int e = max(eo, ee);
+      f = max(fo, fe);
+      const int m1 = max(hd, e);
+      const int h = max(max(m1, f), 0);
+      if (act) {
+        H[k] = h;
+        E[k] = e;
+      }
+      if constexpr (TB) {
+        dw = dw * 16u + dir_code32(hd >= e, m1 >= f, eo >= ee, fo >= fe);
+        if ((k & 3) == 3) {
+          if (act) reinterpret_cast<uint16_t*>(DP + (static_cast<size_t>(i) * WQ + ((d0 + k) >> 2)) * 32)[half] =
+              static_cast<uint16_t>(dw);
+          dw = 0;
+        } else if (k == CH) {  // cell W - 1 opens the last, partial word
+          dw <<= 12;
+          if (act) reinterpret_cast<uint16_t*>(DP + (static_cast<size_t>(i) * WQ + ((d0 + k) >> 2)) * 32)[half] =
+              static_cast<uint16_t>(dw);
+        }
+        if (h > rmax) {  // first strict maximum of the lane's part of the row
+          rmax = h;
+          rk = k;
+        }
+      } else {
+        rmax = max(rmax, h);
+      }
+      hleft = h;
+      hdiag = hup;
+    }
+    hout = hleft;
+    fout = f;
+    if (act) {
+      if (rmax > best) {
+        best = rmax;
+        bi = i;
+        bd = d0 + rk;
+      }
+#pragma unroll
+      for (int k = 0; k < CH; ++k) T[k] = T[k + 1];
+      T[CH] = t_next;
+    }
+  }
+  // the lanes of the alignment: larger value, then earlier row, then smaller column
+  uint64_t key = static_cast<uint64_t>(best) << 40 |
+                 static_cast<uint64_t>(0xFFFFFu - static_cast<uint32_t>(bi + 1)) << 12 |
+                 (0xFFFu - static_cast<uint32_t>(bd < 0 ? 0xFFF : bd));
+#pragma unroll
+  for (int o = 1; o < LANES; o <<= 1) {
+    const uint64_t x = __shfl_xor_sync(FULL, key, o);
+    key = x > key ? x : key;
+  }
+  if (c != 0 || !live) return;
+  const int kb = static_cast<int>(key >> 40);
+  const int kbi = static_cast<int>(0xFFFFFu - static_cast<uint32_t>((key >> 12) & 0xFFFFFu)) - 1;
+  const int kbd = static_cast<int>(0xFFFu - static_cast<uint32_t>(key & 0xFFFu));
+  res[tk.slot] = TB ? stash(kb, kbi, kbd) : stash(kb, 0, 0);
+}
+
 // Traceback of every task of the launch from the stashed best cell (one task per thread;
 // the DP kernels are done with the scratch, so this runs at full occupancy).
 template <int W>
@@ -786,6 +928,10 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
   const int pairs = (count + 1) / 2;
   const int blocks_pairs = (pairs + kSwThreads - 1) / kSwThreads;
   const int blocks_tasks = (count + kSwThreads - 1) / kSwThreads;
+  // W = 65: the fallback list runs two lanes per alignment (k_sw_fb_lanes<2>); narrower
+  // bands keep the one-thread kernel, whose band fits in registers
+  constexpr bool kLanesFb = W == 65;
+  const int blocks_fb = static_cast<int>((static_cast<int64_t>(count) * 2 + kSwThreads - 1) / kSwThreads);
   const KernelTrace none;
   const KernelTrace& t = kt ? *kt : none;
   cudaMemsetAsync(fb, 0, sizeof(int), st);
@@ -804,7 +950,10 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
                                                                   rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<tb>");
-    k_sw_fb<W, true><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    if constexpr (kLanesFb)
+      k_sw_fb_lanes<2, true><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    else
+      k_sw_fb<W, true><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_walk");
     k_sw_walk<W><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, count, n, n_dev, qbase, tbase, p, res, dir,
@@ -816,7 +965,10 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
                                                            fb);
     t.end(st);
     t.begin(st, "k_sw_fb<score>");
-    k_sw_fb<W, false><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    if constexpr (kLanesFb)
+      k_sw_fb_lanes<2, false><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    else
+      k_sw_fb<W, false><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     t.end(st);
   }
 }
@@ -829,6 +981,8 @@ void launch_wide(cudaStream_t st, bool tb, const SwTask* tasks, int base, int co
   const int pairs = (count + 1) / 2;
   const int blocks_pairs = static_cast<int>((static_cast<int64_t>(pairs) * LANES + kSwThreads - 1) / kSwThreads);
   const int blocks_tasks = (count + kSwThreads - 1) / kSwThreads;
+  // the fallback list holds at most `count` tasks (its length is known on the device only)
+  const int blocks_fb = static_cast<int>((static_cast<int64_t>(count) * LANES + kSwThreads - 1) / kSwThreads);
   const KernelTrace none;
   const KernelTrace& t = kt ? *kt : none;
   cudaMemsetAsync(fb, 0, sizeof(int), st);
@@ -839,7 +993,7 @@ void launch_wide(cudaStream_t st, bool tb, const SwTask* tasks, int base, int co
                                                                         dir, rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<tb>");
-    k_sw_fb<W, true><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    k_sw_fb_lanes<LANES, true><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_walk");
     k_sw_walk<W><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, count, n, n_dev, qbase, tbase, p, res, dir,
@@ -851,7 +1005,8 @@ void launch_wide(cudaStream_t st, bool tb, const SwTask* tasks, int base, int co
                                                                  rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<score>");
-    k_sw_fb<W, false><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    k_sw_fb_lanes<LANES, false><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max,
+                                                                  fb);
     t.end(st);
   }
 }
