@@ -377,7 +377,7 @@ def run_ours(args) -> None:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
 
-    g, reads, _ = synth.workload(args.workload, seed=args.seed + 7919 * rank, n_reads=args.n_reads)
+    g, reads, truth = synth.workload(args.workload, seed=args.seed + 7919 * rank, n_reads=args.n_reads)
     n_reads = len(reads)
     p = D.default_map_params(bw=args.bw)
     ctx = D.Context(local)
@@ -531,6 +531,14 @@ def run_ours(args) -> None:
     wall_e2e = time.perf_counter() - w0
     ms_e2e = max_over_ranks(f0.elapsed_time(f1))
     e2e_value = world * n_reads * e2e_steps / (ms_e2e / 1e3)
+    # accuracy gate on the end-to-end results (Evaluator::add against the simulator's truth)
+    acc = {"records": 0, "correct": 0, "mapq60_mapped": 0, "mapq60_wrong": 0}
+    for (a, b), h in zip(spans, host):
+        recs = h["out"].numpy().view(D.MAP_RECORD_DTYPE)[:b - a]
+        ev = D.evaluate(D.MapResult(recs, h["cig"].numpy().view(np.uint32)), truth.contig[a:b], truth.start[a:b],
+                        truth.rev[a:b])
+        for k in acc:
+            acc[k] += int(ev[k])
     h2d = sum(h["h2d"] for h in host)
     d2h = sum(40 * h["n"] for h in host) + 4 * sum(e2e_used.values())
 
@@ -583,6 +591,8 @@ def run_ours(args) -> None:
            "sw_gcups": cells / (sw_ms / 1e3) / 1e9 if sw_ms > 0 else None,
            "sw_cells_per_step": cells / args.steps,
            "mapped_frac": st["mapped"] / max(st["reads"], 1),
+           "accuracy": {"placed_correctly": acc["correct"] / max(acc["records"], 1), **acc,
+                        "how": "dnaln_eval_records (Evaluator::add, tol 10) on the e2e records vs the generator's truth"},
            "clocks": clk,
            "index": dict(build_s=index_build_s, where="dnaln_gpu_index_build",
                          **{k: v for k, v in ctx.index_stats(iid).items() if k in ("n_keys", "device_bytes")}),

@@ -27,7 +27,7 @@ from . import _native as N
 from ._native import (ALIGN_RESULT_DTYPE, MAP_RECORD_DTYPE, ChainParams, MapParams, ScoreParams, Stats, lib, ptr)
 
 __all__ = ["Context", "Genome", "ReadBatch", "DnalnError", "ScoreParams", "ChainParams", "MapParams",
-           "default_map_params", "sam_format", "parse_reads", "fnv1a", "lib", "MAP_RECORD_DTYPE", "ALIGN_RESULT_DTYPE",
+           "default_map_params", "sam_format", "parse_reads", "evaluate", "fnv1a", "lib", "MAP_RECORD_DTYPE", "ALIGN_RESULT_DTYPE",
            "cigar_to_string"]
 
 CIGAR_OPS = "MIDNSHP=X"
@@ -432,6 +432,25 @@ def parse_reads(text: bytes, threads: int = 0) -> ReadBatch:
         return rb
     finally:
         lib().dnaln_reads_free(h)
+
+
+def evaluate(res: MapResult, truth_contig, truth_start, truth_rev, tol: int = 10) -> dict:
+    """Evaluator::add over a batch (src/evaluate.cpp:57-84): placed-correctly counts and the
+    per-MAPQ mapped / wrong tallies."""
+    tc = np.ascontiguousarray(truth_contig, np.int32)
+    ts = np.ascontiguousarray(truth_start, np.int64)
+    tr = np.ascontiguousarray(truth_rev, np.uint8)
+    out = N.EvalCounts()
+    rec = np.ascontiguousarray(res.records)
+    cig = np.ascontiguousarray(res.cigar, np.uint32) if len(res.cigar) else np.zeros(1, np.uint32)
+    rc = lib().dnaln_eval_records(ptr(rec), ptr(cig), ptr(tc), ptr(ts), ptr(tr), len(rec), tol, C.byref(out))
+    if rc != N.OK:
+        raise DnalnError(rc, "evaluation failed")
+    mq = np.array(out.mapped_at_mapq, np.uint64)
+    wq = np.array(out.wrong_at_mapq, np.uint64)
+    return {"records": out.records, "mapped": out.mapped, "correct": out.correct,
+            "placed_correctly": out.correct / max(out.records, 1),
+            "mapq60_mapped": int(mq[60]), "mapq60_wrong": int(wq[60]), "mapped_at_mapq": mq, "wrong_at_mapq": wq}
 
 
 def sam_format(reads: ReadBatch, res: MapResult, genome: Genome, threads: int = 1) -> bytes:

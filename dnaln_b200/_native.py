@@ -72,6 +72,11 @@ class ServeStats(C.Structure):
                [(n, C.c_double) for n in ("ms_form", "ms_gather", "ms_device", "ms_scatter", "ms_complete")]
 
 
+class EvalCounts(C.Structure):
+    _fields_ = [("records", C.c_uint64), ("mapped", C.c_uint64), ("correct", C.c_uint64),
+                ("mapped_at_mapq", C.c_uint64 * 61), ("wrong_at_mapq", C.c_uint64 * 61)]
+
+
 class SynthGenomeSpec(C.Structure):
     _fields_ = [("n_contigs", C.c_int32), ("contig_len", C.c_uint32), ("gc", C.c_double),
                 ("n_repeat_units", C.c_int32), ("repeat_unit_len", C.c_int32), ("repeat_frac", C.c_double),
@@ -146,6 +151,7 @@ SIGNATURES = {
     "dnaln_parse_reads": (C.c_int, [P, i64, i32, C.POINTER(P), P, i64]),
     "dnaln_reads_view": (C.c_int, [P, C.POINTER(i64)] + [C.POINTER(P)] * 8),
     "dnaln_reads_free": (None, [P]),
+    "dnaln_eval_records": (C.c_int, [P, P, P, P, P, i64, i32, C.POINTER(EvalCounts)]),
     "dnaln_synth_genome": (C.c_int, [u64, C.POINTER(SynthGenomeSpec), P]),
     "dnaln_synth_reads_bytes": (i64, [u64, C.POINTER(SynthReadsSpec)]),
     "dnaln_synth_reads": (C.c_int, [u64, P, P, P, i32, C.POINTER(SynthReadsSpec), P, i64, P, P, i64, P, P, P, P]),

@@ -23,7 +23,7 @@ LIB = PKG / "libdnaln_b200.so"
 CUDA_SOURCES = ["csrc/sw.cu", "csrc/seed.cu", "csrc/seed_thread.cu", "csrc/map.cu", "csrc/capi.cu", "csrc/noalloc.cu",
                 "csrc/serve.cu", "csrc/index_build.cu",
                 "csrc/seed_long.cu"]
-HOST_SOURCES = ["host/sam.cpp", "host/synth.cpp", "host/reads.cpp"]
+HOST_SOURCES = ["host/sam.cpp", "host/synth.cpp", "host/reads.cpp", "host/eval.cpp"]
 HEADERS = ["csrc/common.cuh", "csrc/sw.cuh", "csrc/seed.cuh", "csrc/map.cuh", "csrc/index_build.cuh"]
 PUBLIC_HEADERS = ["dnaln_b200.h", "dnaln_synth.h"]
 

@@ -329,6 +329,19 @@ int dnaln_reads_view(const dnaln_reads* r, int64_t* n, const char** seq, const i
                      const int64_t** qual_off, const uint32_t** name_hash);
 void dnaln_reads_free(dnaln_reads* r);
 
+/* The accuracy gate, Evaluator::add (src/evaluate.cpp:57-84) over n records against the
+ * simulator's truth (contig index, 0-based start, strand): a mapped record is placed
+ * correctly when contig and strand match and its unclipped start (pos minus a leading
+ * S/H clip) is within tol of the true start (the reference's default tol is 10); mapped
+ * and wrong records are also counted per MAPQ, clamped to [0, 60]. */
+typedef struct {
+  uint64_t records, mapped, correct;
+  uint64_t mapped_at_mapq[61], wrong_at_mapq[61];
+} dnaln_eval_counts;
+int dnaln_eval_records(const dnaln_map_record* rec, const uint32_t* cigar, const int32_t* truth_contig,
+                       const int64_t* truth_start, const uint8_t* truth_rev, int64_t n, int32_t tol,
+                       dnaln_eval_counts* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -226,9 +226,24 @@ class Reference:
                               C.POINTER(i64)]
         L.ref_fnv1a.restype = u32
         L.ref_fnv1a.argtypes = [P, i64]
+        L.ref_eval.restype = None
+        L.ref_eval.argtypes = [P, P, P, P, P, P, i64, C.c_int, P]
         L.ref_read_records.restype = C.c_int
         L.ref_read_records.argtypes = [C.c_char_p, P, P, P, P, P, P, P]
         self.L = L
+
+    def evaluate(self, rec, cig, co, truth_contig, truth_start, truth_rev, tol: int = 10) -> np.ndarray:
+        """Evaluator::add over records (n x 7 as map returns them): [records, mapped, correct,
+        mapped_at(0..60), wrong_at(0..60)] (cumulative over MAPQ >= q)."""
+        out = np.zeros(3 + 2 * 61, np.uint64)
+        rec = np.ascontiguousarray(rec, np.int64)
+        cig = np.ascontiguousarray(cig, np.uint32) if len(cig) else np.zeros(1, np.uint32)
+        tc = np.ascontiguousarray(truth_contig, np.int32)
+        ts = np.ascontiguousarray(truth_start, np.int64)
+        tr = np.ascontiguousarray(truth_rev, np.uint8)
+        self.L.ref_eval(_p(rec), _p(cig), _p(np.ascontiguousarray(co, np.int64)), _p(tc), _p(ts), _p(tr), len(rec),
+                        tol, _p(out))
+        return out
 
     def read_records(self, path: str):
         """read_all_records of a FASTA/FASTQ file: (seq, seq_off, names, name_off, qual, qual_off)."""

@@ -11,6 +11,7 @@
 //   ref_align         -> dnaln::ScalarAligner / SimdAligner (src/align.hpp:70-104)
 //   ref_map           -> dnaln::Mapper::map + append_sam    (src/mapper.hpp:51-58)
 //   ref_read_records  -> dnaln::read_all_records            (src/seqio.hpp:47)
+//   ref_eval          -> dnaln::Evaluator::add              (src/evaluate.hpp:29-31)
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -22,6 +23,7 @@
 #include "align.hpp"
 #include "chain.hpp"
 #include "common.hpp"
+#include "evaluate.hpp"
 #include "index.hpp"
 #include "mapper.hpp"
 #include "minimizer.hpp"
@@ -302,6 +304,38 @@ int ref_read_records(const char* path, int64_t* sizes4, char* seq, int64_t* seq_
   sizes4[2] = nb;
   sizes4[3] = qb;
   return 0;
+}
+
+// Evaluator::add over n records (read i named "r<i>", contig names "c<index>"): rec
+// columns as ref_map writes them (contig, pos, rev, mapq, ...), CIGAR of record i at
+// cigar[cig_off[i], cig_off[i+1]). out = {records, mapped, correct, mapped_at(q) for q =
+// 0..60, wrong_at(q) for q = 0..60} (cumulative over MAPQ >= q, as the reference reports).
+void ref_eval(const int64_t* rec, const uint32_t* cigar, const int64_t* cig_off, const int32_t* t_contig,
+              const int64_t* t_start, const uint8_t* t_rev, int64_t n, int tol, uint64_t* out) {
+  TruthMap truth;
+  for (int64_t i = 0; i < n; ++i) {
+    TruthRec t;
+    t.contig = "c" + std::to_string(t_contig[i]);
+    t.start = t_start[i];
+    t.end = t_start[i];
+    t.rev = t_rev[i] != 0;
+    truth.emplace("r" + std::to_string(i), std::move(t));
+  }
+  Evaluator ev(truth, tol);
+  std::vector<uint32_t> cg;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t* x = rec + 7 * i;
+    cg.assign(cigar + cig_off[i], cigar + cig_off[i + 1]);
+    ev.add("r" + std::to_string(i), x[0] >= 0, x[0] >= 0 ? "c" + std::to_string(x[0]) : "*", x[1], x[2] != 0,
+           static_cast<int>(x[3]), cg);
+  }
+  out[0] = ev.records();
+  out[1] = ev.mapped();
+  out[2] = ev.correct();
+  for (int q = 0; q <= 60; ++q) {
+    out[3 + q] = ev.mapped_at(q);
+    out[64 + q] = ev.wrong_at(q);
+  }
 }
 
 // fnv1a of the reference (src/common.hpp:136-140), for tie-break checks.

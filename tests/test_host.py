@@ -121,3 +121,20 @@ def test_default_params_are_the_references():
     assert (p.sc.match, p.sc.mismatch, p.sc.gap_open, p.sc.gap_ext, p.sc.ambig, p.sc.bw) == (2, 4, 4, 2, 1, 16)
     assert (p.ch.max_gap, p.ch.band, p.ch.lookback, p.ch.min_score, p.ch.min_anchors) == (5000, 16, 50, 20, 2)
     assert p.pri_ratio == 0.5
+
+
+def test_eval_records_matches_reference_evaluator(ref):
+    # Evaluator::add (src/evaluate.cpp:57-84) on the reference mapper's own records of a
+    # workload with repeats (multi-candidate reads, MAPQ < 60, some misplaced)
+    g, reads, truth = synth.workload("repeat-2Mbp-20k-150bp", seed=9)
+    p = D.default_map_params()
+    rec, cig, co = ref.map(ref.genome(g), reads, p, nthreads=4)
+    res = records_from_oracle(rec, cig, co)
+    for tol in (10, 0, 1000):
+        ours = D.evaluate(res, truth.contig, truth.start, truth.rev, tol)
+        exp = ref.evaluate(rec, cig, co, truth.contig, truth.start, truth.rev, tol)
+        assert (ours["records"], ours["mapped"], ours["correct"]) == tuple(int(x) for x in exp[:3])
+        cum_m = np.cumsum(ours["mapped_at_mapq"][::-1])[::-1]
+        cum_w = np.cumsum(ours["wrong_at_mapq"][::-1])[::-1]
+        assert np.array_equal(cum_m, exp[3:64]) and np.array_equal(cum_w, exp[64:125])
+    assert 0.9 < D.evaluate(res, truth.contig, truth.start, truth.rev)["placed_correctly"] <= 1.0
