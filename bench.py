@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--n-reads", type=int, default=None, help="override the workload's read count (testing)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-e2e", action="store_true",
+                    help="also time the step through the request server (each batch one request)")
     ap.add_argument("--workload", default=WORKLOAD,
                     help="synthetic workload (dnaln_b200.synth.WORKLOADS); the default is the headline one")
     ap.add_argument("--bw", type=int, default=16, help="SW band half-width (16, or 64 for the mixed-length workload)")
@@ -531,6 +533,23 @@ def run_ours(args) -> None:
     wall_e2e = time.perf_counter() - w0
     ms_e2e = max_over_ranks(f0.elapsed_time(f1))
     e2e_value = world * n_reads * e2e_steps / (ms_e2e / 1e3)
+    # ---- the same step through the request server (dnaln_serve_*): each batch a request,
+    # three lanes whose batches overlap on the device ------------------------------------
+    e2e_serve = None
+    if world == 1 and args.serve_e2e:
+        from dnaln_b200.serve import Server
+        with Server(ctx, lanes=3, max_batch_reads=BATCH) as srv:
+            for _ in range(2):
+                [srv.wait(r) for r in [srv.submit(iid, part, p) for part in parts]]
+            barrier()
+            s0 = time.perf_counter()
+            for _ in range(e2e_steps):
+                [srv.wait(r) for r in [srv.submit(iid, part, p) for part in parts]]
+            barrier()
+            ws = time.perf_counter() - s0
+        e2e_serve = {"value": n_reads * e2e_steps / ws, "unit": METRIC, "ms_per_step": 1e3 * ws / e2e_steps,
+                     "what": "dnaln_serve_submit / wait, each batch of the step one request, 3 lanes; wall clock"}
+
     # accuracy gate on the end-to-end results (Evaluator::add against the simulator's truth)
     acc = {"records": 0, "correct": 0, "mapq60_mapped": 0, "mapq60_wrong": 0}
     for (a, b), h in zip(spans, host):
@@ -578,6 +597,7 @@ def run_ours(args) -> None:
            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                    "ms_per_step": ms_e2e / e2e_steps, "wall_s": wall_e2e},
            "gpu_launches": int(st["launches"]),
+           "e2e_server": e2e_serve,
            "plain": {"value": plain_value, "ms_per_step": ms_plain / args.steps,
                      "what": "same step, every read through the warp-per-read kernels, SW tasks in read order"},
            "batched_vs_plain": value / plain_value,
