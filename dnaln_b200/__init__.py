@@ -244,6 +244,14 @@ class Context:
         """Tuning switch (sub_batch, warp_seed_only, dir_cap_bytes); results do not change."""
         self._check(self._lib.dnaln_gpu_set_option(self._h, name.encode(), int(value)))
 
+    def sw_tuning(self) -> list[dict]:
+        """The SW kernel forms chosen so far (dnaln_gpu_sw_tuning)."""
+        n = C.c_int32()
+        self._check(self._lib.dnaln_gpu_sw_tuning(self._h, None, 0, C.byref(n)))
+        arr = (N.SwTuning * max(n.value, 1))()
+        self._check(self._lib.dnaln_gpu_sw_tuning(self._h, arr, n.value, C.byref(n)))
+        return [{f: getattr(arr[i], f) for f, _ in N.SwTuning._fields_} for i in range(n.value)]
+
     def set_sub_batch(self, reads: int) -> None:
         """Reads per pipelined sub-batch of map_batch (0 = the whole batch at once)."""
         self._check(self._lib.dnaln_gpu_set_sub_batch(self._h, int(reads)))

@@ -59,6 +59,11 @@ class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 48), ("launches", C.c_int64), ("ms", C.c_double)]
 
 
+class SwTuning(C.Structure):
+    _fields_ = [("W", C.c_int32), ("traceback", C.c_int32), ("len_bucket", C.c_int32), ("form", C.c_int32),
+                ("ms_inter", C.c_double), ("ms_intra", C.c_double), ("tasks", C.c_int64)]
+
+
 class ServeParams(C.Structure):
     _fields_ = [("lanes", C.c_int32), ("coalesce", C.c_int32), ("max_batch_reads", C.c_int64),
                 ("hbm_budget_bytes", C.c_int64)]
@@ -116,6 +121,7 @@ SIGNATURES = {
     "dnaln_gpu_kernel_times": (C.c_int, [P, C.POINTER(KernelTime), i32, C.POINTER(i32)]),
     "dnaln_gpu_set_sub_batch": (C.c_int, [P, i64]),
     "dnaln_gpu_set_option": (C.c_int, [P, C.c_char_p, i64]),
+    "dnaln_gpu_sw_tuning": (C.c_int, [P, C.POINTER(SwTuning), i32, C.POINTER(i32)]),
     "dnaln_gpu_map_submit": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64, C.POINTER(i64),
                              C.POINTER(i64)]),
     "dnaln_gpu_map_wait": (C.c_int, [P, i64]),

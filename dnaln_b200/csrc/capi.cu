@@ -141,6 +141,12 @@ struct dnaln_ctx {
   bool warp_seed_only = false;  // option: every read through the warp-per-read seeding kernels
   bool length_order = true;     // option: SW tasks of mixed-length batches run longest first
   bool long_thread = true;      // option: listed long reads one thread each before the warp kernels
+  // SW kernel form per (band width, traceback, read-length bucket): option "sw_form" 0 =
+  // tuned on the first batch that needs it, 1 = inter-sequence, 2 = intra-sequence
+  int sw_mode = 0;
+  std::map<int, dnaln_sw_tuning> sw_tune;
+  cudaEvent_t tune_ev[3] = {};
+  int* h_tune = nullptr;  // pinned read-back of a device task count
   // kernel trace: event pairs of the current batch, totals per kernel name
   bool trace_on = false, trace_open = false;
   std::string trace_only;  // non-empty: trace only the kernel of this name
@@ -412,12 +418,59 @@ int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks,
   int* fb = dbuf<int>(c, "sw_fb", static_cast<size_t>(chunk) + 1);
   if (!fb) return DNALN_ERR_OOM;
   const KernelTrace kt = tracer(c);
+  // the kernel form: fixed by the option, or tuned once per (W, traceback, length bucket)
+  // by timing both forms on the first chunk (they give identical results, so the second
+  // run only rewrites the same outputs)
+  SwForm form = kSwInter;
+  bool tune = false;
+  const int bucket = rows_max <= 256 ? 0 : (rows_max <= 1024 ? 1 : 2);
+  const int key = sp.W | (tb ? 1 : 0) << 10 | bucket << 11;
+  if (sw_has_both_forms(sp.W, bytes_ok)) {
+    if (c->sw_mode == 1) {
+      form = kSwInter;
+    } else if (c->sw_mode == 2) {
+      form = kSwIntra;
+    } else {
+      auto it = c->sw_tune.find(key);
+      if (it != c->sw_tune.end()) form = it->second.form ? kSwIntra : kSwInter;
+      else tune = true;
+    }
+  }
   for (int64_t b = 0; b < n_max; b += chunk) {
     const int cnt = static_cast<int>(n_max - b < chunk ? n_max - b : chunk);
-    if (!launch_sw(c->st, tb, bytes_ok, tasks, static_cast<int>(b), cnt, n_max, n_dev, qbase, tbase, sp, res, dir,
-                   rows_max, cig, cig_off, band, fb, c->d_err, &kt))
-      return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
-    c->stats.launches += static_cast<uint64_t>(sw_launches(sp.W, bytes_ok, tb));
+    const auto run = [&](SwForm f) {
+      const bool ok = launch_sw(c->st, tb, bytes_ok, tasks, static_cast<int>(b), cnt, n_max, n_dev, qbase, tbase, sp,
+                                res, dir, rows_max, cig, cig_off, band, fb, c->d_err, &kt, f);
+      c->stats.launches += static_cast<uint64_t>(sw_launches(sp.W, bytes_ok, tb));
+      return ok;
+    };
+    if (b == 0 && tune) {
+      CK(cudaEventRecord(c->tune_ev[0], c->st));
+      if (!run(kSwInter)) return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
+      CK(cudaEventRecord(c->tune_ev[1], c->st));
+      if (!run(kSwIntra)) return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
+      CK(cudaEventRecord(c->tune_ev[2], c->st));
+      int64_t live = cnt;
+      if (n_dev) {
+        CK(cudaMemcpyAsync(c->h_tune, n_dev, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        live = std::min<int64_t>(cnt, *c->h_tune);
+      } else {
+        CK(cudaEventSynchronize(c->tune_ev[2]));
+      }
+      dnaln_sw_tuning t{};
+      t.W = sp.W;
+      t.traceback = tb ? 1 : 0;
+      t.len_bucket = bucket;
+      t.ms_inter = ev_ms(c->tune_ev[0], c->tune_ev[1]);
+      t.ms_intra = ev_ms(c->tune_ev[1], c->tune_ev[2]);
+      t.form = t.ms_intra < t.ms_inter ? 1 : 0;
+      t.tasks = live;
+      form = t.form ? kSwIntra : kSwInter;
+      c->sw_tune[key] = t;
+      continue;
+    }
+    if (!run(form)) return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
   }
   CK(cudaGetLastError());
   return DNALN_OK;
@@ -964,6 +1017,8 @@ int dnaln_gpu_ctx_create(int device, dnaln_ctx** out) {
   bad(cudaMalloc(&c->d_err, sizeof(uint32_t)));
   bad(cudaMalloc(&c->d_count, 4 * sizeof(int)));
   bad(cudaHostAlloc(&c->h_info, 8 * sizeof(int64_t), cudaHostAllocDefault));
+  bad(cudaHostAlloc(&c->h_tune, sizeof(int), cudaHostAllocDefault));
+  for (auto& x : c->tune_ev) bad(cudaEventCreate(&x));
   if (e != DNALN_OK) {
     dnaln_gpu_ctx_destroy(c);
     return e;
@@ -1002,6 +1057,9 @@ int dnaln_gpu_ctx_destroy(dnaln_ctx* c) {
   if (c->d_err) cudaFree(c->d_err);
   if (c->d_count) cudaFree(c->d_count);
   if (c->h_info) cudaFreeHost(c->h_info);
+  if (c->h_tune) cudaFreeHost(c->h_tune);
+  for (auto& x : c->tune_ev)
+    if (x) cudaEventDestroy(x);
   if (c->h_lut) cudaFreeHost(c->h_lut);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
@@ -1093,6 +1151,11 @@ int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
     c->warp_seed_only = value != 0;
     return DNALN_OK;
   }
+  if (k == "sw_form") {
+    if (value < 0 || value > 2) return fail(c, DNALN_ERR_INVALID_ARG, "sw_form must be 0 (tuned), 1 or 2");
+    c->sw_mode = static_cast<int>(value);
+    return DNALN_OK;
+  }
   if (k == "long_thread") {
     c->long_thread = value != 0;
     return DNALN_OK;
@@ -1107,6 +1170,18 @@ int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
     return DNALN_OK;
   }
   return fail(c, DNALN_ERR_INVALID_ARG, "unknown option '%s'", name);
+}
+
+int dnaln_gpu_sw_tuning(const dnaln_ctx* cc, dnaln_sw_tuning* out, int32_t cap, int32_t* n_out) {
+  if (!cc || !n_out) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(cc->mu);
+  int32_t i = 0;
+  for (const auto& kv : cc->sw_tune) {
+    if (out && i < cap) out[i] = kv.second;
+    ++i;
+  }
+  *n_out = i;
+  return DNALN_OK;
 }
 
 int dnaln_gpu_host_alloc(dnaln_ctx* c, size_t bytes, void** out) {

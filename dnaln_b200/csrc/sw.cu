@@ -1045,13 +1045,24 @@ size_t sw_band_bytes_per_task(int W, bool bytes_ok) {
 
 int sw_launches(int W, bool bytes_ok, bool tb) { return sw_uses_generic(W, bytes_ok) ? 1 : (tb ? 3 : 2); }
 
+bool sw_has_both_forms(int W, bool bytes_ok) { return !sw_uses_generic(W, bytes_ok) && (W == 33 || W == 65); }
+
 bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int base, int count, int n,
                const int* n_dev, const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res,
                uint32_t* dir, int rows_max, uint32_t* cig, const int64_t* cig_off, int* band, int* fb,
-               uint32_t* err, const KernelTrace* kt) {
+               uint32_t* err, const KernelTrace* kt, SwForm form) {
   if (count <= 0) return true;
   const bool generic = sw_uses_generic(p.W, bytes_ok);
   if ((tb && !dir) || (generic && !band) || (!generic && !fb) || (base % kSwTaskGroup) != 0) return false;
+  if (!generic && form == kSwIntra && sw_has_both_forms(p.W, bytes_ok)) {
+    if (p.W == 33)
+      launch_wide<1>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, fb, err,
+                     kt);
+    else
+      launch_wide<2>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, fb, err,
+                     kt);
+    return true;
+  }
   if (!generic) {
 #define DNB_SW_U2(WV)                                                                                       \
   case WV:                                                                                                  \

@@ -24,6 +24,13 @@ size_t sw_band_bytes_per_task(int W, bool bytes_ok);
 // Kernels one launch_sw call issues (for launch accounting).
 int sw_launches(int W, bool bytes_ok, bool tb);
 
+// Two kernel forms compute the same register-resident bands: inter-sequence (k_sw_u2, a
+// thread holds the whole band row of two alignments) and intra-sequence (k_sw_wide, the
+// row of a pair spread over (W - 1) / 32 lanes in a skewed wavefront). W = 33 and 65 have
+// both; W = 129 only the intra form; the others only the inter form.
+enum SwForm : int { kSwInter = 0, kSwIntra = 1 };
+bool sw_has_both_forms(int W, bool bytes_ok);
+
 // Aligns tasks[base, base + count) that are below the task count min(n, *n_dev) (n_dev
 // may be null; it lets a device-side producer size the batch without a host sync).
 // Results go to res[task.slot]; with tb, CIGAR ops (walk order) to cig +
@@ -36,6 +43,6 @@ int sw_launches(int W, bool bytes_ok, bool tb);
 bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int base, int count, int n,
                const int* n_dev, const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res,
                uint32_t* dir, int rows_max, uint32_t* cig, const int64_t* cig_off, int* band, int* fb,
-               uint32_t* err, const KernelTrace* kt);
+               uint32_t* err, const KernelTrace* kt, SwForm form = kSwInter);
 
 }  // namespace dnb

@@ -129,12 +129,27 @@ int dnaln_gpu_set_sub_batch(dnaln_ctx* ctx, int64_t reads);
  *   "sub_batch"      same as dnaln_gpu_set_sub_batch;
  *   "warp_seed_only" 1 = seed and chain every read one warp per read (default 0: short
  *                    reads one thread per read, the others one warp per read);
+ *   "sw_form"        banded SW kernel form where a band width has two (W = 33, 65): 0 =
+ *                    tuned per context (default), 1 = inter-sequence, 2 = intra-sequence;
  *   "long_thread"    1 = reads the short thread kernel lists go one thread each through
  *                    the long-read kernel first (default); 0 = straight to the warp kernels;
  *   "length_order"   1 = SW tasks of a batch whose reads differ in length run longest
  *                    first (default); 0 = in read order;
  *   "dir_cap_bytes"  traceback direction-code scratch per launch (default 1 GiB). */
 int dnaln_gpu_set_option(dnaln_ctx* ctx, const char* name, int64_t value);
+/* The SW kernel-form tuner (no reference counterpart): band widths with two register-
+ * resident kernel forms (W = 33, 65) — inter-sequence, a thread holding the band rows of
+ * two alignments, and intra-sequence, a pair's row spread over (W - 1) / 32 lanes — are
+ * timed against each other on the first batch of each (band width, traceback or score-
+ * only, read-length bucket <= 256 / <= 1024 / longer) a context maps, and the faster form
+ * runs from then on (`tasks` says how large the timed sample was). Both give identical
+ * results. Writes min(cap, count) entries; *n_out = count. */
+typedef struct {
+  int32_t W, traceback, len_bucket, form; /* form: 0 inter-sequence, 1 intra-sequence */
+  double ms_inter, ms_intra;              /* the timed first chunk */
+  int64_t tasks;
+} dnaln_sw_tuning;
+int dnaln_gpu_sw_tuning(const dnaln_ctx* ctx, dnaln_sw_tuning* out, int32_t cap, int32_t* n_out);
 /* Page-locked host buffers for fast transfers (pass to the *_batch calls). */
 int dnaln_gpu_host_alloc(dnaln_ctx* ctx, size_t bytes, void** out);
 int dnaln_gpu_host_free(dnaln_ctx* ctx, void* p);

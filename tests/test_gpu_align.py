@@ -135,3 +135,22 @@ def test_traceback_consistency(ctx):
             assert s == r["score"]
             assert qspan == r["qe"] - r["qb"] and tspan == r["te"] - r["tb"]
             assert int(cig[0]) & 0xF == 0 and int(cig[-1]) & 0xF == 0
+
+
+@pytest.mark.parametrize("bw", [16, 32])
+def test_sw_forms_identical_and_tuned(ctx, port, bw):
+    # W = 33 and 65 have an inter-sequence and an intra-sequence kernel; both must give the
+    # oracle's results, and the tuner (sw_form 0) times them on the first batch
+    rng = np.random.default_rng(100 + bw)
+    qs, ts = random_tasks(rng, 9000, bw, max_len=300)
+    sc = (2, 4, 4, 2, 1, bw)
+    try:
+        for tb in (False, True):
+            exp = port.align(qs, ts, tb, sc)
+            for form in (1, 2, 0):
+                ctx.set_option("sw_form", form)
+                check_same(ctx.align(qs, ts, tb, D.ScoreParams(*sc)), exp, tb)
+    finally:
+        ctx.set_option("sw_form", 0)
+    tuned = [t for t in ctx.sw_tuning() if t["W"] == 2 * bw + 1]
+    assert tuned and all(t["form"] in (0, 1) and t["ms_inter"] > 0 and t["ms_intra"] > 0 for t in tuned)

@@ -88,6 +88,25 @@ def test_mixed_lengths_parity(ctx, ref, mixed, bw):
         ctx.index_free(iid)
 
 
+@pytest.mark.parametrize("bw", [16, 32])
+def test_sw_forms_give_the_same_records(ctx, repeat, bw):
+    # the inter- and intra-sequence SW kernels (and whichever the tuner picks) map alike
+    g, reads, _ = repeat
+    p = D.default_map_params(bw=bw)
+    iid = ctx.index_build(g)
+    try:
+        got = []
+        for form in (1, 2, 0):
+            ctx.set_option("sw_form", form)
+            got.append(ctx.map_batch(iid, reads, p))
+    finally:
+        ctx.set_option("sw_form", 0)
+        ctx.index_free(iid)
+    for other in got[1:]:
+        assert np.array_equal(gpu_records(got[0]), gpu_records(other))
+        assert np.array_equal(got[0].cigar, other.cigar)
+
+
 def test_port_agrees_with_gpu_on_parameter_variants(ctx, port, repeat):
     g, reads, _ = repeat
     sub = reads.slice(0, 3000)
