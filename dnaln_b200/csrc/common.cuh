@@ -19,6 +19,10 @@ enum : uint32_t {
   kErrCigarOverflow = 1u << 1,
   kErrChainScratch = 1u << 2,
   kErrProbeLoop = 1u << 3,
+  // not failures of the input: the chaining scratch pool of a batch was too small (the
+  // host grows it and maps the batch again), and the caller's CIGAR buffer was too small
+  kErrChainPool = 1u << 4,
+  kErrOutputCapacity = 1u << 5,
 };
 
 // Thomas Wang's 64-bit mix restricted to `mask` bits, step for step as the index keys are

@@ -176,13 +176,17 @@ __global__ void k_records(int64_t n, const int32_t* __restrict__ seq_len, CandBu
 __global__ void k_cigar_gather(int64_t n, const int64_t* __restrict__ pofs, const int32_t* __restrict__ seq_len,
                                const SwResult* __restrict__ res_tb, const uint32_t* __restrict__ cig_src,
                                const int64_t* __restrict__ dst_off, int64_t rec_base, dnaln_map_record* __restrict__ out,
-                               uint32_t* __restrict__ dst) {
+                               uint32_t* __restrict__ dst, int64_t cap, uint32_t* __restrict__ err) {
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= n) return;
   const int64_t o = dst_off[r], cnt = dst_off[r + 1] - o;
   out[r].cigar_off = rec_base + o;
   out[r].cigar_len = static_cast<int32_t>(cnt);
   if (cnt == 0) return;
+  if (o + cnt > cap) {  // the caller's buffer is too small: the call reports the size it needs
+    atomicOr(err, kErrOutputCapacity);
+    return;
+  }
   const SwResult a = res_tb[r];
   const uint32_t* src = cig_src + 2 * pofs[r] + r;
   int64_t x = o;
@@ -244,9 +248,10 @@ void launch_records(cudaStream_t st, int64_t n, const int32_t* seq_len, CandBuf 
 
 void launch_cigar_gather(cudaStream_t st, int64_t n, const int64_t* pofs, const int32_t* seq_len,
                          const SwResult* res_tb, const uint32_t* cig_src, const int64_t* dst_off, int64_t rec_base,
-                         dnaln_map_record* out, uint32_t* dst) {
-  if (n > 0)
-    k_cigar_gather<<<blocks_for(n), kThreads, 0, st>>>(n, pofs, seq_len, res_tb, cig_src, dst_off, rec_base, out, dst);
+                         dnaln_map_record* out, uint32_t* dst, int64_t cap, uint32_t* err) {
+  if (n <= 0) return;
+  k_cigar_gather<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(n, pofs, seq_len, res_tb, cig_src, dst_off,
+                                                                         rec_base, out, dst, cap, err);
 }
 
 void launch_align_counts(cudaStream_t st, int64_t n, const SwResult* res, int64_t* counts) {

@@ -31,11 +31,12 @@ void launch_records(cudaStream_t st, int64_t n, const int32_t* seq_len, CandBuf 
                     dnaln_map_record* out, int64_t* cig_count, unsigned long long* ctr);
 
 // Writes each mapped read's CIGAR (leading S, the walk's ops reversed, trailing S) at
-// dst + dst_off[r] and sets out[r].cigar_off = rec_base + dst_off[r] and cigar_len.
+// dst + dst_off[r] and sets out[r].cigar_off = rec_base + dst_off[r] and cigar_len; a
+// CIGAR that would end past cap ops is not written and sets kErrOutputCapacity.
 // cig_src slot of read r is 2 * pofs[r] + r.
 void launch_cigar_gather(cudaStream_t st, int64_t n, const int64_t* pofs, const int32_t* seq_len,
                          const SwResult* res_tb, const uint32_t* cig_src, const int64_t* dst_off, int64_t rec_base,
-                         dnaln_map_record* out, uint32_t* dst);
+                         dnaln_map_record* out, uint32_t* dst, int64_t cap, uint32_t* err);
 
 // GpuAligner: reversed walk ops of task i (slot i, source cig_src + src_off[i]) to
 // dst + dst_off[i]; fills out[i].

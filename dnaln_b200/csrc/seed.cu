@@ -633,13 +633,16 @@ __global__ void __launch_bounds__(kSeedWarps * 32)
 }
 
 // Pass 2 of read r by one warp.
+// Scratch of a read with more than 32 anchors (chain records, and the anchors themselves
+// past kSmCap) is taken from a pool by one atomic add; a read the pool cannot hold sets
+// kErrChainPool, and the host maps the batch again with a pool of the size asked for.
 __device__ void chain_read(int64_t r, const int64_t* __restrict__ pofs, const int32_t* __restrict__ seq_len,
-                           const int32_t* __restrict__ n_min, const int64_t* __restrict__ anchor_off, const MinBuf& mb,
+                           const int32_t* __restrict__ n_min, const int64_t* __restrict__ n_anchor, const MinBuf& mb,
                            const DevIndex& ix, const ChainParamsDev& cp, const CandParams& cand,
-                           const AnchorScratch& as, const CandBuf& cb, uint32_t* __restrict__ err, ChainSmem& smw) {
+                           const AnchorScratch& as, unsigned long long* __restrict__ pool_top, int64_t pool_cap,
+                           const CandBuf& cb, uint32_t* __restrict__ err, ChainSmem& smw) {
   const int lane = threadIdx.x & 31;
-  const int64_t a0 = anchor_off[r];
-  const int64_t na64 = anchor_off[r + 1] - a0;
+  const int64_t na64 = n_anchor[r];
   if (na64 > 0x3FFFFFFF) {
     if (lane == 0) {
       atomicOr(err, kErrChainScratch);
@@ -648,6 +651,19 @@ __device__ void chain_read(int64_t r, const int64_t* __restrict__ pofs, const in
     return;
   }
   const int na = static_cast<int>(na64);
+  int64_t a0 = 0;
+  if (na > 32) {
+    unsigned long long b = 0;
+    if (lane == 0) b = atomicAdd(pool_top, static_cast<unsigned long long>(na));
+    a0 = static_cast<int64_t>(__shfl_sync(0xffffffffu, b, 0));
+    if (a0 + na > pool_cap) {
+      if (lane == 0) {
+        atomicOr(err, kErrChainPool);
+        cb.n_cand[r] = 0;
+      }
+      return;
+    }
+  }
   const bool small = na <= kSmCap;
   ChainArrays a;
   a.keys = small ? smw.keys : as.keys + a0;
@@ -715,14 +731,17 @@ __device__ void chain_read(int64_t r, const int64_t* __restrict__ pofs, const in
 // One warp per read: reads [0, n), or with a list the reads list[0, list_n) (grid-stride).
 __global__ void __launch_bounds__(kChainWarps * 32)
     k_chain_map(const int64_t* __restrict__ pofs, const int32_t* __restrict__ seq_len, int64_t n,
-                const int32_t* __restrict__ list, const int32_t* __restrict__ n_min,
-                const int64_t* __restrict__ anchor_off, MinBuf mb, DevIndex ix, ChainParamsDev cp, CandParams cand,
-                AnchorScratch as, CandBuf cb, uint32_t* __restrict__ err) {
+                const int32_t* __restrict__ list, const int* __restrict__ list_n, const int32_t* __restrict__ n_min,
+                const int64_t* __restrict__ n_anchor, MinBuf mb, DevIndex ix, ChainParamsDev cp, CandParams cand,
+                AnchorScratch as, unsigned long long* __restrict__ pool_top, int64_t pool_cap, CandBuf cb,
+                uint32_t* __restrict__ err) {
   __shared__ ChainSmem sm[kChainWarps];
   const int wib = threadIdx.x >> 5;
   const int64_t gw = static_cast<int64_t>(blockIdx.x) * kChainWarps + wib;
-  for (int64_t x = gw; x < n; x += static_cast<int64_t>(gridDim.x) * kChainWarps)
-    chain_read(list ? list[x] : x, pofs, seq_len, n_min, anchor_off, mb, ix, cp, cand, as, cb, err, sm[wib]);
+  const int64_t m = list ? static_cast<int64_t>(*list_n) : n;
+  for (int64_t x = gw; x < m; x += static_cast<int64_t>(gridDim.x) * kChainWarps)
+    chain_read(list ? list[x] : x, pofs, seq_len, n_min, n_anchor, mb, ix, cp, cand, as, pool_top, pool_cap, cb, err,
+               sm[wib]);
 }
 
 __global__ void __launch_bounds__(kSeedWarps * 32)
@@ -802,12 +821,14 @@ void launch_seed_list(cudaStream_t st, const char* seq, const int64_t* seq_off, 
 }
 
 void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* list,
-                      const int32_t* n_min, const int64_t* anchor_off, MinBuf mb, const DevIndex& ix,
-                      const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as, CandBuf cb, uint32_t* err) {
+                      const int* list_n, const int32_t* n_min, const int64_t* n_anchor, MinBuf mb,
+                      const DevIndex& ix, const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as,
+                      unsigned long long* pool_top, int64_t pool_cap, CandBuf cb, uint32_t* err) {
   if (n <= 0) return;
-  const int64_t blocks = (n + kChainWarps - 1) / kChainWarps;
-  k_chain_map<<<static_cast<unsigned>(blocks), kChainWarps * 32, 0, st>>>(pofs, seq_len, n, list, n_min, anchor_off,
-                                                                         mb, ix, cp, cand, as, cb, err);
+  // grid-stride over a count that may be known on the device only: a few resident waves
+  const int64_t blocks = std::min<int64_t>((n + kChainWarps - 1) / kChainWarps, 148 * 16);
+  k_chain_map<<<static_cast<unsigned>(blocks), kChainWarps * 32, 0, st>>>(
+      pofs, seq_len, n, list, list_n, n_min, n_anchor, mb, ix, cp, cand, as, pool_top, pool_cap, cb, err);
 }
 
 void launch_sketch_codes(cudaStream_t st, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,

@@ -133,11 +133,14 @@ void launch_seed_list(cudaStream_t st, const char* seq, const int64_t* seq_off, 
                       const int* list_n, uint8_t* codes, const DevIndex& ix, const SeedParams& sp, MinBuf mb,
                       int32_t* n_min, int64_t* n_anchor, uint32_t* err);
 
-// Pass 2: anchors, chaining, candidates. anchor_off = exclusive prefix of n_anchor (n+1).
-// With a list, the reads list[0, n) instead of [0, n).
+// Pass 2: anchors, chaining, candidates of the reads [0, n), or with a list of the reads
+// list[0, *list_n) (n = the list's size). n_anchor[r] = the read's anchor count (pass 1);
+// reads of more than 32 anchors take their scratch (as, pool_cap entries per array) from
+// the pool by an atomic add on *pool_top; past the capacity a read sets kErrChainPool.
 void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* list,
-                      const int32_t* n_min, const int64_t* anchor_off, MinBuf mb, const DevIndex& ix,
-                      const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as, CandBuf cb, uint32_t* err);
+                      const int* list_n, const int32_t* n_min, const int64_t* n_anchor, MinBuf mb,
+                      const DevIndex& ix, const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as,
+                      unsigned long long* pool_top, int64_t pool_cap, CandBuf cb, uint32_t* err);
 
 // One thread per read (seed_thread.cu): passes 1 and 2 of the reads the per-thread budgets
 // admit, writing codes of every read, candidates of the admitted ones, n_min, n_anc_t (their
