@@ -52,7 +52,7 @@ class Stats(C.Structure):
                [(n, C.c_double) for n in ("ms_seed", "ms_chain", "ms_sw_score", "ms_sw_tb", "ms_post", "ms_h2d",
                                           "ms_d2h", "ms_total")] + \
                [(n, C.c_uint64) for n in ("launches", "warp_reads", "warp_minimizers", "warp_anchors",
-                                          "warp_bases", "long_reads")]
+                                          "warp_bases", "long_reads", "graph_launches")]
 
 
 class KernelTime(C.Structure):

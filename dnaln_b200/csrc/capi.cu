@@ -106,6 +106,21 @@ struct BatchHints {
   int64_t max_len = -1;    // longest read, -1 = read back from the device
   int64_t cigar_base = 0;  // added to every record's cigar_off
   bool retry = false;      // the batch is being mapped again with a grown chaining pool
+  bool caller_cigar = false;  // the CIGARs go to the caller's buffer (not the internal one)
+};
+
+// Host facts of an enqueued batch that its completion needs.
+struct MapRun {
+  int64_t B = 0, max_len = 0, cigar_cap = 0;
+  uint32_t* d_cigar = nullptr;
+  bool thread_path = false, long_used = false;
+  uint64_t launches = 0;  // kernels the enqueue issued (counted again at each graph replay)
+};
+
+struct CachedGraph {  // an instantiated batch graph and the buffer epoch it was captured at
+  cudaGraphExec_t exec;
+  uint64_t epoch;
+  MapRun run;
 };
 
 }  // namespace
@@ -149,6 +164,12 @@ struct dnaln_ctx {
   cudaEvent_t tune_ev[3] = {};
   int* h_tune = nullptr;  // pinned read-back of a device task count
   int64_t pool_cap = 0;   // entries of the warp-path chaining pool (grown from the batches' use)
+  // CUDA graphs of batches (run_map): cache by launch key, keys seen once, and the buffer
+  // epoch, bumped whenever a buffer a graph may reference is reallocated or rewritten
+  bool graphs = true, capturing = false;
+  std::map<std::string, CachedGraph> graph_cache;
+  std::map<std::string, uint64_t> graph_seen;
+  uint64_t epoch = 0, graph_launches = 0;
   // kernel trace: event pairs of the current batch, totals per kernel name
   bool trace_on = false, trace_open = false;
   std::string trace_only;  // non-empty: trace only the kernel of this name
@@ -189,6 +210,11 @@ T* dbuf(dnaln_ctx* c, const char* name, size_t count) {
   DevBuf& b = c->bufs[name];
   const size_t need = (count ? count : 1) * sizeof(T);
   if (b.cap < need) {
+    if (c->capturing) {  // a graph cannot hold an allocation: the caller runs the batch eagerly
+      fail(c, DNALN_ERR_CUDA, "capture stopped: buffer %s must grow", name);
+      return nullptr;
+    }
+    ++c->epoch;  // graphs captured before may reference the old buffer
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
@@ -301,6 +327,8 @@ int chain_lut_dev(dnaln_ctx* c, int k, int band, const int32_t** out) {
   const size_t n = static_cast<size_t>(band) + 1;
   DBUF(d, int32_t, "chain_lut", n);
   if (c->lut_k != k || c->lut_band != band) {
+    if (c->capturing) return fail(c, DNALN_ERR_CUDA, "capture stopped: the gap-cost table must be uploaded");
+    ++c->epoch;  // graphs captured before read the previous table
     const std::vector<int32_t> lut = chain_cost_lut(k, band);
     CK(cudaStreamSynchronize(c->st));  // the staging buffer may still feed an earlier upload
     if (c->h_lut_cap < n) {
@@ -444,6 +472,7 @@ int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks,
     } else {
       auto it = c->sw_tune.find(key);
       if (it != c->sw_tune.end()) form = it->second.form ? kSwIntra : kSwInter;
+      else if (c->capturing) return fail(c, DNALN_ERR_CUDA, "capture stopped: a kernel form is still to be tuned");
       else tune = true;
     }
   }
@@ -507,20 +536,21 @@ int validate_map_params(dnaln_ctx* c, const dnaln_map_params* p, const IndexRes&
   return DNALN_OK;
 }
 
-// The device pipeline. Inputs and d_out in device memory; CIGARs go to d_cigar
-// (capacity cigar_cap) or, when d_cigar is null, to an internal buffer returned via
-// *cigar_dev. *cigar_used = total ops.
-int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_off, const int32_t* d_seq_len,
-            const uint32_t* d_hash, int64_t n, const dnaln_map_params& p, dnaln_map_record* d_out, uint32_t* d_cigar,
-            int64_t cigar_cap, int64_t* cigar_used, uint32_t** cigar_dev, const BatchHints& hint) {
+// Enqueues the whole batch on the context's stream, ending with the copies of its totals
+// and counters into h_info. With the batch's total bases and longest read given (hints)
+// and no kernel-form tuning pending it waits for nothing, so it can be captured as a CUDA
+// graph; while capturing (c->capturing) anything that would allocate, upload or wait
+// fails it instead.
+int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_off, const int32_t* d_seq_len,
+                const uint32_t* d_hash, int64_t n, const dnaln_map_params& p, dnaln_map_record* d_out,
+                uint32_t* d_cigar, int64_t cigar_cap, const BatchHints& hint, MapRun& run) {
   cudaStream_t st = c->st;
   const KernelTrace kt = tracer(c);
   c->trace_n = 0;
   c->trace_open = false;
+  const uint64_t launches0 = c->stats.launches;  // the enqueue's own launches go to run.launches
   const int bw = p.sc.bw, W = 2 * bw + 1, MC = p.max_cand;
   const int chain_band = p.ch.band < bw ? p.ch.band : bw;  // src/mapper.cpp:9
-  *cigar_used = 0;
-  if (n == 0) return DNALN_OK;
 
   // packed offsets, total bases, longest read
   DBUF(len64, int64_t, "len64", n + 1);
@@ -540,6 +570,7 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   if (int e = exclusive_scan(c, len64, pofs, n + 1)) return e;
   int64_t B = hint.bases, max_len = hint.max_len;
   if (B < 0 || max_len < 0) {
+    if (c->capturing) return fail(c, DNALN_ERR_CUDA, "capture needs the batch's size");
     CK(cudaMemcpyAsync(c->h_info, pofs + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(c->h_info + 1, info, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -737,7 +768,6 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
     d_cigar = dbuf<uint32_t>(c, "cig_out", cigar_cap);
     if (!d_cigar) return DNALN_ERR_OOM;
   }
-  if (cigar_dev) *cigar_dev = d_cigar;
   kt.begin(st, "k_cigar_gather");
   launch_cigar_gather(st, n, pofs, d_seq_len, res_tb, cig_tb, cig_off, hint.cigar_base, d_out, d_cigar, cigar_cap,
                       c->d_err);
@@ -751,6 +781,30 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   CK(cudaMemcpyAsync(h + 3, c->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(h + 4, ctr, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(h + 7, info + 4, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  run.B = B;
+  run.max_len = max_len;
+  run.cigar_cap = cigar_cap;
+  run.d_cigar = d_cigar;
+  run.thread_path = thread_path;
+  run.long_used = warp_list != big_list;
+  run.launches = c->stats.launches - launches0;
+  c->stats.launches = launches0;
+  return DNALN_OK;
+}
+
+int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_off, const int32_t* d_seq_len,
+            const uint32_t* d_hash, int64_t n, const dnaln_map_params& p, dnaln_map_record* d_out, uint32_t* d_cigar,
+            int64_t cigar_cap, int64_t* cigar_used, uint32_t** cigar_dev, const BatchHints& hint);
+
+// Waits for an enqueued batch and turns its read-back into the call's result and the
+// context's counters; a batch that outgrew the chaining pool is mapped again.
+int map_finish(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_off, const int32_t* d_seq_len,
+               const uint32_t* d_hash, int64_t n, const dnaln_map_params& p, dnaln_map_record* d_out,
+               int64_t* cigar_used, uint32_t** cigar_dev, const BatchHints& hint, const MapRun& run) {
+  cudaStream_t st = c->st;
+  const int64_t B = run.B, max_len = run.max_len, cigar_cap = run.cigar_cap;
+  const bool thread_path = run.thread_path;
+  int64_t* h = c->h_info;
   CK(cudaStreamSynchronize(st));
   const int64_t total_ops = h[0];
   int counts[4];
@@ -771,9 +825,10 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
     again.bases = B;
     again.max_len = max_len;
     trace_collect(c);
-    return run_map(c, ix, d_seq, d_seq_off, d_seq_len, d_hash, n, p, d_out, d_cigar, cigar_cap, cigar_used, cigar_dev,
-                   again);
+    return run_map(c, ix, d_seq, d_seq_off, d_seq_len, d_hash, n, p, d_out, hint.caller_cigar ? run.d_cigar : nullptr,
+                   hint.caller_cigar ? cigar_cap : 0, cigar_used, cigar_dev, again);
   }
+  if (cigar_dev) *cigar_dev = run.d_cigar;
   if (pool_used > c->pool_cap / 2) c->pool_cap = std::max<int64_t>(c->pool_cap, pool_used + pool_used / 2);
   *cigar_used = total_ops;
   if (errbits & kErrOutputCapacity)
@@ -782,8 +837,8 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   if (int e = check_device_errors(c, errbits)) return e;
   trace_collect(c);
 
-  const int n_listed = counts[2];                               // reads the short thread kernel listed
-  const int n_warp = thread_path ? counts[warp_n == big_n ? 2 : 3] : static_cast<int>(n);  // warp kernels
+  const int n_listed = counts[2];                                        // reads the short thread kernel listed
+  const int n_warp = thread_path ? counts[run.long_used ? 3 : 2] : static_cast<int>(n);  // warp kernels
   dnaln_stats& s = c->stats;
   s.reads += static_cast<uint64_t>(n);
   s.anchors += static_cast<uint64_t>(n_anchors_thread + n_anchors_warp);
@@ -792,21 +847,128 @@ int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_
   s.warp_minimizers += static_cast<uint64_t>(thread_path ? n_minimizers_warp_l : n_minimizers);
   s.warp_anchors += static_cast<uint64_t>(n_anchors_warp);
   s.warp_bases += static_cast<uint64_t>(thread_path ? n_bases_warp_l : B);
-  s.long_reads += static_cast<uint64_t>(thread_path && warp_list != big_list ? n_listed - n_warp : 0);
+  s.long_reads += static_cast<uint64_t>(thread_path && run.long_used ? n_listed - n_warp : 0);
   s.sw_tasks_score += static_cast<uint64_t>(counts[0]);
   s.sw_tasks_tb += static_cast<uint64_t>(counts[1]);
   s.cells += n_cells;
   s.mapped += n_mapped;
   s.candidates += n_cands;
-  // k_len64, k_score_tasks, k_choose, k_cig_slots, k_records, k_cigar_gather, pass 1 / 2
-  s.launches += 7 + (thread_path ? 5 : 1);
+  // k_len64, k_score_tasks, k_choose, k_cig_slots, k_records, k_cigar_gather, pass 1 / 2,
+  // plus the SW and sorting kernels the enqueue counted
+  s.launches += 7 + (thread_path ? 5 : 1) + run.launches;
   s.ms_seed += ev_ms(c, kEvSeed0, kEvSeed1);
   s.ms_chain += ev_ms(c, kEvChain0, kEvChain1);
   s.ms_sw_score += ev_ms(c, kEvSc0, kEvSc1);
   s.ms_sw_tb += ev_ms(c, kEvTb0, kEvTb1);
   s.ms_post += ev_ms(c, kEvPost0, kEvPost1);
   s.ms_total += ev_ms(c, kEvSeed0, kEvPost1);
+  s.graph_launches = c->graph_launches;
   return DNALN_OK;
+}
+
+// Everything that decides the launches of a batch and their arguments, as bytes: a cached
+// graph is replayed only for an identical key captured at the current buffer epoch.
+std::string graph_key(const dnaln_ctx* c, const IndexRes& ix, const char* d_seq, const int64_t* d_seq_off,
+                      const int32_t* d_seq_len, const uint32_t* d_hash, int64_t n, const dnaln_map_params& p,
+                      const dnaln_map_record* d_out, const uint32_t* d_cigar, int64_t cigar_cap,
+                      const BatchHints& hint) {
+  std::string k;
+  const auto put = [&](const void* v, size_t bytes) { k.append(static_cast<const char*>(v), bytes); };
+  put(&ix.dev, sizeof ix.dev);  // every pointer and dimension of the index the kernels take
+  const void* ptrs[] = {d_seq, d_seq_off, d_seq_len, d_hash, d_out, d_cigar, c->st};
+  put(ptrs, sizeof ptrs);
+  const int64_t nums[] = {n, hint.seq_base, hint.bases, hint.max_len, hint.cigar_base, cigar_cap, c->pool_cap,
+                          static_cast<int64_t>(c->dir_cap_bytes), c->sw_mode, c->warp_seed_only, c->long_thread,
+                          c->length_order};
+  put(nums, sizeof nums);
+  put(&p, sizeof p);
+  return k;
+}
+
+// The device pipeline. Inputs and d_out in device memory; CIGARs go to d_cigar
+// (capacity cigar_cap) or, when d_cigar is null, to an internal buffer returned via
+// *cigar_dev. *cigar_used = total ops.
+//
+// A batch whose size is known on the host (hints) is a candidate for a CUDA graph: the
+// first time its key is seen it runs eagerly (growing buffers, tuning kernel forms); the
+// second time, with nothing reallocated since, its launches are captured into a graph;
+// from then on the graph is launched, one launch for the batch's ~30 kernels, copies and
+// event records.
+int run_map(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_seq_off, const int32_t* d_seq_len,
+            const uint32_t* d_hash, int64_t n, const dnaln_map_params& p, dnaln_map_record* d_out, uint32_t* d_cigar,
+            int64_t cigar_cap, int64_t* cigar_used, uint32_t** cigar_dev, const BatchHints& hint0) {
+  *cigar_used = 0;
+  if (n == 0) return DNALN_OK;
+  BatchHints hint = hint0;
+  hint.caller_cigar = d_cigar != nullptr;
+  if ((hint.bases < 0 || hint.max_len < 0) && c->graphs && !c->trace_on) {
+    // the batch's size first (two small kernels and one read-back), so that the rest of it
+    // can run as a graph
+    cudaStream_t st = c->st;
+    DBUF(len64, int64_t, "len64", n + 1);
+    DBUF(pofs, int64_t, "pofs", n + 1);
+    DBUF(info, unsigned long long, "info", 10);
+    CK(cudaMemsetAsync(info, 0, sizeof(unsigned long long), st));
+    k_len64<<<nblk(n + 1), 256, 0, st>>>(d_seq_len, n, len64, info);
+    if (int e = exclusive_scan(c, len64, pofs, n + 1)) return e;
+    CK(cudaMemcpyAsync(c->h_info, pofs + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c->h_info + 1, info, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    hint.bases = c->h_info[0];
+    hint.max_len = c->h_info[1];
+    c->stats.launches += 1;
+  }
+  const bool graphable = c->graphs && hint.bases >= 0 && hint.max_len >= 0 && !c->trace_on && !hint.retry;
+  std::string key;
+  if (graphable) {
+    key = graph_key(c, ix, d_seq, d_seq_off, d_seq_len, d_hash, n, p, d_out, d_cigar, cigar_cap, hint);
+    auto it = c->graph_cache.find(key);
+    if (it != c->graph_cache.end() && it->second.epoch == c->epoch) {
+      CK(cudaGraphLaunch(it->second.exec, c->st));
+      ++c->graph_launches;
+      return map_finish(c, ix, d_seq, d_seq_off, d_seq_len, d_hash, n, p, d_out, cigar_used, cigar_dev, hint,
+                        it->second.run);
+    }
+    if (it != c->graph_cache.end()) {  // captured before a reallocation: stale
+      cudaGraphExecDestroy(it->second.exec);
+      c->graph_cache.erase(it);
+    }
+    auto seen = c->graph_seen.find(key);
+    if (seen != c->graph_seen.end() && seen->second == c->epoch) {
+      // second sighting with the same buffers: capture, instantiate, launch
+      if (c->graph_cache.size() >= 64) {
+        for (auto& kv : c->graph_cache) cudaGraphExecDestroy(kv.second.exec);
+        c->graph_cache.clear();
+      }
+      MapRun run;
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      c->capturing = true;
+      const int e = map_enqueue(c, ix, d_seq, d_seq_off, d_seq_len, d_hash, n, p, d_out, d_cigar, cigar_cap, hint,
+                                run);
+      c->capturing = false;
+      const cudaError_t ce = cudaStreamEndCapture(c->st, &g);
+      cudaGraphExec_t x = nullptr;
+      if (e == DNALN_OK && ce == cudaSuccess && g && cudaGraphInstantiate(&x, g, 0) == cudaSuccess) {
+        cudaGraphDestroy(g);
+        c->graph_cache[key] = CachedGraph{x, c->epoch, run};
+        CK(cudaGraphLaunch(x, c->st));
+        ++c->graph_launches;
+        return map_finish(c, ix, d_seq, d_seq_off, d_seq_len, d_hash, n, p, d_out, cigar_used, cigar_dev, hint, run);
+      }
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      c->graph_seen.erase(key);  // not capturable now: run eagerly below
+    }
+  }
+  MapRun run;
+  if (int e = map_enqueue(c, ix, d_seq, d_seq_off, d_seq_len, d_hash, n, p, d_out, d_cigar, cigar_cap, hint, run))
+    return e;
+  if (graphable) {
+    if (c->graph_seen.size() > 4096) c->graph_seen.clear();
+    c->graph_seen[key] = c->epoch;
+  }
+  return map_finish(c, ix, d_seq, d_seq_off, d_seq_len, d_hash, n, p, d_out, cigar_used, cigar_dev, hint, run);
 }
 
 IndexRes* find_index(dnaln_ctx* c, int32_t id) {
@@ -1066,6 +1228,8 @@ int dnaln_gpu_ctx_destroy(dnaln_ctx* c) {
   if (c->worker.joinable()) c->worker.join();
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
+  for (auto& kv : c->graph_cache) cudaGraphExecDestroy(kv.second.exec);
+  c->graph_cache.clear();
   for (auto& kv : c->idx) free_index(kv.second);
   for (auto& kv : c->bufs)
     if (kv.second.p) cudaFree(kv.second.p);
@@ -1178,6 +1342,10 @@ int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
   std::lock_guard<std::mutex> ctx_lock(c->mu);
   if (k == "warp_seed_only") {
     c->warp_seed_only = value != 0;
+    return DNALN_OK;
+  }
+  if (k == "graphs") {
+    c->graphs = value != 0;
     return DNALN_OK;
   }
   if (k == "sw_form") {

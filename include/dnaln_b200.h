@@ -94,6 +94,7 @@ typedef struct {
    * budget), their minimizers, anchors and bases */
   uint64_t warp_reads, warp_minimizers, warp_anchors, warp_bases;
   uint64_t long_reads; /* reads seeded and chained by the long-read thread kernel */
+  uint64_t graph_launches; /* batches launched as a captured CUDA graph (running total) */
 } dnaln_stats;
 
 /* ---- context ---------------------------------------------------------------------- */
@@ -129,6 +130,9 @@ int dnaln_gpu_set_sub_batch(dnaln_ctx* ctx, int64_t reads);
  *   "sub_batch"      same as dnaln_gpu_set_sub_batch;
  *   "warp_seed_only" 1 = seed and chain every read one warp per read (default 0: short
  *                    reads one thread per read, the others one warp per read);
+ *   "graphs"         1 = a batch whose size the host knows (the host-buffer calls) and
+ *                    whose launches repeat is captured once as a CUDA graph and replayed
+ *                    (default); 0 = launched kernel by kernel;
  *   "sw_form"        banded SW kernel form where a band width has two (W = 33, 65): 0 =
  *                    tuned per context (default), 1 = inter-sequence, 2 = intra-sequence;
  *   "long_thread"    1 = reads the short thread kernel lists go one thread each through

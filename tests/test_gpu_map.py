@@ -170,6 +170,27 @@ def test_thread_and_warp_seed_paths_identical(ctx, request, wl):
         assert np.array_equal(mixed_path.cigar, other.cigar)
 
 
+def test_graph_replays_give_the_same_results(ctx, repeat, mixed):
+    # a batch whose launches repeat is captured as a CUDA graph on its second run and
+    # replayed from the third on; every run must give what kernel-by-kernel launches give
+    for g, reads, bw in [(repeat[0], repeat[1], 16), (mixed[0], mixed[1], 64)]:
+        p = D.default_map_params(bw=bw)
+        iid = ctx.index_build(g)
+        try:
+            ctx.set_option("graphs", 0)
+            want = ctx.map_batch(iid, reads, p)
+            ctx.set_option("graphs", 1)
+            g0 = ctx.stats()["graph_launches"]
+            for _ in range(4):
+                got = ctx.map_batch(iid, reads, p)
+                assert np.array_equal(gpu_records(got), gpu_records(want))
+                assert np.array_equal(got.cigar, want.cigar)
+            assert ctx.stats()["graph_launches"] >= g0 + 2
+        finally:
+            ctx.set_option("graphs", 1)
+            ctx.index_free(iid)
+
+
 @pytest.mark.parametrize("sub_batch", [0, 3000])
 def test_submit_wait_matches_map_batch(ctx, repeat, sub_batch):
     # several batches in flight through the worker (reads copied in while the previous batch
