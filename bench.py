@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD,
                     help="synthetic workload (dnaln_b200.synth.WORKLOADS); the default is the headline one")
     ap.add_argument("--bw", type=int, default=16, help="SW band half-width (16, or 64 for the mixed-length workload)")
+    ap.add_argument("--sw-form", type=int, default=0, choices=[0, 1, 2],
+                    help="SW kernel form: 0 tuned per context, 1 inter-sequence, 2 intra-sequence (pin it under a "
+                         "profiler, whose serialised replays distort the tuner's timing)")
     ap.add_argument("--cigar-per-read", type=int, default=0,
                     help="CIGAR capacity per read of the output buffers (0 = the 2*len+3 bound)")
     ap.add_argument("--serve-requests", type=int, default=1500, help="requests per rate point (--workload serve)")
@@ -383,6 +386,7 @@ def run_ours(args) -> None:
     n_reads = len(reads)
     p = D.default_map_params(bw=args.bw)
     ctx = D.Context(local)
+    ctx.set_option("sw_form", args.sw_form)
     t_ix = time.perf_counter()
     iid = ctx.index_build(g)
     index_build_s = time.perf_counter() - t_ix
