@@ -583,7 +583,7 @@ def run_ours(args) -> None:
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         try:
-            traffic = json.loads(tf.read_text()).get(dom.split("<")[0])
+            traffic = json.loads(tf.read_text()).get(args.workload, {}).get(dom.split("<")[0])
         except (OSError, ValueError):
             traffic = None
     cells = st["cells"]
