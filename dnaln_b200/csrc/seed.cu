@@ -311,86 +311,12 @@ __device__ void chain_dp_rounds(const ChainArrays& a, int n, const ChainParamsDe
   }
 }
 
-// Sorts the n anchor keys, runs the DP, extracts chains into as.ch_*[c0 + j] and leaves
-// their final order in ord[0, m) (low 32 bits = j). Returns m in every lane.
-__device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const AnchorScratch& as, int64_t c0) {
+// Chain extraction (src/chain.cpp:49-68) as the reference runs it: ends in order of f
+// descending, index ascending; each walks prev links until an anchor an earlier chain
+// took. Chains go to as.ch_*[c0 + j]; returns m with the final order in ord[0, m).
+__device__ int extract_serial(const ChainArrays& a, int n, const ChainParamsDev& cp, const AnchorScratch& as,
+                              int64_t c0) {
   const int lane = threadIdx.x & 31;
-  warp_sort_u64(a.keys, n);
-  // DP (src/chain.cpp:22-45) over a window of the 64 nearest predecessors kept in
-  // registers: for row i, lane t holds the key and f of anchors i-1-t (window 0) and
-  // i-33-t (window 1); after the row both windows move up one lane and row i enters at
-  // lane 0, so f never makes a round trip through memory on the DP's serial path. One
-  // redux per row takes the max of score * 64 + (63 - distance): the largest score, ties
-  // to the nearest predecessor (the reference scans j downward with a strict '>').
-  // A predecessor is considered only while the scan would not have stopped before it:
-  // anchors are sorted by (strand, rpos), so a strand change or dr > max_gap at j holds
-  // for every farther j too, and each lane can test its own j.
-  const unsigned FULL = 0xffffffffu;
-  if (cp.lookback > 64) {
-    chain_dp_rounds(a, n, cp);
-  } else {
-  // window registers: rpos, qpos, strand and f of anchors i-1-lane and i-33-lane
-  int rw0 = 0, qw0 = 0, fw0 = 0, rw1 = 0, qw1 = 0, fw1 = 0;
-  uint32_t sw0 = 0, sw1 = 0;
-  const bool two = cp.lookback > 32;  // window 1 holds predecessors only beyond 32
-  uint64_t ki = n > 0 ? a.keys[0] : 0;
-  for (int i = 0; i < n; ++i) {
-    const uint64_t knext = i + 1 < n ? a.keys[i + 1] : 0;
-    const uint32_t si = key_strand(ki);
-    const int ri = static_cast<int>(key_rpos(ki)), qi = key_qpos(ki);
-    // rpos < 2^31 and |qpos| < 2^30, so dr and dq fit 32 bits; dd is formed in unsigned
-    // arithmetic and used only when dr and dq passed the range tests
-    const auto score_of = [&](int rj, int qj, uint32_t sj, int fj, int t) -> int {
-      const int dr = ri - rj, dq = qi - qj;
-      const int dd = static_cast<int>(dr > dq ? static_cast<uint32_t>(dr) - static_cast<uint32_t>(dq)
-                                              : static_cast<uint32_t>(dq) - static_cast<uint32_t>(dr));
-      if (t >= cp.lookback || t >= i || sj != si || dr > cp.max_gap || dr <= 0 || dq <= 0 || dd > cp.band)
-        return INT_MIN;
-      const int g = min(min(dq, dr), cp.k);
-      return (fj + g - cp.cost[dd]) * 64 + (63 - t);
-    };
-    int c = score_of(rw0, qw0, sw0, fw0, lane);
-    if (two && i > 32) c = max(c, score_of(rw1, qw1, sw1, fw1, 32 + lane));
-    const int m = __reduce_max_sync(FULL, c);
-    int fi = cp.k, pi = -1;
-    if (m != INT_MIN && (m >> 6) > cp.k) {
-      fi = m >> 6;
-      pi = i - 1 - (63 - (m & 63));
-    }
-    if (lane == 0) {
-      a.f[i] = fi;
-      a.prev[i] = pi;
-    }
-    // move the windows up one lane; row i enters window 0 at lane 0
-    if (two) {
-      const int out_r = __shfl_sync(FULL, rw0, 31), out_q = __shfl_sync(FULL, qw0, 31);
-      const int out_f = __shfl_sync(FULL, fw0, 31);
-      const uint32_t out_s = __shfl_sync(FULL, sw0, 31);
-      rw1 = __shfl_up_sync(FULL, rw1, 1);
-      qw1 = __shfl_up_sync(FULL, qw1, 1);
-      fw1 = __shfl_up_sync(FULL, fw1, 1);
-      sw1 = __shfl_up_sync(FULL, sw1, 1);
-      if (lane == 0) {
-        rw1 = out_r;
-        qw1 = out_q;
-        fw1 = out_f;
-        sw1 = out_s;
-      }
-    }
-    rw0 = __shfl_up_sync(FULL, rw0, 1);
-    qw0 = __shfl_up_sync(FULL, qw0, 1);
-    fw0 = __shfl_up_sync(FULL, fw0, 1);
-    sw0 = __shfl_up_sync(FULL, sw0, 1);
-    if (lane == 0) {
-      rw0 = ri;
-      qw0 = qi;
-      fw0 = fi;
-      sw0 = si;
-    }
-    ki = knext;
-  }
-  }
-  __syncwarp();
   // extraction order: f descending, index ascending (src/chain.cpp:49-50)
   for (int i = lane; i < n; i += 32) {
     a.ord[i] = static_cast<uint64_t>(desc32(a.f[i])) << 32 | static_cast<uint32_t>(i);
@@ -433,6 +359,235 @@ __device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const 
   __syncwarp();
   warp_sort_u64(a.ord, m);
   return m;
+}
+
+// The same chains for n <= 32 * E <= 256 anchors, found without the serial walk. Rank the
+// anchors by the extraction order (f descending, index ascending). The walk of end e
+// takes exactly the anchors x whose lowest-ranked descendant in the prev forest (the
+// anchors whose prev path passes through x, x included) is e: ranks of ends taken
+// earlier are lower, and a walk stops at the first anchor an earlier walk took, from
+// where on its path every anchor is taken by earlier walks too. An end whose own
+// lowest-ranked descendant is not itself lies on an earlier walk and is skipped. So:
+//  1. claim[x] = min over descendants of (desc f, index), by pointer jumping: each round
+//     every anchor pushes its claim to its ancestor 2^t links up (a shared-memory atomic
+//     min) and then doubles its link, until no link is left (log2 n + 1 rounds);
+//  2. the chain of end e is {x : claim[x] = e}; its last member's prev is the anchor
+//     where the walk stopped (score = f[e] - f[stop]), and count, min and max diagonal
+//     are shared-memory atomics into slots at index e.
+// Chain records go to as.ch_*[c0 + e] (slot = end index) and ord[0, m) holds the final
+// order (score descending, extraction order ascending; low 32 bits = slot). The rank key
+// (desc f, index) is packed into 32 bits as (0x7FFFFF - f) << 8 | index, which needs
+// 0 <= f <= 0x7FFFFF; a read outside that (never for k <= 32) uses extract_serial.
+template <int E>
+__device__ int extract_par(const ChainArrays& a, int n, const ChainParamsDev& cp, const AnchorScratch& as,
+                           int64_t c0) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  bool f_ok = true;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int y = e * 32 + lane;
+    if (y < n) f_ok = f_ok && a.f[y] >= 0 && a.f[y] <= 0x7FFFFF;
+  }
+  if (!__all_sync(FULL, f_ok)) return extract_serial(a, n, cp, as, c0);
+  uint64_t* claim = a.ord;  // claim keys: desc32(f) << 32 | index, min over descendants
+  uint8_t* link = a.used;   // pointer-jumping links + 1 (0 = none); every link < n <= 256
+  int anc[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int y = e * 32 + lane;
+    anc[e] = -1;
+    if (y < n) {
+      anc[e] = a.prev[y];
+      link[y] = static_cast<uint8_t>(anc[e] + 1);
+      claim[y] = static_cast<uint64_t>(desc32(a.f[y])) << 32 | static_cast<uint32_t>(y);
+    }
+  }
+  __syncwarp();
+  for (;;) {
+    bool more = false;
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (anc[e] >= 0) atomicMin(reinterpret_cast<unsigned long long*>(claim + anc[e]),
+                                 static_cast<unsigned long long>(claim[e * 32 + lane]));
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      if (anc[e] >= 0) anc[e] = static_cast<int>(link[anc[e]]) - 1;
+      more = more || anc[e] >= 0;
+    }
+    if (!__any_sync(FULL, more)) break;
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int y = e * 32 + lane;
+      if (y < n) link[y] = static_cast<uint8_t>(anc[e] + 1);
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  // per anchor: its chain's end, or (ends) 0x80000000 | f; the stop and score of a chain
+  // from its last member
+  uint32_t pk[E];
+  int sc[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int y = e * 32 + lane;
+    pk[e] = 0;
+    sc[e] = INT_MIN;
+    if (y < n) {
+      const int c = static_cast<int>(claim[y] & 0xFFu);
+      const int p = a.prev[y];
+      pk[e] = c == y ? 0x80000000u | static_cast<uint32_t>(a.f[y]) : static_cast<uint32_t>(c);
+      if (p < 0 || static_cast<int>(claim[p] & 0xFFu) != c) sc[e] = a.f[c] - (p >= 0 ? a.f[p] : 0);
+    }
+  }
+  __syncwarp();
+  // slots at the end's index: claim -> min | max biased diagonal, prev -> count, f -> score
+  uint32_t* dlo = reinterpret_cast<uint32_t*>(claim);
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int y = e * 32 + lane;
+    if (y < n && (pk[e] >> 31)) {
+      claim[y] = 0xFFFFFFFFull;
+      a.prev[y] = 0;
+    }
+    if (sc[e] != INT_MIN) a.f[(pk[e] >> 31) ? y : static_cast<int>(pk[e])] = sc[e];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int y = e * 32 + lane;
+    if (y < n) {
+      const int c = (pk[e] >> 31) ? y : static_cast<int>(pk[e]);
+      const uint64_t ky = a.keys[y];
+      // rpos < 2^31 and |qpos| < 2^30: rpos - qpos + 2^30 fits 32 bits unsigned
+      const uint32_t d = key_rpos(ky) - static_cast<uint32_t>(key_qpos(ky)) + (1u << 30);
+      atomicMin(dlo + 2 * c, d);
+      atomicMax(dlo + 2 * c + 1, d);
+      atomicAdd(a.prev + c, 1);
+    }
+  }
+  __syncwarp();
+  // chain records of the ends that pass the filters
+  bool keep[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int y = e * 32 + lane;
+    keep[e] = false;
+    if (y < n && (pk[e] >> 31)) {
+      const int score = a.f[y], cnt = a.prev[y];
+      keep[e] = !(score < cp.min_score || cnt < cp.min_anchors);
+      if (keep[e]) {
+        const uint64_t ke = a.keys[y];
+        as.ch_score[c0 + y] = score;
+        as.ch_sn[c0 + y] = key_strand(ke) | static_cast<uint32_t>(cnt) << 1;
+        as.ch_dmin[c0 + y] = static_cast<int64_t>(dlo[2 * y]) - (1ll << 30);
+        as.ch_dmax[c0 + y] = static_cast<int64_t>(dlo[2 * y + 1]) - (1ll << 30);
+        as.ch_rpos[c0 + y] = key_rpos(ke);
+      }
+    }
+  }
+  __syncwarp();
+  // final order: score descending, extraction order ascending (stable_sort, src/chain.cpp:68)
+  int m = 0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const unsigned b = __ballot_sync(FULL, keep[e]);
+    if (keep[e]) {
+      const int y = e * 32 + lane;
+      const uint32_t rank = (0x7FFFFFu - (pk[e] & 0x7FFFFFu)) << 8 | static_cast<uint32_t>(y);
+      a.ord[m + __popc(b & ((1u << lane) - 1u))] = static_cast<uint64_t>(desc32(a.f[y])) << 32 | rank;
+    }
+    m += __popc(b);
+  }
+  __syncwarp();
+  warp_sort_u64(a.ord, m);
+  for (int j = lane; j < m; j += 32) a.ord[j] = (a.ord[j] & 0xFFFFFFFF00000000ull) | (a.ord[j] & 0xFFu);
+  __syncwarp();
+  return m;
+}
+
+// Sorts the n anchor keys, runs the DP, extracts chains into as.ch_*[c0 + j] (j a slot
+// below n) and leaves their final order in ord[0, m) (low 32 bits = j). Returns m in
+// every lane.
+__device__ int chain_core(ChainArrays a, int n, const ChainParamsDev& cp, const AnchorScratch& as, int64_t c0) {
+  const int lane = threadIdx.x & 31;
+  warp_sort_u64(a.keys, n);
+  // DP (src/chain.cpp:22-45). For row i, lane t holds in registers the key and f of
+  // anchor i-1-t (the 32 nearest predecessors); after the row the window moves up one
+  // lane and row i enters at lane 0, so f never makes a round trip through memory on the
+  // DP's serial path. Predecessors at distance 33..lookback are read from a.keys / a.f
+  // only when the one at distance 32 has not stopped the scan: anchors are sorted by
+  // (strand, rpos), so a strand change or dr > max_gap at j holds for every farther j
+  // too (and each lane can test its own j). One redux per row takes the max of
+  // score * 64 + (63 - distance): the largest score, ties to the nearest predecessor
+  // (the reference scans j downward with a strict '>').
+  const unsigned FULL = 0xffffffffu;
+  if (cp.lookback > 64) {
+    chain_dp_rounds(a, n, cp);
+  } else {
+  int rw = 0, qw = 0, fw = 0;
+  uint32_t sw = 0;
+  const bool two = cp.lookback > 32;
+  uint64_t ki = n > 0 ? a.keys[0] : 0;
+  for (int i = 0; i < n; ++i) {
+    const uint64_t knext = i + 1 < n ? a.keys[i + 1] : 0;
+    const uint32_t si = key_strand(ki);
+    const int ri = static_cast<int>(key_rpos(ki)), qi = key_qpos(ki);
+    // rpos < 2^31 and |qpos| < 2^30, so dr and dq fit 32 bits; dd is formed in unsigned
+    // arithmetic and used only when dr and dq passed the range tests
+    const auto score_of = [&](int rj, int qj, uint32_t sj, int fj, int t) -> int {
+      const int dr = ri - rj, dq = qi - qj;
+      const int dd = static_cast<int>(dr > dq ? static_cast<uint32_t>(dr) - static_cast<uint32_t>(dq)
+                                              : static_cast<uint32_t>(dq) - static_cast<uint32_t>(dr));
+      if (t >= cp.lookback || t >= i || sj != si || dr > cp.max_gap || dr <= 0 || dq <= 0 || dd > cp.band)
+        return INT_MIN;
+      const int g = min(min(dq, dr), cp.k);
+      return (fj + g - cp.cost[dd]) * 64 + (63 - t);
+    };
+    int c = score_of(rw, qw, sw, fw, lane);
+    if (two && i > 32) {
+      const bool live = sw == si && ri - rw <= cp.max_gap;  // lane 31: the predecessor i-32
+      if (__shfl_sync(FULL, live, 31)) {
+        __syncwarp();  // f of rows <= i-33, written by lane 0, is visible to every lane
+        const int j = i - 33 - lane;
+        if (j >= 0) {
+          const uint64_t kj = a.keys[j];
+          c = max(c, score_of(static_cast<int>(key_rpos(kj)), key_qpos(kj), key_strand(kj), a.f[j], 32 + lane));
+        }
+      }
+    }
+    const int m = __reduce_max_sync(FULL, c);
+    int fi = cp.k, pi = -1;
+    if (m != INT_MIN && (m >> 6) > cp.k) {
+      fi = m >> 6;
+      pi = i - 1 - (63 - (m & 63));
+    }
+    if (lane == 0) {
+      a.f[i] = fi;
+      a.prev[i] = pi;
+    }
+    // move the window up one lane; row i enters at lane 0
+    rw = __shfl_up_sync(FULL, rw, 1);
+    qw = __shfl_up_sync(FULL, qw, 1);
+    fw = __shfl_up_sync(FULL, fw, 1);
+    sw = __shfl_up_sync(FULL, sw, 1);
+    if (lane == 0) {
+      rw = ri;
+      qw = qi;
+      fw = fi;
+      sw = si;
+    }
+    ki = knext;
+  }
+  }
+  __syncwarp();
+  if (n <= 32) return extract_par<1>(a, n, cp, as, c0);
+  if (n <= 64) return extract_par<2>(a, n, cp, as, c0);
+  if (n <= 128) return extract_par<4>(a, n, cp, as, c0);
+  if (n <= 256) return extract_par<8>(a, n, cp, as, c0);
+  return extract_serial(a, n, cp, as, c0);
 }
 
 // Ascending bitonic sort of one 64-bit key per lane across the warp (lane order).
@@ -700,9 +855,62 @@ __device__ void chain_read(int64_t r, const int64_t* __restrict__ pofs, const in
   }
   const int m = chain_core(a, na, cp, as, a0);
   // candidate loci (src/mapper.cpp:40-62)
+  const int64_t cbase = r * cand.max_cand;
+  if (cand.max_cand <= 32) {
+    // the chains are read 32 at a time, one per lane (one memory round trip for all of
+    // them), then taken in order by a warp-uniform loop over shuffles; accepted
+    // candidate x is kept by lane x and written out at the end
+    const unsigned FULL = 0xffffffffu;
+    int nd = 0;
+    int64_t my_diag = 0;
+    uint32_t my_rev = 0, my_rpos = 0;
+    double min_score = 0;
+    bool done = m == 0;
+    for (int base = 0; base < m && !done; base += 32) {
+      const int c = base + lane;
+      int sc = 0;
+      int64_t dg = 0;
+      uint32_t st = 0, rp = 0;
+      if (c < m) {
+        const int64_t ci = a0 + static_cast<int64_t>(a.ord[c] & 0xffffffffu);
+        sc = as.ch_score[ci];
+        const int64_t dmin = as.ch_dmin[ci], dmax = as.ch_dmax[ci];
+        dg = dmin + (dmax - dmin) / 2;
+        st = as.ch_sn[ci] & 1u;
+        rp = as.ch_rpos[ci];
+      }
+      if (base == 0) min_score = static_cast<double>(__shfl_sync(FULL, sc, 0)) * cand.pri_ratio;
+      const int cnt = min(32, m - base);
+      for (int t = 0; t < cnt; ++t) {
+        const int sc_t = __shfl_sync(FULL, sc, t);
+        if (static_cast<double>(sc_t) < min_score || nd >= cand.max_cand) {
+          done = true;
+          break;
+        }
+        const int64_t diag = __shfl_sync(FULL, dg, t);
+        const uint32_t strand = __shfl_sync(FULL, st, t);
+        const int64_t dd = my_diag - diag;
+        if (__any_sync(FULL, lane < nd && my_rev == strand && (dd < 0 ? -dd : dd) <= cand.bw)) continue;
+        const uint32_t rpos = __shfl_sync(FULL, rp, t);
+        if (lane == nd) {
+          my_diag = diag;
+          my_rev = strand;
+          my_rpos = rpos;
+        }
+        ++nd;
+      }
+    }
+    if (lane < nd) {
+      cb.rev[cbase + lane] = static_cast<uint8_t>(my_rev);
+      cb.contig[cbase + lane] = contig_of(ix, my_rpos);
+      cb.diag[cbase + lane] = my_diag;
+      cb.wstart[cbase + lane] = my_diag - cand.bw;
+    }
+    if (lane == 0) cb.n_cand[r] = nd;
+    return;
+  }
   if (lane == 0) {
     int nd = 0;
-    const int64_t cbase = r * cand.max_cand;
     if (m > 0) {
       const double min_score = static_cast<double>(as.ch_score[a0 + (a.ord[0] & 0xffffffffu)]) * cand.pri_ratio;
       for (int c = 0; c < m; ++c) {
@@ -729,7 +937,7 @@ __device__ void chain_read(int64_t r, const int64_t* __restrict__ pofs, const in
 }
 
 // One warp per read: reads [0, n), or with a list the reads list[0, list_n) (grid-stride).
-__global__ void __launch_bounds__(kChainWarps * 32)
+__global__ void __launch_bounds__(kChainWarps * 32, 8)
     k_chain_map(const int64_t* __restrict__ pofs, const int32_t* __restrict__ seq_len, int64_t n,
                 const int32_t* __restrict__ list, const int* __restrict__ list_n, const int32_t* __restrict__ n_min,
                 const int64_t* __restrict__ n_anchor, MinBuf mb, DevIndex ix, ChainParamsDev cp, CandParams cand,
