@@ -172,6 +172,26 @@ def kernel_bytes(kernel: str, st: dict, mean_len: float, bw: int = 16) -> float 
     return None
 
 
+def index_image_round_trip(ctx, iid) -> dict:
+    """Index admission from a file: dnaln_gpu_index_save, then dnaln_gpu_index_load of the
+    image (read, checksum and structural checks, upload) against the device build above."""
+    import tempfile
+    try:
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "index.img")
+            t0 = time.perf_counter()
+            ctx.index_save(iid, path)
+            t1 = time.perf_counter()
+            size = os.path.getsize(path)
+            iid2 = ctx.index_load(path)
+            t2 = time.perf_counter()
+            ctx.index_free(iid2)
+        return {"bytes": size, "save_s": t1 - t0, "load_s": t2 - t1, "load_gbs": size / (t2 - t1) / 1e9,
+                "where": "dnaln_gpu_index_save / dnaln_gpu_index_load"}
+    except (OSError, D.DnalnError) as e:
+        return {"error": str(e)}
+
+
 def cpu_baseline(g, reads, params) -> dict:
     """The reference's CPU mapper on this host (all hardware threads), on one batch."""
     import oracle
@@ -623,6 +643,8 @@ def run_ours(args) -> None:
            "candidates_per_read": st["candidates"] / max(st["reads"], 1)}
     if e2e_text:
         out["e2e_text"] = e2e_text
+    if rank == 0:
+        out["index"]["image"] = index_image_round_trip(ctx, iid)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(g, reads, p)
     if rank == 0:

@@ -19,6 +19,7 @@ Every call goes to the CUDA library; there is no CPU fallback. Errors raise
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -281,6 +282,33 @@ class Context:
 
     def index_free(self, iid: int) -> None:
         self._check(self._lib.dnaln_gpu_index_free(self._h, iid))
+
+    def index_save(self, iid: int, path) -> None:
+        """Writes index `iid` with its genome as an image file (dnaln_gpu_index_save)."""
+        self._check(self._lib.dnaln_gpu_index_save(self._h, iid, os.fsencode(path)))
+
+    def index_load(self, path) -> int:
+        """A new resident index from an image file written by index_save (checked, no rebuild)."""
+        iid = C.c_int32()
+        self._check(self._lib.dnaln_gpu_index_load(self._h, os.fsencode(path), C.byref(iid)))
+        return iid.value
+
+    def index_upload(self, g: Genome, keys, offsets, counts, positions, k: int = 15, w: int = 10) -> int:
+        """A new resident index from a bucket table built on the host in the reference's layout
+        (MinimizerIndex, src/index.hpp:49-56): keys (~0 = empty) / offsets / counts of a power-of-two
+        number of buckets into positions (pos << 1 | strand)."""
+        keys = np.ascontiguousarray(keys, np.uint64)
+        offsets = np.ascontiguousarray(offsets, np.uint32)
+        counts = np.ascontiguousarray(counts, np.uint32)
+        positions = np.ascontiguousarray(positions, np.uint32)
+        if not (len(keys) == len(offsets) == len(counts)):
+            raise ValueError("keys, offsets and counts must have one entry per bucket")
+        iid = C.c_int32()
+        self._check(self._lib.dnaln_gpu_index_upload(
+            self._h, ptr(g.codes), len(g.codes), ptr(g.contig_off), ptr(g.contig_len), g.n_contigs, k, w, ptr(keys),
+            ptr(offsets), ptr(counts), len(keys), ptr(positions) if len(positions) else None, len(positions),
+            C.byref(iid)))
+        return iid.value
 
     def index_attach(self, src: "Context", iid: int) -> int:
         """Shares index `iid` of context `src` (same device) with this context, no copy."""

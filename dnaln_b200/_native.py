@@ -12,9 +12,9 @@ import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "libdnaln_b200.so"
 
-OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_CAPACITY, ERR_NO_DEVICE, ERR_DEVICE, ERR_NOT_FOUND = range(8)
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_CAPACITY, ERR_NO_DEVICE, ERR_DEVICE, ERR_NOT_FOUND, ERR_IO = range(9)
 ERR_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "CUDA", 3: "OOM", 4: "CAPACITY", 5: "NO_DEVICE", 6: "DEVICE",
-             7: "NOT_FOUND"}
+             7: "NOT_FOUND", 8: "IO"}
 
 
 class ScoreParams(C.Structure):
@@ -132,6 +132,9 @@ SIGNATURES = {
     "dnaln_gpu_index_export": (C.c_int, [P, i32, P, P, P, P]),
     "dnaln_gpu_index_free": (C.c_int, [P, i32]),
     "dnaln_gpu_index_attach": (C.c_int, [P, P, i32, C.POINTER(i32)]),
+    "dnaln_gpu_index_save": (C.c_int, [P, i32, C.c_char_p]),
+    "dnaln_gpu_index_load": (C.c_int, [P, C.c_char_p, C.POINTER(i32)]),
+    "dnaln_gpu_index_upload": (C.c_int, [P, P, u64, P, P, i32, i32, i32, P, P, P, u64, P, u64, C.POINTER(i32)]),
     "dnaln_gpu_ctx_device": (C.c_int, [P, C.POINTER(i32)]),
     "dnaln_serve_create": (C.c_int, [P, C.POINTER(ServeParams), C.POINTER(P)]),
     "dnaln_serve_submit": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64, C.POINTER(i64),

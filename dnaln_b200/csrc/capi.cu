@@ -19,6 +19,7 @@
 #include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <condition_variable>
 #include <cstdarg>
@@ -993,6 +994,55 @@ int dalloc(dnaln_ctx* c, DevBuf& b, size_t bytes) {
 // Drops this holder's reference; the memory goes with the last one.
 void free_index(IndexRes& r) { r.mem.reset(); }
 
+// Points r.dev at r.mem's buffers, fills its scalars from r and registers r under a new id.
+void register_index(dnaln_ctx* c, IndexRes& r, uint64_t mask, int32_t n_n_runs, int32_t* index_id) {
+  IndexMem& m = *r.mem;
+  r.dev.table = static_cast<const ulonglong2*>(m.table.p);
+  r.dev.positions = static_cast<const uint32_t*>(m.positions.p);
+  r.dev.genome = static_cast<const uint8_t*>(m.genome.p);
+  r.dev.contig_off = static_cast<const uint64_t*>(m.coff.p);
+  r.dev.contig_len = static_cast<const uint32_t*>(m.clen.p);
+  r.dev.n_runs = static_cast<const uint2*>(m.nruns.p);
+  r.dev.n_n_runs = n_n_runs;
+  r.dev.mask = mask;
+  r.dev.n_contigs = r.n_contigs;
+  r.dev.k = r.k;
+  r.dev.w = r.w;
+  const int32_t id = c->next_id++;
+  c->idx[id] = r;
+  *index_id = id;
+}
+
+// Checks a contig table against the genome length: in bounds and in order.
+int check_contigs(dnaln_ctx* c, const uint64_t* contig_off, const uint32_t* contig_len, int32_t n_contigs,
+                  uint64_t n_bases, int code) {
+  for (int32_t i = 0; i < n_contigs; ++i)
+    if (contig_off[i] + contig_len[i] > n_bases || (i > 0 && contig_off[i] < contig_off[i - 1]))
+      return fail(c, code, "contig %d is outside the genome or out of order", i);
+  return DNALN_OK;
+}
+
+// Structural checks of a bucket table / position array, chunk by chunk: every non-empty
+// bucket's positions lie inside the array, every position inside the genome. Counts the
+// non-empty buckets and the largest count.
+struct TableCheck {
+  uint64_t n_pos = 0, n_bases = 0, n_keys = 0;
+  uint32_t max_count = 0;
+  bool ok = true;
+  void buckets(const ulonglong2* t, size_t n) {
+    for (size_t i = 0; i < n; ++i) {
+      if (t[i].x == kInvalidHash) continue;
+      const uint64_t off = static_cast<uint32_t>(t[i].y), cnt = t[i].y >> 32;
+      ok = ok && off + cnt <= n_pos;
+      ++n_keys;
+      if (cnt > max_count) max_count = static_cast<uint32_t>(cnt);
+    }
+  }
+  void positions(const uint32_t* v, size_t n) {
+    for (size_t i = 0; i < n; ++i) ok = ok && (v[i] >> 1) < n_bases;
+  }
+};
+
 
 // ---- the worker behind dnaln_gpu_map_submit ----------------------------------------------
 // Parts are taken from the queue in order. While part j computes on the context's stream
@@ -1444,20 +1494,7 @@ int dnaln_gpu_index_build(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases,
   r.n_contigs = n_contigs;
   r.k = k;
   r.w = w;
-  r.dev.table = static_cast<const ulonglong2*>(m.table.p);
-  r.dev.positions = static_cast<const uint32_t*>(m.positions.p);
-  r.dev.genome = static_cast<const uint8_t*>(m.genome.p);
-  r.dev.contig_off = static_cast<const uint64_t*>(m.coff.p);
-  r.dev.contig_len = static_cast<const uint32_t*>(m.clen.p);
-  r.dev.n_runs = static_cast<const uint2*>(m.nruns.p);
-  r.dev.n_n_runs = b.n_n_runs;
-  r.dev.mask = b.mask;
-  r.dev.n_contigs = n_contigs;
-  r.dev.k = k;
-  r.dev.w = w;
-  const int32_t id = c->next_id++;
-  c->idx[id] = r;
-  *index_id = id;
+  register_index(c, r, b.mask, b.n_n_runs, index_id);
   return DNALN_OK;
 }
 
@@ -1507,6 +1544,302 @@ int dnaln_gpu_index_free(dnaln_ctx* c, int32_t id) {
   cudaStreamSynchronize(c->st);
   free_index(*r);
   c->idx.erase(id);
+  return DNALN_OK;
+}
+
+// ---- index image files ---------------------------------------------------------------
+namespace {
+
+constexpr char kImageMagic[8] = {'D', 'N', 'B', 'I', 'D', 'X', '0', '1'};
+constexpr uint32_t kImageVersion = 1;
+constexpr size_t kImageChunk = 64ull << 20;  // staging chunk (a multiple of 32 bytes)
+
+struct ImageHeader {
+  char magic[8];
+  uint32_t version, header_bytes;
+  int32_t k, w, n_contigs, n_n_runs;
+  uint32_t max_count, reserved;
+  uint64_t n_bases, n_keys, n_pos, n_buckets, mask;
+  uint64_t checksum;  // ImageHash of every section, in file order
+};
+
+// 64-bit checksum of a byte stream given in chunks whose sizes are multiples of 32 except
+// the last of each section: four independent multiply-rotate lanes over 8-byte words.
+struct ImageHash {
+  uint64_t h[4] = {0x243F6A8885A308D3ull, 0x13198A2E03707344ull, 0xA4093822299F31D0ull, 0x082EFA98EC4E6C89ull};
+  static uint64_t mix(uint64_t h, uint64_t w) {
+    h ^= w * 0x9E3779B97F4A7C15ull;
+    return ((h << 27) | (h >> 37)) * 0xBF58476D1CE4E5B9ull;
+  }
+  void add(const void* data, size_t len) {
+    const uint8_t* p = static_cast<const uint8_t*>(data);
+    size_t i = 0;
+    for (; i + 32 <= len; i += 32) {
+      uint64_t w[4];
+      std::memcpy(w, p + i, 32);
+      for (int l = 0; l < 4; ++l) h[l] = mix(h[l], w[l]);
+    }
+    for (; i + 8 <= len; i += 8) {
+      uint64_t w;
+      std::memcpy(&w, p + i, 8);
+      h[0] = mix(h[0], w);
+    }
+    if (i < len) {
+      uint64_t w = 0;
+      std::memcpy(&w, p + i, len - i);
+      h[1] = mix(h[1], w ^ static_cast<uint64_t>(len - i) << 56);
+    }
+  }
+  uint64_t done() const { return mix(mix(h[0], h[1]), mix(h[2], h[3])); }
+};
+
+struct FileCloser {
+  FILE* f = nullptr;
+  ~FileCloser() {
+    if (f) std::fclose(f);
+  }
+};
+
+struct PinnedChunks {  // two page-locked staging chunks
+  void* p[2] = {nullptr, nullptr};
+  ~PinnedChunks() {
+    for (void* x : p)
+      if (x) cudaFreeHost(x);
+  }
+};
+
+}  // namespace
+
+int dnaln_gpu_index_save(dnaln_ctx* c, int32_t id, const char* path) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
+  if (!path) return fail(c, DNALN_ERR_INVALID_ARG, "null path");
+  if (int e = set_device(c)) return e;
+  IndexRes* r = find_index(c, id);
+  if (!r) return DNALN_ERR_NOT_FOUND;
+  const IndexMem& m = *r->mem;
+  ImageHeader h{};
+  std::memcpy(h.magic, kImageMagic, sizeof h.magic);
+  h.version = kImageVersion;
+  h.header_bytes = sizeof(ImageHeader);
+  h.k = r->k;
+  h.w = r->w;
+  h.n_contigs = r->n_contigs;
+  h.n_n_runs = r->dev.n_n_runs;
+  h.max_count = r->max_count;
+  h.n_bases = r->n_bases;
+  h.n_keys = r->n_keys;
+  h.n_pos = r->n_pos;
+  h.n_buckets = r->n_buckets;
+  h.mask = r->dev.mask;
+  const struct {
+    const void* d;
+    size_t bytes;
+  } sec[] = {{m.coff.p, static_cast<size_t>(h.n_contigs) * sizeof(uint64_t)},
+             {m.clen.p, static_cast<size_t>(h.n_contigs) * sizeof(uint32_t)},
+             {m.genome.p, h.n_bases},
+             {m.table.p, h.n_buckets * sizeof(ulonglong2)},
+             {m.positions.p, h.n_pos * sizeof(uint32_t)},
+             {m.nruns.p, static_cast<size_t>(h.n_n_runs) * sizeof(uint2)}};
+  CK(cudaStreamSynchronize(c->st));  // nothing queued may still write the index
+  PinnedChunks pc;
+  CK(cudaMallocHost(&pc.p[0], kImageChunk));
+  const std::string tmp = std::string(path) + ".tmp";
+  FileCloser fc;
+  fc.f = std::fopen(tmp.c_str(), "wb");
+  if (!fc.f) return fail(c, DNALN_ERR_IO, "cannot open %s for writing", tmp.c_str());
+  bool ok = std::fwrite(&h, sizeof h, 1, fc.f) == 1;  // the checksum is filled in at the end
+  ImageHash hs;
+  for (const auto& x : sec) {
+    for (size_t at = 0; ok && at < x.bytes; at += kImageChunk) {
+      const size_t n = std::min(kImageChunk, x.bytes - at);
+      CK(cudaMemcpy(pc.p[0], static_cast<const char*>(x.d) + at, n, cudaMemcpyDeviceToHost));
+      hs.add(pc.p[0], n);
+      ok = std::fwrite(pc.p[0], 1, n, fc.f) == n;
+    }
+  }
+  h.checksum = hs.done();
+  ok = ok && std::fseek(fc.f, 0, SEEK_SET) == 0 && std::fwrite(&h, sizeof h, 1, fc.f) == 1;
+  ok = ok && std::fflush(fc.f) == 0;
+  const bool closed = std::fclose(fc.f) == 0;
+  fc.f = nullptr;
+  if (!ok || !closed || std::rename(tmp.c_str(), path) != 0) {
+    std::remove(tmp.c_str());
+    return fail(c, DNALN_ERR_IO, "writing the index image %s failed", path);
+  }
+  return DNALN_OK;
+}
+
+int dnaln_gpu_index_load(dnaln_ctx* c, const char* path, int32_t* index_id) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
+  if (!path || !index_id) return fail(c, DNALN_ERR_INVALID_ARG, "null argument");
+  if (int e = set_device(c)) return e;
+  FileCloser fc;
+  fc.f = std::fopen(path, "rb");
+  if (!fc.f) return fail(c, DNALN_ERR_IO, "cannot open %s", path);
+  ImageHeader h{};
+  if (std::fread(&h, sizeof h, 1, fc.f) != 1 || std::memcmp(h.magic, kImageMagic, sizeof h.magic) != 0 ||
+      h.version != kImageVersion || h.header_bytes != sizeof(ImageHeader))
+    return fail(c, DNALN_ERR_IO, "%s is not an index image of this version", path);
+  const bool pow2 = h.n_buckets >= 1 && (h.n_buckets & (h.n_buckets - 1)) == 0;
+  if (h.k < 4 || h.k > 28 || h.w < 1 || h.w > 255 || h.n_contigs < 1 || h.n_bases >= (1ULL << 31) || !pow2 ||
+      h.mask != h.n_buckets - 1 || h.n_keys >= h.n_buckets || h.n_pos >= (1ULL << 32) || h.n_n_runs < 0 ||
+      static_cast<uint64_t>(h.n_n_runs) > h.n_bases || h.n_buckets > (1ULL << 34))
+    return fail(c, DNALN_ERR_IO, "%s: header out of range", path);
+  IndexRes r;
+  r.mem = std::make_shared<IndexMem>();
+  r.device = c->device;
+  IndexMem& m = *r.mem;
+  int e = DNALN_OK;
+  if ((e = dalloc(c, m.coff, h.n_contigs * sizeof(uint64_t))) || (e = dalloc(c, m.clen, h.n_contigs * sizeof(uint32_t))) ||
+      (e = dalloc(c, m.genome, h.n_bases)) || (e = dalloc(c, m.table, h.n_buckets * sizeof(ulonglong2))) ||
+      (e = dalloc(c, m.positions, h.n_pos * sizeof(uint32_t))) ||
+      (e = dalloc(c, m.nruns, static_cast<size_t>(h.n_n_runs) * sizeof(uint2))))
+    return e;
+  std::vector<uint64_t> coff(static_cast<size_t>(h.n_contigs));
+  std::vector<uint32_t> clen(static_cast<size_t>(h.n_contigs));
+  const struct {
+    void* d;
+    size_t bytes;
+    int kind;  // 0 contig offsets, 1 contig lengths, 2 genome, 3 buckets, 4 positions, 5 N runs
+  } sec[] = {{m.coff.p, coff.size() * sizeof(uint64_t), 0},
+             {m.clen.p, clen.size() * sizeof(uint32_t), 1},
+             {m.genome.p, h.n_bases, 2},
+             {m.table.p, h.n_buckets * sizeof(ulonglong2), 3},
+             {m.positions.p, h.n_pos * sizeof(uint32_t), 4},
+             {m.nruns.p, static_cast<size_t>(h.n_n_runs) * sizeof(uint2), 5}};
+  PinnedChunks pc;
+  CK(cudaMallocHost(&pc.p[0], kImageChunk));
+  CK(cudaMallocHost(&pc.p[1], kImageChunk));
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  CK(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
+  if (cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming) != cudaSuccess) {
+    cudaEventDestroy(done[0]);
+    return fail(c, DNALN_ERR_CUDA, "event creation failed");
+  }
+  ImageHash hs;
+  TableCheck tc;
+  tc.n_pos = h.n_pos;
+  tc.n_bases = h.n_bases;
+  bool ok = true;
+  uint32_t prev_end = 0;
+  int slot = 0;
+  cudaError_t x = cudaSuccess;
+  // chunk j is read into staging slot j % 2 while chunk j-1's copy to the device runs
+  for (const auto& s : sec) {
+    for (size_t at = 0; ok && x == cudaSuccess && at < s.bytes; at += kImageChunk) {
+      const size_t n = std::min(kImageChunk, s.bytes - at);
+      x = cudaEventSynchronize(done[slot]);  // the copy that last used this slot is done
+      if (x != cudaSuccess) break;
+      void* buf = pc.p[slot];
+      if (std::fread(buf, 1, n, fc.f) != n) {
+        ok = false;
+        break;
+      }
+      hs.add(buf, n);
+      switch (s.kind) {
+        case 0: std::memcpy(coff.data(), buf, n); break;
+        case 1: std::memcpy(clen.data(), buf, n); break;
+        case 3: tc.buckets(static_cast<const ulonglong2*>(buf), n / sizeof(ulonglong2)); break;
+        case 4: tc.positions(static_cast<const uint32_t*>(buf), n / sizeof(uint32_t)); break;
+        case 5: {
+          const uint2* v = static_cast<const uint2*>(buf);
+          for (size_t i = 0; i < n / sizeof(uint2); ++i) {
+            ok = ok && v[i].x < v[i].y && v[i].y <= h.n_bases && v[i].x >= prev_end;
+            prev_end = v[i].y;
+          }
+          break;
+        }
+        default: break;
+      }
+      x = cudaMemcpyAsync(static_cast<char*>(s.d) + at, buf, n, cudaMemcpyHostToDevice, c->st);
+      if (x == cudaSuccess) x = cudaEventRecord(done[slot], c->st);
+      slot ^= 1;
+    }
+  }
+  if (x == cudaSuccess) x = cudaStreamSynchronize(c->st);
+  cudaEventDestroy(done[0]);
+  cudaEventDestroy(done[1]);
+  if (x != cudaSuccess) return fail(c, DNALN_ERR_CUDA, "index image upload: %s", cudaGetErrorString(x));
+  const bool at_end = ok && std::fgetc(fc.f) == EOF;
+  if (!at_end || hs.done() != h.checksum)
+    return fail(c, DNALN_ERR_IO, "%s: truncated, longer than its header says, or its checksum does not match", path);
+  if (!tc.ok || tc.n_keys != h.n_keys || tc.max_count != h.max_count)
+    return fail(c, DNALN_ERR_IO, "%s: the bucket table or positions are inconsistent with the header", path);
+  if (check_contigs(c, coff.data(), clen.data(), h.n_contigs, h.n_bases, DNALN_ERR_IO)) return DNALN_ERR_IO;
+  r.n_keys = h.n_keys;
+  r.n_pos = h.n_pos;
+  r.n_buckets = h.n_buckets;
+  r.n_bases = h.n_bases;
+  r.max_count = h.max_count;
+  r.n_contigs = h.n_contigs;
+  r.k = h.k;
+  r.w = h.w;
+  register_index(c, r, h.mask, h.n_n_runs, index_id);
+  return DNALN_OK;
+}
+
+int dnaln_gpu_index_upload(dnaln_ctx* c, const uint8_t* genome, uint64_t n_bases, const uint64_t* contig_off,
+                           const uint32_t* contig_len, int32_t n_contigs, int32_t k, int32_t w, const uint64_t* keys,
+                           const uint32_t* offsets, const uint32_t* counts, uint64_t n_buckets,
+                           const uint32_t* positions, uint64_t n_pos, int32_t* index_id) {
+  if (!c) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(c->mu);
+  if (!genome || !contig_off || !contig_len || !keys || !offsets || !counts || (n_pos && !positions) || !index_id ||
+      n_contigs < 1)
+    return fail(c, DNALN_ERR_INVALID_ARG, "null argument or no contigs");
+  if (k < 4 || k > 28) return fail(c, DNALN_ERR_INVALID_ARG, "k must be in [4, 28] (got %d)", k);
+  if (w < 1 || w > 255) return fail(c, DNALN_ERR_INVALID_ARG, "w must be in [1, 255] (got %d)", w);
+  if (n_bases >= (1ULL << 31)) return fail(c, DNALN_ERR_INVALID_ARG, "reference is too large (limit: 2^31 bp)");
+  if (n_buckets < 1 || (n_buckets & (n_buckets - 1)) != 0 || n_buckets > (1ULL << 34))
+    return fail(c, DNALN_ERR_INVALID_ARG, "n_buckets must be a power of two (got %llu)",
+                static_cast<unsigned long long>(n_buckets));
+  if (n_pos >= (1ULL << 32)) return fail(c, DNALN_ERR_INVALID_ARG, "too many positions");
+  if (int e = check_contigs(c, contig_off, contig_len, n_contigs, n_bases, DNALN_ERR_INVALID_ARG)) return e;
+  if (int e = set_device(c)) return e;
+  // the table in the device layout, checked as it is packed
+  std::vector<ulonglong2> t(static_cast<size_t>(n_buckets));
+  for (size_t i = 0; i < t.size(); ++i)
+    t[i] = make_ulonglong2(keys[i], keys[i] == kInvalidHash
+                                        ? 0ull
+                                        : (static_cast<uint64_t>(offsets[i]) | static_cast<uint64_t>(counts[i]) << 32));
+  TableCheck tc;
+  tc.n_pos = n_pos;
+  tc.n_bases = n_bases;
+  tc.buckets(t.data(), t.size());
+  tc.positions(positions, static_cast<size_t>(n_pos));
+  if (!tc.ok) return fail(c, DNALN_ERR_INVALID_ARG, "a bucket or position lies outside the positions or the genome");
+  if (tc.n_keys >= n_buckets) return fail(c, DNALN_ERR_INVALID_ARG, "the table has no empty bucket");
+  IndexRes r;
+  r.mem = std::make_shared<IndexMem>();
+  r.device = c->device;
+  IndexMem& m = *r.mem;
+  int e = DNALN_OK;
+  if ((e = dalloc(c, m.genome, n_bases)) || (e = dalloc(c, m.coff, n_contigs * sizeof(uint64_t))) ||
+      (e = dalloc(c, m.clen, n_contigs * sizeof(uint32_t))) || (e = dalloc(c, m.table, t.size() * sizeof(ulonglong2))) ||
+      (e = dalloc(c, m.positions, n_pos * sizeof(uint32_t))))
+    return e;
+  CK(cudaMemcpy(m.genome.p, genome, n_bases, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m.coff.p, contig_off, n_contigs * sizeof(uint64_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m.clen.p, contig_len, n_contigs * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m.table.p, t.data(), t.size() * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+  if (n_pos) CK(cudaMemcpy(m.positions.p, positions, n_pos * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  uint2* runs = nullptr;
+  int32_t n_runs = 0;
+  char why[256] = {};
+  e = find_n_runs_on_device(c->st, static_cast<const uint8_t*>(m.genome.p), n_bases, &runs, &n_runs, why, sizeof why);
+  m.nruns = DevBuf{runs, static_cast<size_t>(n_runs) * sizeof(uint2)};
+  if (e != DNALN_OK) return fail(c, e, "%s", why);
+  r.n_keys = tc.n_keys;
+  r.n_pos = n_pos;
+  r.n_buckets = n_buckets;
+  r.n_bases = n_bases;
+  r.max_count = tc.max_count;
+  r.n_contigs = n_contigs;
+  r.k = k;
+  r.w = w;
+  register_index(c, r, n_buckets - 1, n_runs, index_id);
   return DNALN_OK;
 }
 

@@ -216,6 +216,59 @@ inline unsigned blocks_for(int64_t n, int t = 256) { return static_cast<unsigned
 
 }  // namespace
 
+int find_n_runs_on_device(cudaStream_t st, const uint8_t* d_genome, uint64_t n_bases, uint2** runs_out,
+                          int32_t* n_runs_out, char* err, size_t err_len) {
+  *runs_out = nullptr;
+  *n_runs_out = 0;
+  auto failed = [&](cudaError_t e) {
+    snprintf(err, err_len, "index (N runs): %s", cudaGetErrorString(e));
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? DNALN_ERR_OOM : DNALN_ERR_CUDA;
+  };
+  Scratch tmp;
+  cudaError_t e = cudaSuccess;
+  uint8_t* is_start = tmp.get<uint8_t>(n_bases, e);
+  uint8_t* is_end = tmp.get<uint8_t>(n_bases, e);
+  int64_t* d_nr = tmp.get<int64_t>(2, e);
+  if (e != cudaSuccess) return failed(e);
+  int64_t n_runs = 0;
+  int64_t* starts = nullptr;
+  int64_t* ends = nullptr;
+  if (n_bases) {
+    k_nrun_flags<<<blocks_for(static_cast<int64_t>(n_bases)), 256, 0, st>>>(d_genome, static_cast<int64_t>(n_bases),
+                                                                            is_start, is_end);
+    size_t cb = 0;  // the number of runs first, so that their arrays are sized exactly
+    if ((e = cub::DeviceReduce::Sum(nullptr, cb, is_start, d_nr, static_cast<int64_t>(n_bases), st)) != cudaSuccess)
+      return failed(e);
+    void* d_cb = tmp.get<uint8_t>(cb, e);
+    if (e == cudaSuccess) e = cub::DeviceReduce::Sum(d_cb, cb, is_start, d_nr, static_cast<int64_t>(n_bases), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&n_runs, d_nr, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    starts = tmp.get<int64_t>(n_runs, e);
+    ends = tmp.get<int64_t>(n_runs, e);
+    if (e != cudaSuccess) return failed(e);
+    thrust::counting_iterator<int64_t> idx(0);
+    size_t fb = 0;
+    if ((e = cub::DeviceSelect::Flagged(nullptr, fb, idx, is_start, starts, d_nr, static_cast<int64_t>(n_bases),
+                                        st)) != cudaSuccess)
+      return failed(e);
+    void* d_fb = tmp.get<uint8_t>(fb, e);
+    if (e == cudaSuccess)
+      e = cub::DeviceSelect::Flagged(d_fb, fb, idx, is_start, starts, d_nr, static_cast<int64_t>(n_bases), st);
+    if (e == cudaSuccess)
+      e = cub::DeviceSelect::Flagged(d_fb, fb, idx, is_end, ends, d_nr + 1, static_cast<int64_t>(n_bases), st);
+    if (e != cudaSuccess) return failed(e);
+  }
+  uint2* runs = nullptr;
+  if ((e = cudaMalloc(&runs, (n_runs ? n_runs : 1) * sizeof(uint2))) != cudaSuccess) return failed(e);
+  *runs_out = runs;
+  *n_runs_out = static_cast<int32_t>(n_runs);
+  if (n_runs) k_nrun_pack<<<blocks_for(n_runs), 256, 0, st>>>(starts, ends, n_runs, runs);
+  // the scratch is freed on return: the pack must be done with it first
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess) return failed(e);
+  return DNALN_OK;
+}
+
 int build_index_on_device(cudaStream_t st, const uint8_t* d_genome, uint64_t n_bases, const uint64_t* contig_off,
                           const uint32_t* contig_len, int32_t n_contigs, int k, int w, DeviceIndexBuild* out,
                           char* err, size_t err_len) {
@@ -334,43 +387,10 @@ int build_index_on_device(cudaStream_t st, const uint8_t* d_genome, uint64_t n_b
   if (n_keys) k_place_keys<<<blocks_for(n_keys), 256, 0, st>>>(keys, n_keys, cap - 1, slot_rank, d_err);
   k_fill_table<<<blocks_for(static_cast<int64_t>(cap)), 256, 0, st>>>(slot_rank, cap, keys, offs, counts, table);
   // 5. runs of non-ACGT codes
-  uint8_t* is_start = tmp.get<uint8_t>(n_bases, e);
-  uint8_t* is_end = tmp.get<uint8_t>(n_bases, e);
-  int64_t* d_nr = tmp.get<int64_t>(2, e);
-  if (e != cudaSuccess) return failed("N runs", e);
-  int64_t n_runs = 0;
-  int64_t* starts = nullptr;
-  int64_t* ends = nullptr;
-  if (n_bases) {
-    k_nrun_flags<<<blocks_for(static_cast<int64_t>(n_bases)), 256, 0, st>>>(d_genome, static_cast<int64_t>(n_bases),
-                                                                            is_start, is_end);
-    size_t cb = 0;  // the number of runs first, so that their arrays are sized exactly
-    if ((e = cub::DeviceReduce::Sum(nullptr, cb, is_start, d_nr, static_cast<int64_t>(n_bases), st)) != cudaSuccess)
-      return failed("N runs", e);
-    void* d_cb = tmp.get<uint8_t>(cb, e);
-    if (e == cudaSuccess) e = cub::DeviceReduce::Sum(d_cb, cb, is_start, d_nr, static_cast<int64_t>(n_bases), st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&n_runs, d_nr, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    starts = tmp.get<int64_t>(n_runs, e);
-    ends = tmp.get<int64_t>(n_runs, e);
-    if (e != cudaSuccess) return failed("N runs", e);
-    thrust::counting_iterator<int64_t> idx(0);
-    size_t fb = 0;
-    if ((e = cub::DeviceSelect::Flagged(nullptr, fb, idx, is_start, starts, d_nr, static_cast<int64_t>(n_bases),
-                                        st)) != cudaSuccess)
-      return failed("N runs", e);
-    void* d_fb = tmp.get<uint8_t>(fb, e);
-    if (e == cudaSuccess)
-      e = cub::DeviceSelect::Flagged(d_fb, fb, idx, is_start, starts, d_nr, static_cast<int64_t>(n_bases), st);
-    if (e == cudaSuccess)
-      e = cub::DeviceSelect::Flagged(d_fb, fb, idx, is_end, ends, d_nr + 1, static_cast<int64_t>(n_bases), st);
-    if (e != cudaSuccess) return failed("N runs", e);
+  {
+    const int en = find_n_runs_on_device(st, d_genome, n_bases, &out->n_runs, &out->n_n_runs, err, err_len);
+    if (en != DNALN_OK) return en;
   }
-  uint2* runs = nullptr;
-  if (cudaMalloc(&runs, (n_runs ? n_runs : 1) * sizeof(uint2)) != cudaSuccess) return failed("N runs", cudaErrorMemoryAllocation);
-  out->n_runs = runs;
-  out->n_n_runs = static_cast<int32_t>(n_runs);
-  if (n_runs) k_nrun_pack<<<blocks_for(n_runs), 256, 0, st>>>(starts, ends, n_runs, runs);
   uint32_t h_err = 0;
   if ((e = cudaMemcpyAsync(&h_err, d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st)) != cudaSuccess || (e = cudaGetLastError()) != cudaSuccess)

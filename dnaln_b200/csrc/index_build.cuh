@@ -28,4 +28,10 @@ int build_index_on_device(cudaStream_t st, const uint8_t* d_genome, uint64_t n_b
                           const uint32_t* contig_len, int32_t n_contigs, int k, int w, DeviceIndexBuild* out,
                           char* err, size_t err_len);
 
+// The maximal runs [x, y) of non-ACGT codes (> 3) of the resident genome d_genome[0,
+// n_bases), ascending, into a new device array *runs (the caller frees it, also when the
+// call fails after setting it); synchronises st. Returns DNALN_OK or a DNALN_ERR_* code.
+int find_n_runs_on_device(cudaStream_t st, const uint8_t* d_genome, uint64_t n_bases, uint2** runs, int32_t* n_runs,
+                          char* err, size_t err_len);
+
 }  // namespace dnb

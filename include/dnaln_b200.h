@@ -32,6 +32,7 @@ extern "C" {
 #define DNALN_ERR_NO_DEVICE 5    /* no usable CUDA device */
 #define DNALN_ERR_DEVICE 6       /* a kernel reported an internal inconsistency (error flag) */
 #define DNALN_ERR_NOT_FOUND 7    /* unknown index id */
+#define DNALN_ERR_IO 8           /* an index image file could not be written, read or verified */
 
 typedef struct dnaln_ctx dnaln_ctx;
 
@@ -172,6 +173,27 @@ int dnaln_gpu_index_stats(const dnaln_ctx* ctx, int32_t index_id, uint64_t out6[
 int dnaln_gpu_index_export(dnaln_ctx* ctx, int32_t index_id, uint64_t* keys, uint32_t* offsets, uint32_t* counts,
                            uint32_t* positions);
 int dnaln_gpu_index_free(dnaln_ctx* ctx, int32_t index_id);
+/* A resident index with its genome as an image file at path: a header (k, w, sizes), the
+ * contig table, the genome codes, the bucket table, the positions and the N runs, in the
+ * device layout, with a 64-bit checksum of the contents. Written to path + ".tmp" and
+ * renamed, so a reader never sees half a file. dnaln_gpu_index_load reads an image back
+ * into a new resident index (no rebuild: the serving loop's index admission); the header,
+ * every bucket's offset + count, every position and the checksum are checked before the
+ * index is usable (DNALN_ERR_IO for a file that does not check out). The reference keeps
+ * no index on disk (src/main.cpp:33-35 builds it per run); the image is this library's. */
+int dnaln_gpu_index_save(dnaln_ctx* ctx, int32_t index_id, const char* path);
+int dnaln_gpu_index_load(dnaln_ctx* ctx, const char* path, int32_t* index_id);
+/* A new resident index from a table built on the host in the reference's layout
+ * (MinimizerIndex after build, src/index.hpp:49-56): n_buckets (a power of two, at least
+ * one bucket empty) buckets of keys (~0 = empty) / offsets / counts into positions[n_pos]
+ * (pos << 1 | strand), with the genome and contig table as for dnaln_gpu_index_build.
+ * The caller that already holds a MinimizerIndex uploads it instead of rebuilding it.
+ * Offsets + counts, positions and the contig table are checked (DNALN_ERR_INVALID_ARG);
+ * that the table is the one build() makes for (genome, k, w) is the caller's promise. */
+int dnaln_gpu_index_upload(dnaln_ctx* ctx, const uint8_t* genome, uint64_t n_bases, const uint64_t* contig_off,
+                           const uint32_t* contig_len, int32_t n_contigs, int32_t k, int32_t w, const uint64_t* keys,
+                           const uint32_t* offsets, const uint32_t* counts, uint64_t n_buckets,
+                           const uint32_t* positions, uint64_t n_pos, int32_t* index_id);
 /* Makes index src_id of context src (same device) usable by context dst under the new id
  * *dst_id, without copying it: several contexts (one per host thread, or the lanes of a
  * server below) map against one resident copy. The memory is freed when the last context
