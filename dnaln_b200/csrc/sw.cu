@@ -147,6 +147,19 @@ struct NibbleCodes {
   }
 };
 
+// The bytes p[0..7] as one little-endian word, from the aligned 8-byte word holding p[0]
+// and, unless p is aligned, the next one. Each of the two holds at least one of the eight
+// bytes asked for, so neither lies outside the pages those bytes are in.
+__device__ __forceinline__ uint64_t load8u(const uint8_t* p) {
+  static_assert(kAhead == 8, "one 8-byte word per block of the diagonal run");
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uint64_t* w = reinterpret_cast<const uint64_t*>(a & ~static_cast<uintptr_t>(7));
+  const unsigned sh = static_cast<unsigned>(a & 7) * 8u;
+  const uint64_t lo = __ldg(w);
+  if (sh == 0) return lo;
+  return (lo >> sh) | (__ldg(w + 1) << (64u - sh));
+}
+
 // Walks the direction codes back from (bi, bd) (src/align.cpp:87-143). CIGAR ops are
 // written in walk order (last op first), adjacent equal ops merged as the reference's
 // push() does. Guards flag, and never read, a cell outside the band.
@@ -175,14 +188,28 @@ __device__ void traceback(const Codes& code, int W, int bi, int bd, int best, co
     while (!stop && i >= 0 && v > 0) {
       uint32_t cx[kAhead];
       int qa[kAhead], ta[kAhead];
+      const int64_t x0 = tk.t_start + (i - (kAhead - 1)) + d;  // target of row i - 7
+      if (i >= kAhead - 1 && x0 >= tk.t_lo && x0 + kAhead <= tk.t_hi) {
+        // the block's 8 query and 8 target bytes are contiguous: two 8-byte words each
+        // instead of 16 byte loads (the walk is bound by its L1 requests)
+        const uint64_t qw = load8u(q + i - (kAhead - 1)), tw = load8u(tbase + x0);
 #pragma unroll
-      for (int k = 0; k < kAhead; ++k) {
-        cx[k] = 0;
-        qa[k] = ta[k] = 0;
-        if (i - k >= 0) {
+        for (int k = 0; k < kAhead; ++k) {
           cx[k] = code(i - k, d);
-          qa[k] = q[i - k];
-          ta[k] = static_cast<int>(tcode(tbase, tk, static_cast<int64_t>(i - k) + d));
+          qa[k] = static_cast<int>((qw >> (8 * (kAhead - 1 - k))) & 0xFFu);
+          const int t8 = static_cast<int>((tw >> (8 * (kAhead - 1 - k))) & 0xFFu);
+          ta[k] = t8 > 3 ? 4 : t8;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k) {
+          cx[k] = 0;
+          qa[k] = ta[k] = 0;
+          if (i - k >= 0) {
+            cx[k] = code(i - k, d);
+            qa[k] = q[i - k];
+            ta[k] = static_cast<int>(tcode(tbase, tk, static_cast<int64_t>(i - k) + d));
+          }
         }
       }
 #pragma unroll
