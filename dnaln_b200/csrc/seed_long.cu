@@ -240,7 +240,12 @@ __global__ void __launch_bounds__(kLT)
       // dominant direction first (a reverse-strand read's anchors arrive descending), then
       // insertion sort within a budget of moves that colinear sets never reach
       int desc = 0;
-      for (int a = 1; a < na; ++a) desc += key_ld(a) < key_ld(a - 1);
+      uint64_t kprev = key_ld(0);
+      for (int a = 1; a < na; ++a) {
+        const uint64_t kc = key_ld(a);
+        desc += kc < kprev;
+        kprev = kc;
+      }
       if (2 * desc > na - 1) {
         for (int a = 0, b2 = na - 1; a < b2; ++a, --b2) {
           const uint64_t t0 = key_ld(a);
@@ -248,16 +253,27 @@ __global__ void __launch_bounds__(kLT)
           key_st(b2, t0);
         }
       }
+      // The key at position i-1 is kept in a register and key i+1 is loaded while key i is
+      // placed: an anchor already in order costs no wait.
       int budget = 8 * na + 64;
+      uint64_t last = key_ld(0), v_next = na > 1 ? key_ld(1) : 0;
       for (int i = 1; i < na && !big; ++i) {
-        const uint64_t v = key_ld(i);
-        int j = i - 1;
-        while (j >= 0) {
-          const uint64_t y = key_ld(j);
-          if (y <= v) break;
-          key_st(j + 1, y);
-          --j;
-          if (--budget < 0) break;
+        const uint64_t v = v_next;
+        if (i + 1 < na) v_next = key_ld(i + 1);
+        if (last <= v) {  // in place
+          last = v;
+          continue;
+        }
+        key_st(i, last);  // the key at i-1 moves up; it is the key at i from here on
+        int j = i - 2;
+        if (--budget >= 0) {
+          while (j >= 0) {
+            const uint64_t y = key_ld(j);
+            if (y <= v) break;
+            key_st(j + 1, y);
+            --j;
+            if (--budget < 0) break;
+          }
         }
         key_st(j + 1, v);
         if (budget < 0) big = true;
@@ -266,21 +282,31 @@ __global__ void __launch_bounds__(kLT)
     if (!big && na > 0) {
       // ---- DP (src/chain.cpp:22-45) with the prefix-max cutoff: a predecessor j' <= j
       // scores at most max(f[0..j]) + k, so the scan stops once that cannot beat best
+      // Anchors i-1 and i-2 (key words and DP word) stay in registers and anchor i+1's
+      // key is loaded while row i runs: with the cutoff the scan rarely reaches farther,
+      // so a row waits on no load of its own.
       const uint32_t max_gap = static_cast<uint32_t>(cp.max_gap);
       int pm = 0;
+      uint32_t h1 = 0, q1 = 0, w1 = 0, h2 = 0, q2 = 0, w2 = 0;
+      uint32_t h_next = A(0), q_next = A(1);
       for (int i = 0; i < na; ++i) {
-        const uint32_t hi_i = A(2 * i);
-        const int32_t qi = static_cast<int32_t>(A(2 * i + 1));
+        const uint32_t hi_i = h_next;
+        const int32_t qi = static_cast<int32_t>(q_next);
+        if (i + 1 < na) {
+          h_next = A(2 * (i + 1));
+          q_next = A(2 * (i + 1) + 1);
+        }
         int best = k, bj = -1;
         const int lo = i - cp.lookback > 0 ? i - cp.lookback : 0;
         for (int j = i - 1; j >= lo; --j) {
-          const uint32_t wj = B(2 * j);
+          const bool r1 = j == i - 1, r2 = j == i - 2;
+          const uint32_t wj = r1 ? w1 : (r2 ? w2 : B(2 * j));
           if (static_cast<int>(wj >> 16) + k <= best) break;
-          const uint32_t hi_j = A(2 * j);
+          const uint32_t hi_j = r1 ? h1 : (r2 ? h2 : A(2 * j));
           if ((hi_i ^ hi_j) >> 31) break;  // strand change
           const uint32_t dr = hi_i - hi_j;
           if (dr > max_gap) break;
-          const int32_t dq = qi - static_cast<int32_t>(A(2 * j + 1));
+          const int32_t dq = qi - static_cast<int32_t>(r1 ? q1 : (r2 ? q2 : A(2 * j + 1)));
           if (dr == 0 || dq <= 0) continue;
           const int32_t dri = static_cast<int32_t>(dr);
           const int32_t dd = dri > dq ? dri - dq : dq - dri;
@@ -294,8 +320,15 @@ __global__ void __launch_bounds__(kLT)
           }
         }
         pm = best > pm ? best : pm;
-        B(2 * i) = static_cast<uint32_t>(best) | static_cast<uint32_t>(pm) << 16;
+        const uint32_t wi = static_cast<uint32_t>(best) | static_cast<uint32_t>(pm) << 16;
+        B(2 * i) = wi;
         B(2 * i + 1) = static_cast<uint32_t>(bj + 1);
+        h2 = h1;
+        q2 = q1;
+        w2 = w1;
+        h1 = hi_i;
+        q1 = static_cast<uint32_t>(qi);
+        w1 = wi;
       }
       // ---- chains (src/chain.cpp:47-68): walks from each anchor in (f desc, index asc)
       // order, skipping used ones. The order is sorted by insertion after reversing
@@ -304,16 +337,25 @@ __global__ void __launch_bounds__(kLT)
       const auto ord = [&](int e) -> uint32_t& { return B(2 * kLMaxAnc + 4 * kLMaxChains + e); };
       for (int i = 0; i < na; ++i)
         ord(na - 1 - i) = (0xFFFu - (B(2 * i) & 0xFFFu)) << 16 | static_cast<uint32_t>(i);
-      int budget2 = 8 * na + 64;
+      int budget2 = 8 * na + 64;  // the same register-cached insertion as the key sort
+      uint32_t olast = ord(0), o_next = na > 1 ? ord(1) : 0u;
       for (int i = 1; i < na && !big; ++i) {
-        const uint32_t v = ord(i);
-        int j = i - 1;
-        while (j >= 0) {
-          const uint32_t y = ord(j);
-          if (y <= v) break;
-          ord(j + 1) = y;
-          --j;
-          if (--budget2 < 0) break;
+        const uint32_t v = o_next;
+        if (i + 1 < na) o_next = ord(i + 1);
+        if (olast <= v) {
+          olast = v;
+          continue;
+        }
+        ord(i) = olast;
+        int j = i - 2;
+        if (--budget2 >= 0) {
+          while (j >= 0) {
+            const uint32_t y = ord(j);
+            if (y <= v) break;
+            ord(j + 1) = y;
+            --j;
+            if (--budget2 < 0) break;
+          }
         }
         ord(j + 1) = v;
         if (budget2 < 0) big = true;
