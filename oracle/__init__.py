@@ -1,7 +1,7 @@
 """TEST INFRASTRUCTURE ONLY — the oracle of the mapping path.
 
 Two CPU implementations with one Python API, used by tests/, ``__graft_entry__.smoke()``
-and bench.py's CPU-baseline leg as the checker, never by the product:
+and bench.py's CPU-baseline leg to compare the CUDA path against, never by the product:
 
 * :class:`Port` — ``_oracle.so``, our plain-C restatement of the reference's algorithm
   (dnaln_oracle.c, each function citing the dnaln lines it follows);

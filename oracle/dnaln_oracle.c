@@ -1,6 +1,6 @@
 /* dnaln_oracle.c — TEST INFRASTRUCTURE ONLY. A plain-C restatement of dnaln's read-mapping
  * path (sketch -> index probe -> chain -> banded SW + traceback -> MAPQ), written for
- * clarity, not speed: it is the checker the CUDA path is compared against and the scalar
+ * clarity, not speed: it is the oracle the CUDA path is compared against and the scalar
  * CPU baseline. It is never linked into the product. Its agreement with the reference is
  * pinned by tests/test_oracle.py (against the reference built from its own sources in
  * oracle/_ref) and by the committed fixtures in tests/golden/.
