@@ -600,12 +600,15 @@ def run_ours(args) -> None:
     peak, peak_kind = measured_peaks()
     achieved = (algo / launches) / (avg_launch_ms / 1e3) / 1e9 if algo is not None else None
     traffic = None  # DRAM bytes per launch of this kernel from the committed ncu summary
+    issue_active = None  # its fraction of issue slots used, same capture
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         try:
-            traffic = json.loads(tf.read_text()).get(args.workload, {}).get(dom.split("<")[0])
-        except (OSError, ValueError):
-            traffic = None
+            prof = json.loads(tf.read_text())
+            traffic = prof.get(args.workload, {}).get(dom.split("<")[0])
+            issue_active = prof.get("issue_active", {}).get(args.workload, {}).get(dom.split("<")[0])
+        except (OSError, ValueError, AttributeError):
+            traffic = issue_active = None
     cells = st["cells"]
     sw_ms = st["ms_sw_score"] + st["ms_sw_tb"]
     kernels = {k: {"launches_per_step": n / PROFILE_STEPS, "ms_per_step": t / PROFILE_STEPS}
@@ -629,7 +632,10 @@ def run_ours(args) -> None:
                         "frac": achieved / peak if achieved is not None else None, "traffic": traffic,
                         "peak_kind": peak_kind,
                         "algorithmic_bytes_per_launch": algo / launches if algo is not None else None,
-                        "avg_launch_ms": avg_launch_ms, "launches_timed": launches},
+                        "avg_launch_ms": avg_launch_ms, "launches_timed": launches,
+                        "issue_active": issue_active,
+                        "issue_note": "fraction of the kernel's issue slots used, from the committed ncu capture "
+                                      "(profiles/): HBM is not what bounds these integer kernels"},
            "kernels": kernels, "kernels_note": f"untimed breakdown over {PROFILE_STEPS} steps, every launch traced",
            "stages_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
            "sw_gcups": cells / (sw_ms / 1e3) / 1e9 if sw_ms > 0 else None,
