@@ -148,10 +148,12 @@ def kernel_bytes(kernel: str, st: dict, mean_len: float, bw: int = 16) -> float 
     W = 2 * bw + 1
     cand_per_read = st["candidates"] / max(n, 1)
     dir_row = max((W + 3) // 4 * 2, (W + 7) // 8 * 4)  # direction-code bytes per query row
-    if kernel == "k_seed_chain_t":  # ASCII in, codes of both strands out, 16-B bucket per minimizer,
-        # 4-B occurrence per anchor, 21-B candidate out, 36 B of per-read offsets / lengths / counts
-        return n * mean_len * (1 + 2) + mins * 16 + (st["anchors"] - st["warp_anchors"]) * 4 + \
-            st["candidates"] * 21 + n * 36
+    if kernel == "k_seed_chain_t":  # ASCII in, 16-B bucket per minimizer, 4-B occurrence per anchor,
+        # 21-B candidate out, 28 B of per-read offsets / lengths / counts
+        return n * mean_len + mins * 16 + (st["anchors"] - st["warp_anchors"]) * 4 + \
+            st["candidates"] * 21 + n * 28
+    if kernel == "k_encode_reads":  # ASCII in, codes of both strands out, offsets / lengths
+        return n * mean_len * (1 + 2) + n * 20
     if kernel == "k_seed":        # ASCII in, codes of both strands out, 20-B minimizer slot out + 16-B bucket
         return n * mean_len * (1 + 2) + mins * (20 + 16) + n * 24
     if kernel == "k_seed<list>":  # listed reads: ASCII in (codes already written), slots out + buckets

@@ -615,9 +615,13 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
   int* warp_n = big_n;
   CK(cudaEventRecord(c->ev[kEvSeed0], st));
   if (thread_path) {
+    kt.begin(st, "k_encode_reads");
+    launch_encode_reads(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, codes);
+    kt.end(st);
+    c->stats.launches += 1;
     kt.begin(st, "k_seed_chain_t");
-    const bool ok = launch_seed_chain_thread(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, codes, ix.dev,
-                                             sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list, big_n, c->d_err);
+    const bool ok = launch_seed_chain_thread(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, n, ix.dev, sp, cp, cand,
+                                             cb, n_min, n_anchor, n_anc_t, big_list, big_n, c->d_err);
     kt.end(st);
     if (!ok) return fail(c, DNALN_ERR_CUDA, "thread-per-read seeding kernel could not be configured");
     if (c->long_thread && seed_long_supported(sp, cp) && max_len > seed_thread_max_len()) {

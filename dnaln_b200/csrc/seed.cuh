@@ -142,17 +142,22 @@ void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_l
                       const DevIndex& ix, const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as,
                       unsigned long long* pool_top, int64_t pool_cap, CandBuf cb, uint32_t* err);
 
+// Codes of both strands of reads [0, n) (seed_thread.cu): forward at codes[2*pofs[r]],
+// reverse complement right after it (src/mapper.cpp:88-99), from the ASCII reads.
+void launch_encode_reads(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+                         const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes);
+
 // One thread per read (seed_thread.cu): passes 1 and 2 of the reads the per-thread budgets
-// admit, writing codes of every read, candidates of the admitted ones, n_min, n_anc_t (their
-// anchor counts, for statistics) and n_anchor = 0 (no scratch); the others are appended
-// to big_list (count in *big_n, zeroed by the caller)
-// for launch_seed_list / launch_chain_map. Returns false, launching nothing, when the
-// parameters are outside the path's range.
+// admit, from their ASCII bytes (the codes in HBM are launch_encode_reads' job), writing
+// candidates of the admitted reads, n_min, n_anc_t (their anchor counts, for statistics)
+// and n_anchor = 0 (no scratch); the others are appended to big_list (count in *big_n,
+// zeroed by the caller) for launch_seed_list / launch_chain_map. Returns false, launching
+// nothing, when the parameters are outside the path's range.
 bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp);
 int seed_thread_max_len();  // the longest read the short thread kernel stages
 bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
-                              const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes,
-                              const DevIndex& ix, const SeedParams& sp, const ChainParamsDev& cp,
+                              const int32_t* seq_len, int64_t n, const DevIndex& ix, const SeedParams& sp,
+                              const ChainParamsDev& cp,
                               const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
                               int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err);
 

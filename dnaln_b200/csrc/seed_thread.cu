@@ -8,9 +8,12 @@
 // algorithms directly; the 32 reads of a warp advance in lockstep (same k-mer index, same
 // DP row), so the shared-memory layouts [slot][thread] are bank-conflict free.
 //
-//  * Staging: the warp encodes its 32 reads cooperatively (coalesced ASCII loads, forward
-//    and reverse-complement codes written coalesced, src/mapper.cpp:88-99) and leaves each
-//    read's codes, four per word, in shared memory for its thread.
+//  * Staging: the warp copies the ASCII bytes of its 32 reads into shared memory, each
+//    read's aligned words into its thread's column, with one batch of cp.async for all
+//    of them and one wait (one memory latency per warp, not one per group of reads); the
+//    sketch converts the bytes to codes as it reads them. The codes of both strands in
+//    HBM (src/mapper.cpp:88-99), which SW and the warp kernels read, are written by
+//    k_encode_reads, a bandwidth-bound kernel launched before this one.
 //  * Sketch (src/minimizer.cpp:5-68): rolling 2-bit forward / reverse-complement words,
 //    canonical strand, 32-bit hash (hash32); the window minimum of w keys (hash, position,
 //    strand) by van Herk / Gil-Werman blocks of w: a running prefix minimum of the current
@@ -32,6 +35,8 @@
 // when it is longer than kTMaxLen, has more than kTMaxMin minimizers, kTMaxAnc anchors or
 // kTMaxChains chains, or when the parameters are outside this path's range (see
 // seed_thread_supported).
+#include <algorithm>
+
 #include "common.cuh"
 #include "seed.cuh"
 
@@ -47,19 +52,18 @@ constexpr int kTMaxMin = 32;              // minimizers per read
 constexpr int kTMaxAnc = 32;              // anchors per read (one bit each in a 32-bit mask)
 constexpr int kTMaxChains = 8;            // chains per read passing the score / anchor filters
 constexpr int kTW = 10;                   // window length of the compiled sketch
-constexpr int kEncGroup = 4;              // reads whose bytes a warp loads at once
-constexpr int kEncPer = kTMaxLen / 32;    // byte positions per lane and staged read
 constexpr int kProbe = 8;                 // minimizers probed with independent loads at once
 
 // Dynamic shared memory of a block: two regions of 32-bit words, each thread owning one
 // column of each (word w of thread T at w * pitch + T), so that after the cooperative
-// encode no thread ever touches another thread's words. Region A (pitch kTPitch): the
-// staged codes, later the anchor keys (two words each). Region B (pitch kTT): the
+// staging no thread ever touches another thread's words. Region A (pitch kTPitch): the
+// staged ASCII words, later the anchor keys (two words each). Region B (pitch kTT): the
 // minimizers {hash, pos | strand << 31} (two words each), later f << 8 | (prev + 1) of
 // each anchor (words 0..31) and the chain table (words 32..63).
-constexpr int kWordsA = kTWords;
+constexpr int kWordsA = kTWords + 2;  // a read of kTMaxLen bytes at any offset within its first word
 constexpr int kWordsB = 64;
 static_assert(2 * kTMaxAnc <= kWordsA, "anchor keys must fit a staging column");
+static_assert((3 + kTMaxLen + 3) / 4 <= kWordsA, "a staged read must fit its column");
 static_assert(2 * kTMaxMin <= kWordsB && kTMaxAnc + 4 * kTMaxChains <= kWordsB, "region B column too small");
 constexpr int kRegionA = kWordsA * kTPitch * 4;
 constexpr int kRegionB = kWordsB * kTT * 4;
@@ -68,16 +72,45 @@ constexpr int kThreadSmem = kRegionA + kRegionB + (kTMaxBand + 1) * 4;
 
 __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return b < a ? b : a; }
 
+// 4-byte asynchronous copy global -> shared (both 4-byte aligned).
+__device__ __forceinline__ void cp_async4(uint32_t* dst_smem, const void* src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Codes of both strands of every read (src/mapper.cpp:88-99): forward at codes[2*pofs[r]],
+// reverse complement right after it. One warp per read (grid-stride), bytes in lane order
+// so loads and stores are coalesced.
+__global__ void __launch_bounds__(256)
+    k_encode_reads(const char* __restrict__ seq, const int64_t* __restrict__ seq_off, int64_t seq_base,
+                   const int32_t* __restrict__ seq_len, const int64_t* __restrict__ pofs, int64_t n,
+                   uint8_t* __restrict__ codes) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t r = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+    const int len = seq_len[r];
+    const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + (seq_off[r] - seq_base);
+    uint8_t* fw = codes + 2 * pofs[r];
+    uint8_t* rc = fw + len;
+#pragma unroll 4
+    for (int i = lane; i < len; i += 32) {
+      const uint8_t c = static_cast<uint8_t>(nt4(s[i]));
+      fw[i] = c;
+      rc[len - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
+    }
+  }
+}
+
 template <int W>
 __global__ void __launch_bounds__(kTT)
     k_seed_chain_t(const char* __restrict__ seq, const int64_t* __restrict__ seq_off, int64_t seq_base,
-                   const int32_t* __restrict__ seq_len, const int64_t* __restrict__ pofs, int64_t n,
-                   uint8_t* __restrict__ codes, DevIndex ix, SeedParams sp, ChainParamsDev cp, CandParams cand,
+                   const int32_t* __restrict__ seq_len, int64_t n, DevIndex ix, SeedParams sp, ChainParamsDev cp,
+                   CandParams cand,
                    CandBuf cb, int32_t* __restrict__ n_min, int64_t* __restrict__ n_anchor,
                    int32_t* __restrict__ n_anc_t, int32_t* __restrict__ big_list, int* __restrict__ big_n,
                    uint32_t* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem[];
-  uint32_t* const stg = reinterpret_cast<uint32_t*>(smem);  // region A (all columns, for the encode)
+  uint32_t* const stg = reinterpret_cast<uint32_t*>(smem);  // region A (all columns, for the staging)
   int32_t* const lut = reinterpret_cast<int32_t*>(smem + kRegionA + kRegionB);  // chaining gap costs
   const int T = threadIdx.x, lane = T & 31;
   for (int d = T; d <= cp.band; d += kTT) lut[d] = cp.cost[d];
@@ -103,60 +136,28 @@ __global__ void __launch_bounds__(kTT)
   const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kTT + (T & ~31);  // first read of this warp
   const int64_t r = r0 + lane;
   int len = 0;
-  int64_t soff = 0, po = 0;
+  uint64_t a_word = 0;  // this read's first ASCII byte rounded down to a 4-byte boundary
+  int offb = 0, nwords = 0;
   if (r < n) {
     len = seq_len[r];
-    soff = seq_off[r] - seq_base;
-    po = pofs[r];
+    const uint64_t a = reinterpret_cast<uint64_t>(seq) + static_cast<uint64_t>(seq_off[r] - seq_base);
+    offb = static_cast<int>(a & 3u);
+    a_word = a - static_cast<uint64_t>(offb);
+    if (len > 0 && len <= kTMaxLen) nwords = (offb + len + 3) >> 2;
   }
 
-  // ---- cooperative encode: codes of both strands to HBM, staged codes to shared memory.
-  // Reads go in groups of kEncGroup; all byte loads of a group (coalesced across the lanes)
-  // are issued before any is used, so the group costs one memory latency, not one per byte
-  // position.
-  uint8_t* const st8 = reinterpret_cast<uint8_t*>(stg);
-  for (int j0 = 0; j0 < 32; j0 += kEncGroup) {
-    if (r0 + j0 >= n) break;
-    uint32_t by[kEncGroup][kEncPer];
-    int lg[kEncGroup];
-    int64_t sg[kEncGroup], pg[kEncGroup];
-#pragma unroll
-    for (int q = 0; q < kEncGroup; ++q) {
-      lg[q] = __shfl_sync(0xffffffffu, len, j0 + q);  // 0 past the batch
-      sg[q] = __shfl_sync(0xffffffffu, soff, j0 + q);
-      pg[q] = __shfl_sync(0xffffffffu, po, j0 + q);
-      const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + sg[q];
-#pragma unroll
-      for (int u = 0; u < kEncPer; ++u) {
-        const int i = lane + 32 * u;
-        by[q][u] = i < lg[q] ? s[i] : 0u;
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < kEncGroup; ++q) {
-      const int lj = lg[q];
-      const int tj = (T & ~31) + j0 + q;
-      uint8_t* fw = codes + 2 * pg[q];
-      uint8_t* rc = fw + lj;
-      const bool stage = lj <= kTMaxLen;
-#pragma unroll
-      for (int u = 0; u < kEncPer; ++u) {
-        const int i = lane + 32 * u;
-        if (i < lj) {
-          const uint8_t c = static_cast<uint8_t>(nt4(by[q][u]));
-          fw[i] = c;
-          rc[lj - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
-          if (stage) st8[((i >> 2) * kTPitch + tj) * 4 + (i & 3)] = c;
-        }
-      }
-      const uint8_t* s = reinterpret_cast<const uint8_t*>(seq) + sg[q];
-      for (int i = lane + 32 * kEncPer; i < lj; i += 32) {  // the rest of a read too long to stage
-        const uint8_t c = static_cast<uint8_t>(nt4(s[i]));
-        fw[i] = c;
-        rc[lj - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
-      }
-    }
+  // ---- staging: word w of read j's ASCII (from its aligned start) into word w of column j.
+  // Every copied word holds at least one byte of its read, so it lies in the pages the
+  // read is in. All copies of the warp are in flight before the one wait.
+  for (int j = 0; j < 32; ++j) {
+    const uint64_t aj = __shfl_sync(0xffffffffu, a_word, j);
+    const int nwj = __shfl_sync(0xffffffffu, nwords, j);
+    const int tj = (T & ~31) + j;
+    for (int w = lane; w < nwj; w += 32)
+      cp_async4(stg + w * kTPitch + tj, reinterpret_cast<const void*>(aj + 4u * static_cast<uint64_t>(w)));
   }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncwarp();
   if (r >= n) return;
 
@@ -170,8 +171,9 @@ __global__ void __launch_bounds__(kTT)
     uint32_t fwd = 0, rev = 0, wcur = 0;
     int run = 0;
     auto roll = [&](int i) {  // consumes code i (called with i = 0, 1, 2, ...)
-      if ((i & 3) == 0) wcur = ca[(i >> 2) * kTPitch];
-      const uint32_t c = (wcur >> (8 * (i & 3))) & 0xFFu;
+      const int jb = i + offb;  // byte of the staged words
+      if ((jb & 3) == 0 || i == 0) wcur = ca[(jb >> 2) * kTPitch];
+      const uint32_t c = nt4((wcur >> (8 * (jb & 3))) & 0xFFu);
       run = c < 4 ? run + 1 : 0;
       fwd = ((fwd << 2) | (c & 3u)) & mask2k;
       rev = (rev >> 2) | ((3u - (c & 3u)) << (2 * k - 2));
@@ -444,9 +446,16 @@ bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp) {
          cp.band <= kTMaxBand && cp.lookback >= 0;
 }
 
+void launch_encode_reads(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+                         const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes) {
+  if (n <= 0) return;
+  const int64_t blocks = std::min<int64_t>((n + 7) / 8, 148 * 16);  // 8 warps a block, grid-stride
+  k_encode_reads<<<static_cast<unsigned>(blocks), 256, 0, st>>>(seq, seq_off, seq_base, seq_len, pofs, n, codes);
+}
+
 bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
-                              const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes,
-                              const DevIndex& ix, const SeedParams& sp, const ChainParamsDev& cp,
+                              const int32_t* seq_len, int64_t n, const DevIndex& ix, const SeedParams& sp,
+                              const ChainParamsDev& cp,
                               const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
                               int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err) {
   if (!seed_thread_supported(sp, cp)) return false;
@@ -462,8 +471,7 @@ bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* s
   }
   const int64_t blocks = (n + kTT - 1) / kTT;
   k_seed_chain_t<kTW><<<static_cast<unsigned>(blocks), kTT, kThreadSmem, st>>>(
-      seq, seq_off, seq_base, seq_len, pofs, n, codes, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list,
-      big_n, err);
+      seq, seq_off, seq_base, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list, big_n, err);
   return true;
 }
 
