@@ -319,7 +319,8 @@ def text_pipeline(ctx, iid, reads, g, p, steps: int) -> dict:
     no copies in between: dnaln_parse_reads on all host threads, the host-buffer mapping
     call on the parsed arrays in batches of 262,144 (submit / wait, so one batch's copies
     overlap the next one's kernels), dnaln_sam_format_mt on all host threads into one
-    reused buffer. Wall clock per step, the three parts one after another."""
+    reused buffer, each batch as soon as it is mapped while the later ones map. Wall clock
+    per step."""
     import tempfile
 
     import dnaln_b200 as D
@@ -362,12 +363,14 @@ def text_pipeline(ctx, iid, reads, g, p, steps: int) -> dict:
             if rc:
                 raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
             tickets.append(t.value)
-        for t in tickets:
-            if L.dnaln_gpu_map_wait(ctx.handle, t):
-                raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
-        t2 = time.perf_counter()
+        # batch k is formatted as soon as it is mapped, while the later batches map
         out_at = 0
+        wait_s = 0.0
         for k, (a, b) in enumerate(spans):
+            tw = time.perf_counter()
+            if L.dnaln_gpu_map_wait(ctx.handle, tickets[k]):
+                raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
+            wait_s += time.perf_counter() - tw
             u = C.c_int64()
             rc = L.dnaln_sam_format_mt(seq, so + 8 * a, sl + 4 * a, nm, no + 8 * a, ql, qo + 8 * a, recs[k].ctypes.data,
                                        cigs[k].ctypes.data, b - a, cn.ctypes.data, co.ctypes.data, threads,
@@ -379,15 +382,17 @@ def text_pipeline(ctx, iid, reads, g, p, steps: int) -> dict:
         L.dnaln_reads_free(h)
         if step:
             t_parse += t1 - t0
-            t_map += t2 - t1
-            t_sam += t3 - t2
+            t_map += wait_s
+            t_sam += (t3 - t1) - wait_s
             sam_bytes = out_at
     total = t_parse + t_map + t_sam
     return {"value": steps * n_all / total, "unit": METRIC, "host_threads": threads,
-            "ms_per_step": {"parse": 1e3 * t_parse / steps, "map": 1e3 * t_map / steps, "sam": 1e3 * t_sam / steps},
+            "ms_per_step": {"parse": 1e3 * t_parse / steps, "map_wait": 1e3 * t_map / steps,
+                            "sam_and_submit": 1e3 * t_sam / steps},
             "text_bytes_in": int(len(text)), "sam_bytes_out": int(sam_bytes),
-            "what": "FASTQ text in memory -> dnaln_parse_reads -> dnaln_gpu_map_submit/wait on the parsed "
-                    "(pageable) arrays -> dnaln_sam_format_mt -> SAM text in memory; wall clock, parts in sequence"}
+            "what": "FASTQ text in memory -> dnaln_parse_reads -> dnaln_gpu_map_submit on the parsed (pageable) "
+                    "arrays -> per batch dnaln_gpu_map_wait then dnaln_sam_format_mt while the later batches map "
+                    "-> SAM text in memory; wall clock per step (map_wait = time the host waited for the GPU)"}
 
 
 def run_ours(args) -> None:
