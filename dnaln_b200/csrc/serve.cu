@@ -430,6 +430,10 @@ int dnaln_serve_create(dnaln_ctx* home, const dnaln_serve_params* sp, dnaln_serv
     if (e == DNALN_OK && cudaStreamCreateWithFlags(&L->st, cudaStreamNonBlocking) != cudaSuccess) e = DNALN_ERR_CUDA;
     if (e == DNALN_OK) e = dnaln_gpu_set_stream(L->ctx, L->st);
     if (e == DNALN_OK) e = dnaln_gpu_set_option(L->ctx, "dir_cap_bytes", dir_cap);
+    // a server's batches are made of whatever requests are waiting, so a batch shape
+    // seldom repeats: lanes launch kernel by kernel instead of paying a graph capture on
+    // the latency path of every shape seen twice
+    if (e == DNALN_OK) e = dnaln_gpu_set_option(L->ctx, "graphs", 0);
     if (e != DNALN_OK) {
       release_lane(*L);
       for (auto& l : s->lanes) release_lane(*l);

@@ -295,7 +295,8 @@ int dnaln_gpu_map_batch_device(dnaln_ctx* ctx, int32_t index_id, const char* d_s
  * the next batch, and the lanes' batches overlap on the device. A batch takes reads while
  * its estimated device footprint fits the lane's share of the HBM budget. Every request's
  * records and CIGARs are those dnaln_gpu_map_batch gives for it alone (mapping is per
- * read, so batch composition cannot change a result). */
+ * read, so batch composition cannot change a result). Lanes do not capture CUDA graphs
+ * (option "graphs" 0): batch shapes seldom repeat in serving. */
 typedef struct dnaln_server dnaln_server;
 typedef struct {
   int32_t lanes;             /* concurrent batches on the device (0 = 3) */
