@@ -91,7 +91,13 @@ __global__ void __launch_bounds__(kLT)
   };
   const int m_list = *list_n;
   const int k = sp.k;
-  for (int64_t x = tid; x < m_list; x += stride) {
+  // Serpentine order over the (longest-first) list: round j takes positions
+  // [j*stride, (j+1)*stride), forward on even rounds and reversed on odd ones, so the
+  // thread with the longest read of one round gets the shortest of the next. The
+  // kernel is one resident wave and lasts as long as its slowest warp.
+  for (int64_t round = 0;; ++round) {
+    const int64_t x = (round & 1) ? (round + 1) * stride - 1 - tid : round * stride + tid;
+    if (x >= m_list) break;  // every later round's position is further still
     const int64_t r = list[x];
     const int len = seq_len[r];
     if (len <= min_len) {  // listed for its anchors, not its length: the warp kernels are faster there
