@@ -1250,6 +1250,15 @@ int dnaln_gpu_ctx_create(int device, dnaln_ctx** out) {
     if (x != cudaSuccess && e == DNALN_OK) e = fail(c, DNALN_ERR_CUDA, "%s", cudaGetErrorString(x));
   };
   bad(cudaSetDevice(device));
+  {  // direction-code scratch: 1/32 of the device's memory, in [1, 8] GiB, so that a
+     // traceback launch over long reads and wide bands still holds enough tasks to fill
+     // the SMs (1 GiB held ~16,000 1,000-row tasks at W = 129: ~1.7 blocks per SM)
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess)
+      c->dir_cap_bytes = std::min<size_t>(size_t(8) << 30, std::max<size_t>(size_t(1) << 30, prop.totalGlobalMem / 32));
+    else
+      cudaGetLastError();
+  }
   bad(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
   c->st = c->own;
   for (auto& x : c->ev) bad(cudaEventCreate(&x));

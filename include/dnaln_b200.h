@@ -140,7 +140,9 @@ int dnaln_gpu_set_sub_batch(dnaln_ctx* ctx, int64_t reads);
  *                    the long-read kernel first (default); 0 = straight to the warp kernels;
  *   "length_order"   1 = SW tasks of a batch whose reads differ in length run longest
  *                    first (default); 0 = in read order;
- *   "dir_cap_bytes"  traceback direction-code scratch per launch (default 1 GiB). */
+ *   "dir_cap_bytes"  traceback direction-code scratch per launch (default 1/32 of the
+ *                    device's memory, at least 1 GiB and at most 8 GiB; a launch whose
+ *                    tasks need more is split into chunks). */
 int dnaln_gpu_set_option(dnaln_ctx* ctx, const char* name, int64_t value);
 /* The SW kernel-form tuner (no reference counterpart): band widths with two register-
  * resident kernel forms (W = 33, 65) — inter-sequence, a thread holding the band rows of
