@@ -29,7 +29,7 @@ namespace dnb {
 namespace {
 
 constexpr int kLT = 128;          // threads per block
-constexpr int kLBlocksPerSm = 4;  // resident blocks per SM the grid is sized for (126 registers)
+constexpr int kLBlocksPerSm = 8;  // blocks per SM the grid is sized for: two waves of the 4 resident (126 registers)
 constexpr int kLMaxMin = 256;
 constexpr int kLMaxAnc = 256;
 constexpr int kLMaxChains = 32;
@@ -91,10 +91,11 @@ __global__ void __launch_bounds__(kLT)
   };
   const int m_list = *list_n;
   const int k = sp.k;
-  // Serpentine order over the (longest-first) list: round j takes positions
+  // The grid is two waves of resident blocks: the first takes the longest reads of the
+  // (longest-first) list, and the second's blocks start as the first's finish. A thread
+  // with more than one read takes them in serpentine order: round j takes positions
   // [j*stride, (j+1)*stride), forward on even rounds and reversed on odd ones, so the
-  // thread with the longest read of one round gets the shortest of the next. The
-  // kernel is one resident wave and lasts as long as its slowest warp.
+  // thread with the longest read of one round gets the shortest of the next.
   for (int64_t round = 0;; ++round) {
     const int64_t x = (round & 1) ? (round + 1) * stride - 1 - tid : round * stride + tid;
     if (x >= m_list) break;  // every later round's position is further still
