@@ -37,6 +37,8 @@
 // (h == e) is 1,0, and otherwise H came from F — so the walk (src/align.cpp:87-143)
 // takes the reference's steps. The best cell is the first strict maximum in row-major
 // order (per-row maximum with its first column, then strict across rows).
+#include <type_traits>
+
 #include "common.cuh"
 #include "sw.cuh"
 
@@ -566,15 +568,22 @@ __global__ void __launch_bounds__(kSwThreads, TB ? 3 : 1)
   uint32_t* const row_a = sw_rows + threadIdx.x;
   uint32_t* const row_b = sw_rows + (CH + 1) * kSwThreads + threadIdx.x;
   uint32_t hout = kBias2, fout = kBias2;  // this lane's last cell of its previous row
-  for (int t = 0; t < steps; ++t) {
+  const auto step = [&](const int t, auto steady) {
+    constexpr bool kSteady = decltype(steady)::value;
     const int i = t - c;
     const bool act = !skip && i >= 0 && i < qmax;
+    // H, E and the target window advance once the lane has reached row 0 (rows past the
+    // pair's end are N rows: they change no result and no code is stored for them); from
+    // step LANES - 1 on every lane has, so the steady steps carry no per-cell guard
+    const bool he_ok = kSteady || i >= 0;
     // row i's F and H(left) at column d0 - 1, from the left lane (its step t - 1)
     uint32_t hleft = __shfl_up_sync(FULL, hout, 1), f = __shfl_up_sync(FULL, fout, 1);
     if (c == 0) hleft = f = kBias2;
     const uint32_t ca = qcode(qa, qla, i), cb = qcode(qb, qlb, i);
     const uint32_t plo = prof_biased(p, ca), phi = prof_biased(p, cb);
-    const uint32_t t_next = act ? tc2(static_cast<int64_t>(i) + 1 + d0 + CH) : 0u;
+    // past the pair's end the window shifts in a valid selector (code A for both): the
+    // profile of an N row scores every target alike
+    const uint32_t t_next = act ? tc2(static_cast<int64_t>(i) + 1 + d0 + CH) : sel2(0u, 0u);
     uint32_t hdiag = H[0], rmax = 0, dw = 0;
     // local cell 0, then hand (H, E) of it to the left lane: the E input of its last cell
     uint32_t h0, e0;
@@ -600,7 +609,7 @@ __global__ void __launch_bounds__(kSwThreads, TB ? 3 : 1)
       nh = H[CH];
       ne = E[CH];
     }
-    if (act) {
+    if (he_ok) {
       H[0] = h0;
       E[0] = e0;
     }
@@ -615,7 +624,7 @@ __global__ void __launch_bounds__(kSwThreads, TB ? 3 : 1)
       f = __vmaxu2(fo, fe);
       const uint32_t m1 = __vmaxu2(hd, e);
       const uint32_t h = __vimax3_u16x2(m1, f, kBias2);
-      if (act) {
+      if (he_ok) {
         H[k] = h;
         E[k] = e;
       }
@@ -655,11 +664,16 @@ __global__ void __launch_bounds__(kSwThreads, TB ? 3 : 1)
           for (int k = 0; k <= CH; ++k) row_b[k * kSwThreads] = H[k];
         }
       }
+    }
+    if (he_ok) {
 #pragma unroll
       for (int k = 0; k < CH; ++k) T[k] = T[k + 1];
       T[CH] = t_next;
     }
-  }
+  };
+  const int ramp = steps < LANES - 1 ? steps : LANES - 1;
+  for (int t = 0; t < ramp; ++t) step(t, std::false_type{});
+  for (int t = ramp; t < steps; ++t) step(t, std::true_type{});
   // combine the lanes of the pair: larger value, then earlier row, then smaller column
   uint64_t key_a, key_b;
   const int ncell = c == LANES - 1 ? CH + 1 : CH;
