@@ -275,6 +275,16 @@ done:
 }
 
 
+// Best-row checkpoints of the two halves of a pair share two row buffers: a row that
+// improves both halves is stored once (the packed row serves both), and a half that
+// improves alone writes the buffer the other half is not using. Returns the buffer to
+// write; buf_a / buf_b say where each half's best row is.
+__device__ __forceinline__ int row_buffer(bool up_a, bool up_b, int buf_a, int buf_b) {
+  if (up_a && up_b) return buf_a;
+  if (up_a) return buf_a == buf_b ? 1 - buf_b : buf_a;
+  return buf_a == buf_b ? 1 - buf_a : buf_b;
+}
+
 // The DP kernels leave, for the walk, the best cell in the result: qb = its row, qe = its
 // column (the walk kernel then writes the final coordinates).
 __device__ __forceinline__ SwResult stash(int score, int bi, int bd) { return SwResult{score, bi, bd, 0, 0, 0, 0, 0}; }
@@ -422,6 +432,7 @@ __global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1) k_sw_u2(c
   extern __shared__ uint32_t sw_rows[];
   uint32_t* const row_a = sw_rows + threadIdx.x;
   uint32_t* const row_b = sw_rows + W * kSwThreads + threadIdx.x;
+  int buf_a = 0, buf_b = 1;  // which of the two row buffers holds each half's best row
   uint32_t ca = qcode(qa, qla, 0), cb = qcode(qb, qlb, 0);
   for (int i = 0; i < qmax; ++i) {
     // rows past a query's end are N rows for it: they cannot raise its best (values only
@@ -460,17 +471,22 @@ __global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1) k_sw_u2(c
       hdiag = hup;
     }
     if constexpr (TB) {  // a strictly better row (rows in order: the first strict maximum)
-      if ((rmax & 0xFFFFu) > best_a) {
-        best_a = rmax & 0xFFFFu;
-        bi_a = i;
+      const bool up_a = (rmax & 0xFFFFu) > best_a, up_b = (rmax >> 16) > best_b;
+      if (up_a || up_b) {
+        const int dst = row_buffer(up_a, up_b, buf_a, buf_b);
+        uint32_t* const row = dst ? row_b : row_a;
 #pragma unroll
-        for (int d = 0; d < W; ++d) row_a[d * kSwThreads] = H[d];
-      }
-      if ((rmax >> 16) > best_b) {
-        best_b = rmax >> 16;
-        bi_b = i;
-#pragma unroll
-        for (int d = 0; d < W; ++d) row_b[d * kSwThreads] = H[d];
+        for (int d = 0; d < W; ++d) row[d * kSwThreads] = H[d];
+        if (up_a) {
+          best_a = rmax & 0xFFFFu;
+          bi_a = i;
+          buf_a = dst;
+        }
+        if (up_b) {
+          best_b = rmax >> 16;
+          bi_b = i;
+          buf_b = dst;
+        }
       }
     }
 #pragma unroll
@@ -486,10 +502,12 @@ __global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1) k_sw_u2(c
   } else {  // first column of the best row holding the best value, per half
     bd_a = bi_a >= 0 ? W : -1;
     bd_b = bi_b >= 0 ? W : -1;
+    const uint32_t* const ra = buf_a ? row_b : row_a;
+    const uint32_t* const rb = buf_b ? row_b : row_a;
 #pragma unroll 1
     for (int d = W - 1; d >= 0; --d) {
-      if (bi_a >= 0 && (row_a[d * kSwThreads] & 0xFFFFu) == best_a) bd_a = d;
-      if (bi_b >= 0 && (row_b[d * kSwThreads] >> 16) == best_b) bd_b = d;
+      if (bi_a >= 0 && (ra[d * kSwThreads] & 0xFFFFu) == best_a) bd_a = d;
+      if (bi_b >= 0 && (rb[d * kSwThreads] >> 16) == best_b) bd_b = d;
     }
   }
   res[ta.slot] = stash(static_cast<int>(best_a) - static_cast<int>(kBias), TB ? bi_a : 0, bd_a);
@@ -567,6 +585,7 @@ __global__ void __launch_bounds__(kSwThreads, TB ? 3 : 1)
   extern __shared__ uint32_t sw_rows[];
   uint32_t* const row_a = sw_rows + threadIdx.x;
   uint32_t* const row_b = sw_rows + (CH + 1) * kSwThreads + threadIdx.x;
+  int buf_a = 0, buf_b = 1;  // which of the two row buffers holds each half's best row
   uint32_t hout = kBias2, fout = kBias2;  // this lane's last cell of its previous row
   const auto step = [&](const int t, auto steady) {
     constexpr bool kSteady = decltype(steady)::value;
@@ -651,17 +670,22 @@ __global__ void __launch_bounds__(kSwThreads, TB ? 3 : 1)
     fout = f;
     if (act) {
       if constexpr (TB) {  // a strictly better row of this lane's cells
-        if ((rmax & 0xFFFFu) > best_a) {
-          best_a = rmax & 0xFFFFu;
-          bi_a = i;
+        const bool up_a = (rmax & 0xFFFFu) > best_a, up_b = (rmax >> 16) > best_b;
+        if (up_a || up_b) {
+          const int dst = row_buffer(up_a, up_b, buf_a, buf_b);
+          uint32_t* const row = dst ? row_b : row_a;
 #pragma unroll
-          for (int k = 0; k <= CH; ++k) row_a[k * kSwThreads] = H[k];
-        }
-        if ((rmax >> 16) > best_b) {
-          best_b = rmax >> 16;
-          bi_b = i;
-#pragma unroll
-          for (int k = 0; k <= CH; ++k) row_b[k * kSwThreads] = H[k];
+          for (int k = 0; k <= CH; ++k) row[k * kSwThreads] = H[k];
+          if (up_a) {
+            best_a = rmax & 0xFFFFu;
+            bi_a = i;
+            buf_a = dst;
+          }
+          if (up_b) {
+            best_b = rmax >> 16;
+            bi_b = i;
+            buf_b = dst;
+          }
         }
       }
     }
@@ -679,10 +703,12 @@ __global__ void __launch_bounds__(kSwThreads, TB ? 3 : 1)
   const int ncell = c == LANES - 1 ? CH + 1 : CH;
   if constexpr (TB) {
     int bd_a = 0xFFF, bd_b = 0xFFF;
+    const uint32_t* const ra = buf_a ? row_b : row_a;
+    const uint32_t* const rb = buf_b ? row_b : row_a;
 #pragma unroll 1
     for (int k = ncell - 1; k >= 0; --k) {
-      if (bi_a >= 0 && (row_a[k * kSwThreads] & 0xFFFFu) == best_a) bd_a = d0 + k;
-      if (bi_b >= 0 && (row_b[k * kSwThreads] >> 16) == best_b) bd_b = d0 + k;
+      if (bi_a >= 0 && (ra[k * kSwThreads] & 0xFFFFu) == best_a) bd_a = d0 + k;
+      if (bi_b >= 0 && (rb[k * kSwThreads] >> 16) == best_b) bd_b = d0 + k;
     }
     key_a = static_cast<uint64_t>(best_a) << 40 | static_cast<uint64_t>(0xFFFFFu - static_cast<uint32_t>(bi_a + 1)) << 12 |
             (0xFFFu - static_cast<uint32_t>(bd_a));
