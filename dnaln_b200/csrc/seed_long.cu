@@ -29,7 +29,7 @@ namespace dnb {
 namespace {
 
 constexpr int kLT = 128;          // threads per block
-constexpr int kLBlocksPerSm = 8;  // blocks per SM the grid is sized for: two waves of the 4 resident (126 registers)
+constexpr int kLBlocksPerSm = 8;  // blocks per SM the grid is sized for: 6 resident (80 registers), then the rest
 constexpr int kLMaxMin = 256;
 constexpr int kLMaxAnc = 256;
 constexpr int kLMaxChains = 32;
@@ -63,7 +63,7 @@ __global__ void k_long_keys(const int32_t* __restrict__ list, const int* __restr
 }
 
 template <int W>
-__global__ void __launch_bounds__(kLT)
+__global__ void __launch_bounds__(kLT, 6)
     k_seed_chain_tl(const int32_t* __restrict__ seq_len, const int64_t* __restrict__ pofs,
                     const uint8_t* __restrict__ codes, const int32_t* __restrict__ list, const int* __restrict__ list_n,
                     DevIndex ix, SeedParams sp, ChainParamsDev cp, CandParams cand, CandBuf cb,
@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(kLT)
   };
   const int m_list = *list_n;
   const int k = sp.k;
-  // The grid is two waves of resident blocks: the first takes the longest reads of the
-  // (longest-first) list, and the second's blocks start as the first's finish. A thread
+  // The grid is more blocks than are resident: the first wave takes the longest reads of
+  // the (longest-first) list, and the later blocks start as the first's finish. A thread
   // with more than one read takes them in serpentine order: round j takes positions
   // [j*stride, (j+1)*stride), forward on even rounds and reversed on odd ones, so the
   // thread with the longest read of one round gets the shortest of the next.
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(kLT)
     }
     // ---- probe and anchors (src/mapper.cpp:16-40)
     int na = 0;
-    constexpr int kP = 8;
+    constexpr int kP = 4;  // keys probed at once: four keep the kernel at 6 blocks per SM
     for (int j0 = 0; j0 < nmin && !big; j0 += kP) {
       uint32_t mh[kP], mp[kP];
       ulonglong2 bk[kP];
