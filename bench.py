@@ -683,8 +683,16 @@ class ServePools:
         self.genomes = [synth.make_genome(synth.GENOME_4M6, seed), synth.make_genome(synth.GENOME_120M, seed + 1)]
         spec = synth.ReadsSpec(n_reads=pool, len_min=100, len_max=300, len_dist=2)
         self.pools = [synth.make_reads(g, spec, seed + 10 + i)[0] for i, g in enumerate(self.genomes)]
-        self.arrays = [(rb.seq, np.ascontiguousarray(rb.seq_off[:-1]), np.ascontiguousarray(rb.seq_len),
-                        rb.name_hash()) for rb in self.pools]
+        self._arrays = None
+
+    @property
+    def arrays(self):
+        """Per pool: reads, offsets, lengths and name hashes as the C ABI takes them (the
+        hashes come from the mapping library, so the reference arm never asks for them)."""
+        if self._arrays is None:
+            self._arrays = [(rb.seq, np.ascontiguousarray(rb.seq_off[:-1]), np.ascontiguousarray(rb.seq_len),
+                             rb.name_hash()) for rb in self.pools]
+        return self._arrays
 
     def stream(self, n_req: int, seed: int):
         """(genome, first read, size) per request: genome 50/50, size log-uniform."""

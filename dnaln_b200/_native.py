@@ -1,7 +1,10 @@
-"""ctypes declarations of the C ABI in include/dnaln_b200.h and include/dnaln_synth.h.
+"""ctypes declarations of the C ABI in include/dnaln_b200.h (libdnaln_b200.so, the mapping
+path) and include/dnaln_synth.h (libdnaln_synth.so, the seeded workload generator).
 
-The library is loaded from the package directory only (the in-tree build); a missing
-library is an ImportError-like failure, never a silent fallback.
+Both libraries are loaded from the package directory only (the in-tree build); a missing
+library is an ImportError-like failure, never a silent fallback. The generator is a
+library of its own so that programs which only need workloads (the reference's CPU
+baseline) never load the mapping path.
 """
 from __future__ import annotations
 
@@ -11,6 +14,7 @@ from pathlib import Path
 import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "libdnaln_b200.so"
+SYNTH_LIB_PATH = Path(__file__).resolve().parent / "libdnaln_synth.so"
 
 OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_CAPACITY, ERR_NO_DEVICE, ERR_DEVICE, ERR_NOT_FOUND, ERR_IO = range(9)
 ERR_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "CUDA", 3: "OOM", 4: "CAPACITY", 5: "NO_DEVICE", 6: "DEVICE",
@@ -161,27 +165,44 @@ SIGNATURES = {
     "dnaln_reads_view": (C.c_int, [P, C.POINTER(i64)] + [C.POINTER(P)] * 8),
     "dnaln_reads_free": (None, [P]),
     "dnaln_eval_records": (C.c_int, [P, P, P, P, P, i64, i32, C.POINTER(EvalCounts)]),
+}
+
+# include/dnaln_synth.h, in libdnaln_synth.so
+SYNTH_SIGNATURES = {
     "dnaln_synth_genome": (C.c_int, [u64, C.POINTER(SynthGenomeSpec), P]),
     "dnaln_synth_reads_bytes": (i64, [u64, C.POINTER(SynthReadsSpec)]),
     "dnaln_synth_reads": (C.c_int, [u64, P, P, P, i32, C.POINTER(SynthReadsSpec), P, i64, P, P, i64, P, P, P, P]),
 }
 
 _lib: C.CDLL | None = None
+_synth: C.CDLL | None = None
+
+
+def _load(path: Path, sigs: dict) -> C.CDLL:
+    if not path.exists():
+        raise RuntimeError(f"{path} is missing: run `python -m dnaln_b200.build` (needs nvcc)")
+    L = C.CDLL(str(path))
+    for name, (res, args) in sigs.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
 
 
 def lib() -> C.CDLL:
-    """The loaded native library (raises if it has not been built)."""
+    """The loaded mapping library (raises if it has not been built)."""
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
-            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m dnaln_b200.build` (needs nvcc)")
-        L = C.CDLL(str(LIB_PATH))
-        for name, (res, args) in SIGNATURES.items():
-            f = getattr(L, name)
-            f.restype = res
-            f.argtypes = args
-        _lib = L
+        _lib = _load(LIB_PATH, SIGNATURES)
     return _lib
+
+
+def synth_lib() -> C.CDLL:
+    """The loaded workload-generator library (raises if it has not been built)."""
+    global _synth
+    if _synth is None:
+        _synth = _load(SYNTH_LIB_PATH, SYNTH_SIGNATURES)
+    return _synth
 
 
 def ptr(a: np.ndarray | None) -> int | None:

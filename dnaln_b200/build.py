@@ -23,7 +23,11 @@ LIB = PKG / "libdnaln_b200.so"
 CUDA_SOURCES = ["csrc/sw.cu", "csrc/seed.cu", "csrc/seed_thread.cu", "csrc/map.cu", "csrc/capi.cu", "csrc/noalloc.cu",
                 "csrc/serve.cu", "csrc/index_build.cu",
                 "csrc/seed_long.cu"]
-HOST_SOURCES = ["host/sam.cpp", "host/synth.cpp", "host/reads.cpp", "host/eval.cpp"]
+HOST_SOURCES = ["host/sam.cpp", "host/reads.cpp", "host/eval.cpp"]
+# the seeded workload generator, a library of its own (no CUDA): programs that only need
+# workloads, such as the reference's CPU baseline, load it without the mapping path
+SYNTH_SOURCES = ["host/synth.cpp"]
+SYNTH_LIB = PKG / "libdnaln_synth.so"
 HEADERS = ["csrc/common.cuh", "csrc/sw.cuh", "csrc/seed.cuh", "csrc/map.cuh", "csrc/index_build.cuh"]
 PUBLIC_HEADERS = ["dnaln_b200.h", "dnaln_synth.h"]
 
@@ -42,7 +46,8 @@ def _includes() -> list[str]:
 
 
 def _newest_input() -> float:
-    files = [PKG / s for s in CUDA_SOURCES + HOST_SOURCES + HEADERS] + [ROOT / "include" / h for h in PUBLIC_HEADERS]
+    files = [PKG / s for s in CUDA_SOURCES + HOST_SOURCES + SYNTH_SOURCES + HEADERS] + \
+        [ROOT / "include" / h for h in PUBLIC_HEADERS]
     files.append(Path(__file__))
     return max(f.stat().st_mtime for f in files)
 
@@ -69,8 +74,11 @@ def _compile_host(src: str) -> Path:
 
 
 def build(force: bool = False, verbose: bool = False, extra_nvcc: list[str] | None = None) -> Path:
-    """Compiles the CUDA and host sources and links ``libdnaln_b200.so``; returns its path."""
-    if not force and LIB.exists() and LIB.stat().st_mtime >= _newest_input():
+    """Compiles the CUDA and host sources and links ``libdnaln_b200.so`` (and the generator,
+    ``libdnaln_synth.so``); returns the mapping library's path."""
+    newest = _newest_input()
+    if not force and LIB.exists() and SYNTH_LIB.exists() and min(LIB.stat().st_mtime,
+                                                                 SYNTH_LIB.stat().st_mtime) >= newest:
         return LIB
     BUILD.mkdir(exist_ok=True)
     nvcc = _nvcc()
@@ -78,10 +86,15 @@ def build(force: bool = False, verbose: bool = False, extra_nvcc: list[str] | No
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:
         futs = [ex.submit(_compile_cuda, s, nvcc, extra) for s in CUDA_SOURCES]
         futs += [ex.submit(_compile_host, s) for s in HOST_SOURCES]
+        sfuts = [ex.submit(_compile_host, s) for s in SYNTH_SOURCES]
         objs = [f.result() for f in futs]
+        sobjs = [f.result() for f in sfuts]
     tmp = LIB.with_suffix(".so.tmp")
     _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lpthread"])
     os.replace(tmp, LIB)
+    tmp = SYNTH_LIB.with_suffix(".so.tmp")
+    _run([os.environ.get("CXX", "g++"), "-shared", "-o", str(tmp), *map(str, sobjs)])
+    os.replace(tmp, SYNTH_LIB)
     if verbose:
         print(f"built {LIB}", file=sys.stderr)
     return LIB

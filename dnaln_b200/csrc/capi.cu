@@ -1,20 +1,25 @@
 // capi.cu — the C ABI (include/dnaln_b200.h): contexts, HBM-resident genome indexes, and
-// the orchestration of each batch through the kernels of seed.cu, sw.cu and map.cu.
+// the orchestration of each batch through the kernels of seed_thread.cu, seed_long.cu,
+// seed.cu, sw.cu and map.cu.
 //
-// One batch (Mapper::map, src/mapper.cpp:75-223) runs as:
-//   lengths -> packed offsets (scan)                         [1 small host read-back]
-//   k_seed: encode both strands, sketch, probe, anchor counts
-//   anchor offsets (scan)                                    [1 small host read-back]
-//   k_chain_map: anchors, sort, chaining DP, chains, candidate loci
-//   score-only SW over every candidate of reads with >= 2 candidates
-//   k_choose: best / ties / second best, fnv1a tie-break, traceback tasks
-//   SW with traceback over each read's chosen candidate (chunked by scratch size)
-//   k_records: MAPQ, positions, soft clips; CIGAR offsets (scan)  [1 host read-back]
-//   k_cigar_gather: final CIGARs
-// Task counts produced on the device are consumed on the device (kernels read them), so
-// the host only waits where it must size a buffer. The host-buffer entry point splits a
-// batch into sub-batches and overlaps their copies in and out with the compute (two
-// device slots, two copy streams); it knows the lengths, so it skips the first read-back.
+// One batch (Mapper::map, src/mapper.cpp:75-223) is enqueued on the context's stream as:
+//   k_len64 + scan: packed read offsets, total bases, longest read (read back first only
+//     when the caller did not give the batch's size, so the rest can run as a graph)
+//   k_encode_reads: codes of both strands of every read
+//   k_seed_chain_t: short reads one thread each (sketch, probe, anchors, chaining DP,
+//     chains, candidate loci); reads it cannot take are listed
+//   k_seed_chain_tl: listed long reads one thread each, longest first; what exceeds its
+//     bounds is listed again
+//   k_seed<list> + k_chain_map<list>: the reads still listed, one warp each
+//   score-only SW over every candidate of reads with >= 2 candidates, then k_choose
+//     (best / ties / second best, fnv1a tie-break, the traceback task of each read)
+//   SW with traceback over each read's chosen candidate (chunked by scratch size), walk
+//   k_records (MAPQ, positions, soft clips), CIGAR offsets (scan), k_cigar_gather
+//   one read-back of the batch's totals, task counts, error flags and counters
+// Task and list counts produced on the device are consumed on the device, so the host
+// waits once per batch. The host-buffer entry points queue parts of a batch to a worker
+// thread that overlaps their copies in and out with the compute (two device slots, two
+// copy streams).
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
@@ -677,7 +682,7 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
     if (thread_path) {
       CK(cub::DeviceReduce::Sum(t, tmp, n_anc_t, total + 1, n, st));
       kt.begin(st, "k_list_sum");
-      const unsigned lb = nblk(std::min<int64_t>(n, 148 * 256));
+      const unsigned lb = nblk(std::min<int64_t>(n, int64_t{256} * device_sm_count()));
       k_list_sum<<<lb, 256, 0, st>>>(n_min, warp_list, warp_n, info + 6);
       k_list_sum<<<lb, 256, 0, st>>>(d_seq_len, warp_list, warp_n, info + 7);
       k_list_sum64<<<lb, 256, 0, st>>>(n_anchor, warp_list, warp_n, info + 9);

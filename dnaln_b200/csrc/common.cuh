@@ -4,9 +4,50 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "dnaln_b200.h"
 
 namespace dnb {
+
+constexpr int kMaxDevices = 64;
+
+// Streaming multiprocessors of the current device (148 on a B200), looked up once per
+// device; grids that stride over their work are sized by it.
+inline int device_sm_count() {
+  static std::atomic<int> sms[kMaxDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return 148;
+  }
+  int v = sms[dev].load(std::memory_order_relaxed);
+  if (v > 0) return v;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+    cudaGetLastError();
+    v = 148;
+  }
+  sms[dev].store(v, std::memory_order_relaxed);
+  return v;
+}
+
+// Raises a kernel's dynamic shared-memory limit once per device; host threads that map
+// batches at the same time may race to do it, which is harmless (the attribute is the same).
+template <class Kernel>
+bool set_smem_limit_once(Kernel* kernel, int bytes, std::atomic<bool>* done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return false;
+  }
+  if (done[dev].load(std::memory_order_acquire)) return true;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  done[dev].store(true, std::memory_order_release);
+  return true;
+}
 
 constexpr uint64_t kInvalidHash = ~0ULL;  // palindromic k-mer / empty bucket (src/minimizer.cpp:7, src/index.hpp:53)
 constexpr int kWarp = 32;
@@ -23,6 +64,10 @@ enum : uint32_t {
   // host grows it and maps the batch again), and the caller's CIGAR buffer was too small
   kErrChainPool = 1u << 4,
   kErrOutputCapacity = 1u << 5,
+  // a task the caller described wrongly, found on the device (dnaln_gpu_align_noalloc: a
+  // query longer than the stated maximum, a negative length or offset); the call fails
+  // with DNALN_ERR_INVALID_ARG and the other tasks' results stand
+  kErrBadTask = 1u << 6,
 };
 
 // Thomas Wang's 64-bit mix restricted to `mask` bits, step for step as the index keys are

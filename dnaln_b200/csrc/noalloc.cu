@@ -17,9 +17,12 @@
 // them. Each call clears the error flag before its first launch; nothing else in the
 // array needs clearing (every scratch cell is written before it is read).
 //
-// Set-up: the host needs the device address of the array, which it takes with
-// cudaGetSymbolAddress once per device, on the first call made with that device
-// current, and caches. That first call should therefore come before any stream capture.
+// Set-up: host code cannot use the array's name as a device address (in host code it
+// names a host-side stand-in), so each call takes the address with cudaGetSymbolAddress
+// for the device current at the call, unless the caller's stream is being captured, when
+// the address the last uncaptured call on that device took is used instead. The first
+// call on each device should therefore come before any stream capture. The caller's stream
+// must belong to the device that is current at the call.
 #include <algorithm>
 #include <mutex>
 
@@ -32,7 +35,6 @@ namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;  // 64 MiB
 constexpr size_t kHeader = 256;                            // error flag lives at offset 0
-constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -41,8 +43,10 @@ void* g_addr[kMaxDevices] = {};
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Task descriptors for tasks [base, base + count) of the caller's arrays; a query longer
-// than max_qlen is flagged and aligned as empty so that no scratch is overrun.
+// Task descriptors for tasks [base, base + count) of the caller's arrays. A task the
+// caller described wrongly (a query longer than max_qlen, a negative length or offset) is
+// flagged with kErrBadTask and aligned as empty, so that no scratch is overrun and no
+// byte before the caller's buffers is read.
 __global__ void k_na_tasks(int64_t base, int count, const int64_t* __restrict__ q_off,
                            const int32_t* __restrict__ q_len, const int64_t* __restrict__ t_off,
                            const int32_t* __restrict__ t_len, int max_qlen, int W, int64_t cigar_stride,
@@ -52,18 +56,21 @@ __global__ void k_na_tasks(int64_t base, int count, const int64_t* __restrict__ 
   const int64_t i = base + j;
   int ql = q_len[i];
   int tl = t_len[i];
-  if (ql < 0 || ql > max_qlen || tl < 0) {
-    atomicOr(err, kErrCigarOverflow);
+  int64_t qo = q_off[i], to = t_off[i];
+  if (ql < 0 || ql > max_qlen || tl < 0 || qo < 0 || to < 0) {
+    atomicOr(err, kErrBadTask);
     ql = 0;
     tl = 0;
+    qo = 0;
+    to = 0;
   }
   const int64_t tmax = static_cast<int64_t>(ql) + W - 1;
   SwTask t;
-  t.q_off = q_off[i];
+  t.q_off = qo;
   t.qlen = ql;
-  t.t_start = t_off[i];
-  t.t_lo = t_off[i];
-  t.t_hi = t_off[i] + (tl < tmax ? tl : tmax);
+  t.t_start = to;
+  t.t_lo = to;
+  t.t_hi = to + (tl < tmax ? tl : tmax);
   t.slot = j;
   t.flags = 0;
   t.pad_ = 0;
@@ -100,14 +107,21 @@ __global__ void k_na_finish(int64_t base, int count, const SwResult* __restrict_
   }
 }
 
-int scratch_address(unsigned char** out) {
+// The device address of g_noalloc_scratch for the current device. Looked up again on
+// every call made outside a stream capture (so a context created after cudaDeviceReset
+// gets its own array's address); inside a capture the address of the last uncaptured
+// call on this device is used.
+int scratch_address(cudaStream_t st, unsigned char** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     cudaGetLastError();
     return DNALN_ERR_NO_DEVICE;
   }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const bool capturing = cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+  cudaGetLastError();
   std::lock_guard<std::mutex> lk(g_addr_mu);
-  if (!g_addr[dev]) {
+  if (!capturing) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
       cudaGetLastError();
@@ -115,6 +129,7 @@ int scratch_address(unsigned char** out) {
     }
     g_addr[dev] = p;
   }
+  if (!g_addr[dev]) return DNALN_ERR_CUDA;  // first call on this device made inside a capture
   *out = static_cast<unsigned char*>(g_addr[dev]);
   return DNALN_OK;
 }
@@ -136,9 +151,9 @@ extern "C" int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_of
   if (n == 0) return DNALN_OK;
   if (!d_q || !d_q_off || !d_q_len || !d_t || !d_t_off || !d_t_len || !d_out || (tb && !d_cigar))
     return DNALN_ERR_INVALID_ARG;
-  unsigned char* base_ptr = nullptr;
-  if (int e = scratch_address(&base_ptr)) return e;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned char* base_ptr = nullptr;
+  if (int e = scratch_address(st, &base_ptr)) return e;
 
   const SwParams p = make_sw_params(*sp);
   const bool bytes_ok = sw_bytes_ok(*sp);
@@ -184,5 +199,6 @@ extern "C" int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_of
   uint32_t bits = 0;
   if (cudaMemcpyAsync(&bits, err, sizeof bits, cudaMemcpyDeviceToHost, st) != cudaSuccess) return DNALN_ERR_CUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return DNALN_ERR_CUDA;
-  return bits ? DNALN_ERR_DEVICE : DNALN_OK;
+  if (bits & ~kErrBadTask) return DNALN_ERR_DEVICE;  // a kernel's own consistency check
+  return bits ? DNALN_ERR_INVALID_ARG : DNALN_OK;       // only tasks the caller described wrongly
 }

@@ -1022,7 +1022,7 @@ void launch_seed_list(cudaStream_t st, const char* seq, const int64_t* seq_off, 
                       int32_t* n_min, int64_t* n_anchor, uint32_t* err) {
   if (n_max <= 0) return;
   // grid-stride over a list whose length is only known on the device: a few resident waves
-  const int64_t blocks = std::min<int64_t>((n_max + kSeedWarps - 1) / kSeedWarps, 148 * 8);
+  const int64_t blocks = std::min<int64_t>((n_max + kSeedWarps - 1) / kSeedWarps, int64_t{8} * device_sm_count());
   k_seed<<<static_cast<unsigned>(blocks), kSeedWarps * 32, 0, st>>>(seq, seq_off, seq_base, seq_len, pofs, n_max,
                                                                    list, list_n, codes, ix, sp, mb, n_min, n_anchor,
                                                                    err);
@@ -1034,7 +1034,7 @@ void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_l
                       unsigned long long* pool_top, int64_t pool_cap, CandBuf cb, uint32_t* err) {
   if (n <= 0) return;
   // grid-stride over a count that may be known on the device only: a few resident waves
-  const int64_t blocks = std::min<int64_t>((n + kChainWarps - 1) / kChainWarps, 148 * 16);
+  const int64_t blocks = std::min<int64_t>((n + kChainWarps - 1) / kChainWarps, int64_t{16} * device_sm_count());
   k_chain_map<<<static_cast<unsigned>(blocks), kChainWarps * 32, 0, st>>>(
       pofs, seq_len, n, list, list_n, n_min, n_anchor, mb, ix, cp, cand, as, pool_top, pool_cap, cb, err);
 }

@@ -451,7 +451,7 @@ bool seed_long_supported(const SeedParams& sp, const ChainParamsDev& cp) {
 }
 
 int64_t seed_long_threads(int64_t n_max) {
-  const int64_t cap = static_cast<int64_t>(148) * kLBlocksPerSm * kLT;
+  const int64_t cap = static_cast<int64_t>(device_sm_count()) * kLBlocksPerSm * kLT;
   const int64_t want = (n_max + kLT - 1) / kLT * kLT;
   return want < cap ? want : cap;
 }

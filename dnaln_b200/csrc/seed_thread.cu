@@ -449,7 +449,7 @@ bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp) {
 void launch_encode_reads(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
                          const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes) {
   if (n <= 0) return;
-  const int64_t blocks = std::min<int64_t>((n + 7) / 8, 148 * 16);  // 8 warps a block, grid-stride
+  const int64_t blocks = std::min<int64_t>((n + 7) / 8, int64_t{16} * device_sm_count());  // 8 warps a block, grid-stride
   k_encode_reads<<<static_cast<unsigned>(blocks), 256, 0, st>>>(seq, seq_off, seq_base, seq_len, pofs, n, codes);
 }
 
@@ -460,15 +460,8 @@ bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* s
                               int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err) {
   if (!seed_thread_supported(sp, cp)) return false;
   if (n <= 0) return true;
-  static bool attr_set[64] = {};  // per device
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
-  if (!attr_set[dev]) {
-    if (cudaFuncSetAttribute(k_seed_chain_t<kTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, kThreadSmem) !=
-        cudaSuccess)
-      return false;
-    attr_set[dev] = true;
-  }
+  static std::atomic<bool> attr_set[kMaxDevices];
+  if (!set_smem_limit_once(k_seed_chain_t<kTW>, kThreadSmem, attr_set)) return false;
   const int64_t blocks = (n + kTT - 1) / kTT;
   k_seed_chain_t<kTW><<<static_cast<unsigned>(blocks), kTT, kThreadSmem, st>>>(
       seq, seq_off, seq_base, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list, big_n, err);

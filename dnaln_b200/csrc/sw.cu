@@ -1005,12 +1005,8 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
   if (tb) {
     constexpr int kRowBytes = 2 * W * kSwThreads * 4;  // the two saved best rows of each thread
     if (kRowBytes > 48 * 1024) {
-      static bool attr_set[64] = {};
-      int dev = 0;
-      if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && !attr_set[dev] &&
-          cudaFuncSetAttribute(k_sw_u2<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowBytes) ==
-              cudaSuccess)
-        attr_set[dev] = true;
+      static std::atomic<bool> attr_set[kMaxDevices];
+      set_smem_limit_once(k_sw_u2<W, true>, kRowBytes, attr_set);
     }
     t.begin(st, "k_sw_u2<tb>");
     k_sw_u2<W, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,

@@ -14,7 +14,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import Genome, ReadBatch
-from ._native import SynthGenomeSpec, SynthReadsSpec, lib, ptr
+from ._native import SynthGenomeSpec, SynthReadsSpec, ptr, synth_lib
 
 # error model shared by every workload: 1% substitution, 0.1% indel (half ins, half del),
 # indel length geometric(p = 0.7) capped at 5
@@ -78,7 +78,7 @@ def make_genome(spec: GenomeSpec, seed: int) -> Genome:
                         spec.repeat_frac, spec.repeat_div, spec.n_frac, spec.n_run_min, spec.n_run_max)
     total = spec.n_contigs * spec.contig_len
     codes = np.zeros(total, np.uint8)
-    rc = lib().dnaln_synth_genome(seed, C.byref(s), ptr(codes))
+    rc = synth_lib().dnaln_synth_genome(seed, C.byref(s), ptr(codes))
     if rc:
         raise RuntimeError(f"genome generation failed ({rc})")
     off = np.arange(spec.n_contigs, dtype=np.uint64) * np.uint64(spec.contig_len)
@@ -98,7 +98,7 @@ def make_reads(g: Genome, spec: ReadsSpec, seed: int, with_qual: bool = False) -
     s = SynthReadsSpec(spec.n_reads, spec.len_min, spec.len_max, spec.len_dist, ERR["sub"], ERR["indel"],
                        ERR["indel_geom_p"], ERR["indel_cap"], spec.big_del_frac, spec.big_del_min, spec.big_del_max,
                        spec.name_base)
-    L = lib()
+    L = synth_lib()
     nbytes = int(L.dnaln_synth_reads_bytes(seed, C.byref(s)))
     n = spec.n_reads
     seq = np.zeros(max(nbytes, 1), np.uint8)

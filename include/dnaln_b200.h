@@ -246,11 +246,16 @@ int dnaln_gpu_align(dnaln_ctx* ctx, const uint8_t* q, const int64_t* q_off, cons
  * every d_q_len[i] must be <= max_qlen. Its result goes to d_out[i] and, with traceback,
  * its CIGAR to d_cigar[i * cigar_stride ..] (cigar_stride >= 2*max_qlen+1; cigar_off =
  * i * cigar_stride). Launches go to `stream` (a cudaStream_t, NULL = default stream) and
- * the call returns after they finish. Returns DNALN_ERR_INVALID_ARG when one warp of
- * tasks of max_qlen rows at this band width does not fit the 64 MiB, DNALN_ERR_DEVICE
- * when a query exceeds max_qlen. The first call on each device looks up the array's
- * address (cudaGetSymbolAddress) and should come before any stream capture. All calls
- * share the array: calls that overlap on the GPU race, so serialize them. */
+ * the call returns after they finish; the stream must belong to the device current at
+ * the call. Returns DNALN_ERR_INVALID_ARG when one warp of tasks of max_qlen rows at this
+ * band width does not fit the 64 MiB, and also when a task is found on the device to be
+ * described wrongly (a query longer than max_qlen, a negative length or offset): that task
+ * is aligned as empty and every other task's result stands. DNALN_ERR_DEVICE means a
+ * kernel's own consistency check failed. Each call made outside a stream capture looks up
+ * the array's address on the current device (cudaGetSymbolAddress); a call inside a
+ * capture uses the address the last uncaptured call on that device found, so the first
+ * call on each device should come before any stream capture. All calls share the array:
+ * calls that overlap on the GPU race, so serialize them. */
 int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_off, const int32_t* d_q_len, const uint8_t* d_t,
                             const int64_t* d_t_off, const int32_t* d_t_len, int64_t n, int32_t max_qlen,
                             int32_t traceback, const dnaln_score_params* sp, dnaln_align_result* d_out,

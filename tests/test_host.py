@@ -14,21 +14,30 @@ from dnaln_b200 import synth
 ROOT = Path(__file__).resolve().parent.parent
 
 
-def declared_functions():
-    names = set()
-    for h in (ROOT / "include").glob("*.h"):
-        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
-        names |= set(re.findall(r"\b(dnaln_\w+)\s*\(", text))
-    return names
+def declared_functions(header: str):
+    text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / header).read_text(), flags=re.S)
+    return set(re.findall(r"\b(dnaln_\w+)\s*\(", text))
 
 
 def test_library_exports_every_declared_function():
-    lib = N.lib()
-    names = declared_functions()
-    assert len(names) >= 20
-    for n in sorted(names):
-        assert hasattr(lib, n), f"{n} declared in include/ but not exported"
-    assert set(N.SIGNATURES) <= names
+    assert sorted(h.name for h in (ROOT / "include").glob("*.h")) == ["dnaln_b200.h", "dnaln_synth.h"]
+    for header, lib, sigs in [("dnaln_b200.h", N.lib(), N.SIGNATURES),
+                              ("dnaln_synth.h", N.synth_lib(), N.SYNTH_SIGNATURES)]:
+        names = declared_functions(header)
+        assert len(names) >= 3
+        for n in sorted(names):
+            assert hasattr(lib, n), f"{n} declared in include/{header} but not exported"
+        assert set(sigs) <= names
+    assert len(declared_functions("dnaln_b200.h")) >= 20
+
+
+def test_generator_library_is_separate_from_the_mapping_path():
+    # a program that only generates workloads never loads the mapping library
+    import subprocess
+    out = subprocess.run(["nm", "-D", "--defined-only", str(N.SYNTH_LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if ln.split() and ln.split()[-1].startswith("dnaln_")}
+    assert exported == declared_functions("dnaln_synth.h")
 
 
 def test_context_without_gpu_reports_no_device():

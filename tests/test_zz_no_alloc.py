@@ -25,12 +25,16 @@ def concat(seqs):
     return buf.astype(np.uint8), off, lens
 
 
-def run_noalloc(qs, ts, sp, traceback=True):
+def run_noalloc(qs, ts, sp, traceback=True, max_qlen=None, q_off_fix=None, expect=N.OK):
+    """Calls the entry point on device copies of the tasks; q_off_fix (index, value)
+    overwrites one query offset, to describe a task wrongly on purpose."""
     import torch
     qb, qo, ql = concat(qs)
     tb, to, tl = concat(ts)
+    if q_off_fix is not None:
+        qo[q_off_fix[0]] = q_off_fix[1]
     n = len(qs)
-    max_qlen = int(ql.max())
+    max_qlen = int(ql.max()) if max_qlen is None else max_qlen
     stride = 2 * max_qlen + 1
     dev = {k: torch.from_numpy(v).cuda() for k, v in dict(qb=qb, qo=qo, ql=ql, tb=tb, to=to, tl=tl).items()}
     out = torch.zeros(n * 40, dtype=torch.uint8, device="cuda")
@@ -40,20 +44,23 @@ def run_noalloc(qs, ts, sp, traceback=True):
                                          dev["tb"].data_ptr(), dev["to"].data_ptr(), dev["tl"].data_ptr(), n, max_qlen,
                                          int(traceback), C.byref(sp), out.data_ptr(), cig.data_ptr(), stride,
                                          stream.cuda_stream)
-    assert rc == N.OK, f"dnaln_gpu_align_noalloc returned {N.ERR_NAMES.get(rc, rc)}"
+    assert rc == expect, f"dnaln_gpu_align_noalloc returned {N.ERR_NAMES.get(rc, rc)}"
     torch.cuda.synchronize()
     res = out.cpu().numpy().view(D.ALIGN_RESULT_DTYPE)
     return res, cig.cpu().numpy().view(np.uint32)
 
 
-def assert_same(qs, ts, sp, ctx):
+def assert_same(qs, ts, sp, ctx, rows=None, **kw):
+    """rows: the tasks to compare (default all)."""
     exp = ctx.align(qs, ts, True, sp)
-    res, cig = run_noalloc(qs, ts, sp)
+    res, cig = run_noalloc(qs, ts, sp, **kw)
+    rows = np.arange(len(qs)) if rows is None else np.asarray(rows)
     for f in ("score", "qb", "qe", "tb", "te", "nm", "cigar_len"):
-        assert np.array_equal(res[f], exp.results[f]), f
-    for i in range(len(qs)):
+        assert np.array_equal(res[f][rows], exp.results[f][rows]), f
+    for i in rows:
         o, m = int(res["cigar_off"][i]), int(res["cigar_len"][i])
         assert np.array_equal(cig[o:o + m], exp.cigar_of(i)), i
+    return res
 
 
 @pytest.mark.parametrize("scheme", [(2, 4, 4, 2, 1, 16), (2, 4, 4, 2, 1, 64), (1, 4, 6, 1, 1, 8)])
@@ -75,3 +82,29 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                          z.data_ptr(), 1, 2_000_000, 1, C.byref(sp), z.data_ptr(), z.data_ptr(),
                                          4_000_001, None)
     assert rc == N.ERR_INVALID_ARG
+
+
+def test_noalloc_score_only_matches_align(ctx):
+    # without traceback only the score is computed; no CIGAR is written (cigar_len 0)
+    sp = D.ScoreParams(2, 4, 4, 2, 1, 16)
+    qs, ts = random_tasks(np.random.default_rng(5), 500, 16)
+    exp = ctx.align(qs, ts, False, sp)
+    res, _ = run_noalloc(qs, ts, sp, traceback=False)
+    assert np.array_equal(res["score"], exp.results["score"])
+    assert not res["cigar_len"].any()
+
+
+def test_noalloc_refuses_a_task_described_wrongly_and_keeps_the_others(ctx):
+    # a query longer than the stated maximum, then a negative query offset: the call
+    # returns DNALN_ERR_INVALID_ARG, the task is aligned as empty, the others stand
+    sp = D.ScoreParams(2, 4, 4, 2, 1, 16)
+    qs, ts = random_tasks(np.random.default_rng(6), 300, 16, max_len=200)
+    lens = np.array([len(q) for q in qs])
+    long_one = int(np.argmax(lens))
+    limit = int(lens[long_one]) - 1
+    others = [i for i in range(len(qs)) if lens[i] <= limit]
+    res = assert_same(qs, ts, sp, ctx, rows=others, max_qlen=limit, expect=N.ERR_INVALID_ARG)
+    assert res["score"][long_one] == 0 and res["cigar_len"][long_one] == 0
+    rest = [i for i in range(len(qs)) if i != 7]
+    res = assert_same(qs, ts, sp, ctx, rows=rest, q_off_fix=(7, -5), expect=N.ERR_INVALID_ARG)
+    assert res["score"][7] == 0
