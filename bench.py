@@ -54,15 +54,18 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD,
                     help="synthetic workload (dnaln_b200.synth.WORKLOADS); the default is the headline one")
     ap.add_argument("--bw", type=int, default=16, help="SW band half-width (16, or 64 for the mixed-length workload)")
-    ap.add_argument("--sw-form", type=int, default=0, choices=[0, 1, 2],
-                    help="SW kernel form: 0 tuned per context, 1 inter-sequence, 2 intra-sequence (pin it under a "
-                         "profiler, whose serialised replays distort the tuner's timing)")
+    ap.add_argument("--sw-form", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="SW kernel form: 0 tuned per context, 1 inter-sequence, 2 intra-sequence, 3 intra-sequence "
+                         "narrow (pin it under a profiler, whose serialised replays distort the tuner's timing)")
     ap.add_argument("--cigar-per-read", type=int, default=0,
                     help="CIGAR capacity per read of the output buffers (0 = the 2*len+3 bound)")
     ap.add_argument("--serve-requests", type=int, default=1500, help="requests per rate point (--workload serve)")
     ap.add_argument("--serve-lanes", type=int, default=3)
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.5, 0.8],
                     help="offered loads as fractions of the measured capacity (--workload serve)")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the mixed-length (batched vs plain, bw 16 / 64) and serving legs of the default run")
+    ap.add_argument("--leg-requests", type=int, default=600, help="requests per load point of the serving leg")
     return ap.parse_args()
 
 
@@ -147,7 +150,7 @@ def kernel_bytes(kernel: str, st: dict, mean_len: float, bw: int = 16) -> float 
     mins = st["minimizers"] if st.get("minimizers") else 0.18 * mean_len * n
     W = 2 * bw + 1
     cand_per_read = st["candidates"] / max(n, 1)
-    dir_row = max((W + 3) // 4 * 2, (W + 7) // 8 * 4)  # direction-code bytes per query row
+    dir_row = (W + 3) // 4 * 2  # direction-code bytes per query row: ceil(W/4) 16-bit words per alignment
     if kernel == "k_seed_chain_t":  # ASCII in, 16-B bucket per minimizer, 4-B occurrence per anchor,
         # 21-B candidate out, 28 B of per-read offsets / lengths / counts
         return n * mean_len + mins * 16 + (st["anchors"] - st["warp_anchors"]) * 4 + \
@@ -395,6 +398,149 @@ def text_pipeline(ctx, iid, reads, g, p, steps: int) -> dict:
                     "-> SAM text in memory; wall clock per step (map_wait = time the host waited for the GPU)"}
 
 
+MIXED = "mixed-4.6Mbp-1M-50to1000bp"
+
+
+def device_parts(reads, cigar_per_read: int = 0) -> list[dict]:
+    """The workload's batches of 262,144 reads as device tensors (reads, offsets, lengths,
+    name hashes) with their output buffers."""
+    import torch
+    n_reads = len(reads)
+    out = []
+    for a in range(0, n_reads, BATCH):
+        part = reads.slice(a, min(n_reads, a + BATCH))
+        n = len(part)
+        lens = part.seq_len
+        cap = int(np.sum(2 * lens.astype(np.int64) + 3)) if not cigar_per_read else n * cigar_per_read
+        out.append(dict(
+            n=n, cap=cap,
+            seq=torch.from_numpy(part.seq).cuda(),
+            off=torch.from_numpy(np.ascontiguousarray(part.seq_off[:-1])).cuda(),
+            len=torch.from_numpy(lens).cuda(),
+            hash=torch.from_numpy(part.name_hash().view(np.int32)).cuda(),
+            out=torch.empty(n * 40, dtype=torch.uint8, device="cuda"),
+            cig=torch.empty(cap, dtype=torch.int32, device="cuda")))
+    return out
+
+
+def map_device_step(ctx, iid, dev: list[dict], p) -> None:
+    """One step: every batch through dnaln_gpu_map_batch_device (inputs resident in HBM)."""
+    from dnaln_b200 import _native as N
+    L = N.lib()
+    used = C.c_int64()
+    for d in dev:
+        rc = L.dnaln_gpu_map_batch_device(ctx.handle, iid, d["seq"].data_ptr(), d["off"].data_ptr(),
+                                          d["len"].data_ptr(), d["hash"].data_ptr(), d["n"], C.byref(p),
+                                          d["out"].data_ptr(), d["cig"].data_ptr(), d["cap"], C.byref(used))
+        if rc:
+            raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
+
+
+def timed_steps(ctx, iid, dev, p, stream, steps: int, warmup: int) -> float:
+    """Milliseconds per step over `steps` steps after `warmup` untimed ones (CUDA events on
+    the launching stream, synchronized on both sides)."""
+    import torch
+    for _ in range(warmup):
+        map_device_step(ctx, iid, dev, p)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        map_device_step(ctx, iid, dev, p)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def mixed_leg(ctx, stream, seed: int, steps: int, warmup: int) -> dict:
+    """The mixed-length workload (1,000,000 reads, log-uniform 50-1000 bp, 2% with an 8-15 bp
+    deletion, on the 4.6 Mbp genome), inputs resident in HBM, batches of 262,144, at band
+    width 16 and 64: the batched form (short reads one thread each, long reads one thread
+    each longest first, the rest one warp each; SW tasks longest first) against the plain
+    per-batch form (every read one warp, SW tasks in read order)."""
+    import dnaln_b200 as D
+    from dnaln_b200 import synth
+    g, reads, _ = synth.workload(MIXED, seed=seed)
+    iid = ctx.index_build(g)
+    dev = device_parts(reads)
+    out = {"workload": f"{MIXED}: {synth.WORKLOADS[MIXED][2]}, k=15 w=10 A2 B4 O4 E2, batches of 262,144",
+           "reads_per_step": len(reads), "mean_read_len": round(float(np.mean(reads.seq_len)), 1),
+           "steps": steps, "warmup": warmup,
+           "what": "reads/s, inputs resident in HBM, CUDA events; plain = every read one warp, SW tasks in read order"}
+    try:
+        for bw in (16, 64):
+            p = D.default_map_params(bw=bw)
+            ms_b = timed_steps(ctx, iid, dev, p, stream, steps, warmup)
+            ctx.set_option("warp_seed_only", 1)
+            ctx.set_option("length_order", 0)
+            try:
+                ms_p = timed_steps(ctx, iid, dev, p, stream, steps, warmup)
+            finally:
+                ctx.set_option("warp_seed_only", 0)
+                ctx.set_option("length_order", 1)
+            vb, vp = len(reads) / (ms_b / 1e3), len(reads) / (ms_p / 1e3)
+            out[f"bw{bw}"] = {"batched": vb, "plain": vp, "batched_vs_plain": vb / vp,
+                              "ms_per_step": {"batched": ms_b, "plain": ms_p}}
+    finally:
+        ctx.index_free(iid)
+    return out
+
+
+def serve_leg(ctx, seed: int, n_req: int, loads: list[float], lanes: int, bw: int) -> dict:
+    """The serving workload (both indexes resident, Poisson arrivals, requests of log-uniform
+    1-50,000 reads of U[100, 300] bp to either genome): capacity and p50 / p99 latency of the
+    continuously batching server and of the plain one (one lane, one request per batch)."""
+    import dnaln_b200 as D
+    pools = ServePools(seed)
+    iids = [ctx.index_build(g) for g in pools.genomes]
+    try:
+        points, reqs = serve_points(ctx, pools, iids, D.default_map_params(bw=bw), n_req, loads, lanes, seed)
+    finally:
+        for i in iids:
+            ctx.index_free(i)
+    lat = {}
+    for name, pts in points.items():
+        for v in pts:
+            lat[f"{name}@{v['load']}"] = {"p50_ms": round(v["p50_ms"], 3), "p99_ms": round(v["p99_ms"], 3),
+                                          "reads_per_s": v["reads_per_s"]}
+    cap_b, cap_p = points["batched"][0]["reads_per_s"], points["plain"][0]["reads_per_s"]
+    return {"requests_per_point": n_req, "mean_reads_per_request": float(np.mean([r[2] for r in reqs])),
+            "lanes": lanes, "capacity_reads_per_s": {"batched": cap_b, "plain": cap_p},
+            "batched_vs_plain_capacity": cap_b / cap_p, "latency": lat,
+            "what": "load = fraction of that server's own capacity (saturation = all requests at once); "
+                    "batched_at_plain_rates = the batching server at the plain server's offered rates; "
+                    "latency from submit to completion, measured in the library"}
+
+
+def int_roofline(local: int, stream, kernel: str, cells_per_launch: float, avg_launch_ms: float,
+                 inst_per_cell: float | None) -> dict:
+    """Integer roofline of an SW kernel: cells/s against the measured issue rate of the
+    recurrence's instruction mix (dnaln_gpu_int_peak, run here) divided by the cost model's
+    2.5 thread instructions per cell (at least 5 integer instructions per cell, two cells
+    per 16x2 instruction)."""
+    from dnaln_b200 import _native as N
+    L = N.lib()
+    rates = {}
+    for mode, name in ((0, "add_dpxmax3_mix"), (1, "add"), (2, "dpxmax3")):
+        r, ms = C.c_double(), C.c_double()
+        rc = L.dnaln_gpu_int_peak(local, mode, C.c_void_p(stream.cuda_stream), C.byref(r), C.byref(ms))
+        if rc:
+            return {"error": f"dnaln_gpu_int_peak failed ({rc})"}
+        rates[name] = r.value
+    model = 2.5
+    peak_cells = rates["add_dpxmax3_mix"] / model
+    achieved = cells_per_launch / (avg_launch_ms / 1e3)
+    out = {"kernel": kernel, "bound": "int", "achieved_cells_per_s": achieved, "peak_cells_per_s": peak_cells,
+           "frac_int": achieved / peak_cells, "peak_thread_inst_per_s": rates,
+           "model_thread_inst_per_cell": model, "cells_per_launch": cells_per_launch,
+           "what": "peak = measured issue rate of 32-bit add + 16x2 DPX max3 (one to one, every SM, this run) / "
+                   "2.5 thread instructions per cell (5 integer ops per cell, 2 cells per 16x2 op)"}
+    if inst_per_cell:
+        out["thread_inst_per_cell"] = inst_per_cell
+        out["issue_frac"] = achieved * inst_per_cell / rates["add_dpxmax3_mix"]
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import dnaln_b200 as D
@@ -425,28 +571,10 @@ def run_ours(args) -> None:
     parts = [reads.slice(a, b) for a, b in spans]
 
     # ---- device-resident inputs (value) --------------------------------------------
-    dev = []
-    for part in parts:
-        n = len(part)
-        lens = part.seq_len
-        cap = int(np.sum(2 * lens.astype(np.int64) + 3)) if not args.cigar_per_read else n * args.cigar_per_read
-        dev.append(dict(
-            n=n, cap=cap,
-            seq=torch.from_numpy(part.seq).cuda(),
-            off=torch.from_numpy(np.ascontiguousarray(part.seq_off[:-1])).cuda(),
-            len=torch.from_numpy(lens).cuda(),
-            hash=torch.from_numpy(part.name_hash().view(np.int32)).cuda(),
-            out=torch.empty(n * 40, dtype=torch.uint8, device="cuda"),
-            cig=torch.empty(cap, dtype=torch.int32, device="cuda")))
-    used = C.c_int64()
+    dev = device_parts(reads, args.cigar_per_read)
 
     def step_device():
-        for d in dev:
-            rc = L.dnaln_gpu_map_batch_device(ctx.handle, iid, d["seq"].data_ptr(), d["off"].data_ptr(),
-                                              d["len"].data_ptr(), d["hash"].data_ptr(), d["n"], C.byref(p),
-                                              d["out"].data_ptr(), d["cig"].data_ptr(), d["cap"], C.byref(used))
-            if rc:
-                raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
+        map_device_step(ctx, iid, dev, p)
 
     def barrier():
         if dist is not None:
@@ -618,11 +746,26 @@ def run_ours(args) -> None:
             traffic = issue_active = None
     cells = st["cells"]
     sw_ms = st["ms_sw_score"] + st["ms_sw_tb"]
-    kernels = {k: {"launches_per_step": n / PROFILE_STEPS, "ms_per_step": t / PROFILE_STEPS}
-               for k, (n, t) in sorted(breakdown.items(), key=lambda kv: -kv[1][1])}
-    kernels_total = sum(v["ms_per_step"] for v in kernels.values())
-    for v in kernels.values():
-        v["share"] = v["ms_per_step"] / kernels_total
+    ranked = sorted(breakdown.items(), key=lambda kv: -kv[1][1])
+    kernels_total = sum(t for _, (_, t) in ranked) / PROFILE_STEPS
+    kernels = {k: {"launches_per_step": n / PROFILE_STEPS, "ms_per_step": t / PROFILE_STEPS,
+                   "share": t / PROFILE_STEPS / kernels_total} for k, (n, t) in ranked[:8]}
+    rest = ranked[8:]
+    if rest:
+        kernels["(other kernels)"] = {"kernels": len(rest), "ms_per_step": sum(t for _, (_, t) in rest) / PROFILE_STEPS,
+                                      "share": sum(t for _, (_, t) in rest) / PROFILE_STEPS / kernels_total}
+    inst_per_cell = None  # thread instructions per cell of the dominant SW kernel, same ncu capture
+    if tf.exists():
+        try:
+            inst_per_cell = json.loads(tf.read_text()).get("thread_inst_per_cell", {}).get(args.workload, {}).get(
+                dom.split("<")[0])
+        except (OSError, ValueError, AttributeError):
+            inst_per_cell = None
+    roof_int = None
+    if dom.startswith("k_sw_u2<tb>") or dom.startswith("k_sw_wide<tb>"):
+        W = 2 * args.bw + 1
+        cells_per_launch = st["sw_tasks_tb"] * mean_len * W / launches
+        roof_int = int_roofline(local, stream, dom, cells_per_launch, avg_launch_ms, inst_per_cell)
 
     out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -658,6 +801,17 @@ def run_ours(args) -> None:
         out["e2e_text"] = e2e_text
     if rank == 0:
         out["index"]["image"] = index_image_round_trip(ctx, iid)
+    if roof_int:
+        out["roofline_int"] = roof_int
+    # the other two measured workloads, compact (they close the line, so a truncated log
+    # still shows them): mixed lengths batched vs plain, and the request server
+    if rank == 0 and world == 1 and args.workload == WORKLOAD and not args.no_legs:
+        ctx.index_free(iid)
+        del dev, host
+        torch.cuda.empty_cache()
+        leg_steps, leg_warm = max(2, min(args.steps, 5)), 2
+        out["mixed"] = mixed_leg(ctx, stream, args.seed, leg_steps, leg_warm)
+        out["serve"] = serve_leg(ctx, args.seed, args.leg_requests, args.serve_loads, args.serve_lanes, args.bw)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(g, reads, p)
     if rank == 0:
@@ -767,6 +921,39 @@ def replay(srv, pools: ServePools, iids, reqs, rate: float | None, p) -> dict:
             "lane_ms": {k[3:]: st[k] for k in ("ms_form", "ms_gather", "ms_device", "ms_scatter", "ms_complete")}}
 
 
+def serve_points(ctx, pools: ServePools, iids, p, n_req: int, loads: list[float], lanes: int, seed: int):
+    """Replays the seeded request stream through the continuously batching server (`lanes`
+    lanes, requests coalesced) and the plain one (one lane, one request per batch): first all
+    at once (capacity), then at Poisson arrivals of each fraction in `loads` of that server's
+    capacity; then the batching server at the plain server's rates. Returns (points by
+    server, the requests)."""
+    from dnaln_b200.serve import Server
+    warm = pools.stream(64, seed + 99)
+    reqs = pools.stream(n_req, seed + 100)
+    modes = {"batched": dict(lanes=lanes, coalesce=True),
+             "plain": dict(lanes=1, coalesce=False, max_batch_reads=BATCH)}
+    points = {}
+    for name, kw in modes.items():
+        with Server(ctx, **kw) as srv:
+            replay(srv, pools, iids, warm, None, p)        # warm-up: the lanes' staging and scratch
+            replay(srv, pools, iids, reqs, None, p)        # grow to the stream's batch sizes
+            sat = replay(srv, pools, iids, reqs, None, p)  # all requests at once: capacity
+            cap_req = sat["requests"] / sat["wall_s"]
+            pts = [dict(sat, load="saturation")]
+            for frac in loads:
+                r = replay(srv, pools, iids, reqs, frac * cap_req, p)
+                r["load"] = frac
+                pts.append(r)
+            points[name] = pts
+    # offered loads of the plain server, replayed on the batched one: same absolute rates
+    with Server(ctx, **modes["batched"]) as srv:
+        replay(srv, pools, iids, reqs, None, p)
+        plain_cap = points["plain"][0]["requests"] / points["plain"][0]["wall_s"]
+        points["batched_at_plain_rates"] = [dict(replay(srv, pools, iids, reqs, f * plain_cap, p),
+                                                 load=f"{f} x plain capacity") for f in loads]
+    return points, reqs
+
+
 def run_serve(args) -> None:
     """The serving workload: both indexes resident, Poisson arrivals at a swept rate,
     requests of log-uniform 1..50,000 reads (length uniform in [100, 300]) to either genome.
@@ -786,34 +973,11 @@ def run_serve(args) -> None:
     build_s = time.perf_counter() - t_ix
     p = D.default_map_params(bw=args.bw)
     n_req = args.serve_requests
-    warm = pools.stream(64, args.seed + 99)
-    reqs = pools.stream(n_req, args.seed + 100)
-    mean_reads = float(np.mean([r[2] for r in reqs]))
     clocks = ClockSampler(local)
     clocks.start()
-    modes = {"batched": dict(lanes=args.serve_lanes, coalesce=True),
-             "plain": dict(lanes=1, coalesce=False, max_batch_reads=BATCH)}
-    points = {}
-    for name, kw in modes.items():
-        with Server(ctx, **kw) as srv:
-            replay(srv, pools, iids, warm, None, p)        # warm-up: the lanes' staging and scratch
-            replay(srv, pools, iids, reqs, None, p)        # grow to the stream's batch sizes
-            sat = replay(srv, pools, iids, reqs, None, p)  # all requests at once: capacity
-            cap_req = sat["requests"] / sat["wall_s"]
-            pts = [dict(sat, load="saturation")]
-            for frac in args.serve_loads:
-                r = replay(srv, pools, iids, reqs, frac * cap_req, p)
-                r["load"] = frac
-                pts.append(r)
-            points[name] = pts
+    points, reqs = serve_points(ctx, pools, iids, p, n_req, args.serve_loads, args.serve_lanes, args.seed)
     clk = clocks.result()
-    # offered loads of the plain server, replayed on the batched one: same absolute rates
-    with Server(ctx, **modes["batched"]) as srv:
-        replay(srv, pools, iids, reqs, None, p)
-        plain_cap = points["plain"][0]["requests"] / points["plain"][0]["wall_s"]
-        same = [dict(replay(srv, pools, iids, reqs, f * plain_cap, p), load=f"{f} x plain capacity")
-                for f in args.serve_loads]
-    points["batched_at_plain_rates"] = same
+    mean_reads = float(np.mean([r[2] for r in reqs]))
     head = points["batched"][0]
     out = {"metric": "reads/s (served)", "value": head["reads_per_s"], "unit": "reads/s", "n_gpus": 1,
            "steps": len(args.serve_loads) + 1, "warmup": 1, "ms_per_step": 1e3 * head["wall_s"],

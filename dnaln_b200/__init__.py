@@ -245,6 +245,12 @@ class Context:
         """Tuning switch (sub_batch, warp_seed_only, dir_cap_bytes); results do not change."""
         self._check(self._lib.dnaln_gpu_set_option(self._h, name.encode(), int(value)))
 
+    def seed_tuning(self) -> dict:
+        """The reads-per-block choice of the thread-per-read seeding kernel (dnaln_gpu_seed_tuning)."""
+        t = N.SeedTuning()
+        self._check(self._lib.dnaln_gpu_seed_tuning(self._h, C.byref(t)))
+        return {f: getattr(t, f) for f, _ in N.SeedTuning._fields_}
+
     def sw_tuning(self) -> list[dict]:
         """The SW kernel forms chosen so far (dnaln_gpu_sw_tuning)."""
         n = C.c_int32()

@@ -16,9 +16,10 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "libdnaln_b200.so"
 SYNTH_LIB_PATH = Path(__file__).resolve().parent / "libdnaln_synth.so"
 
-OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_CAPACITY, ERR_NO_DEVICE, ERR_DEVICE, ERR_NOT_FOUND, ERR_IO = range(9)
+OK, ERR_INVALID_ARG, ERR_CUDA, ERR_OOM, ERR_CAPACITY, ERR_NO_DEVICE, ERR_DEVICE, ERR_NOT_FOUND, ERR_IO, \
+    ERR_CANCELLED = range(10)
 ERR_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "CUDA", 3: "OOM", 4: "CAPACITY", 5: "NO_DEVICE", 6: "DEVICE",
-             7: "NOT_FOUND", 8: "IO"}
+             7: "NOT_FOUND", 8: "IO", 9: "CANCELLED"}
 
 
 class ScoreParams(C.Structure):
@@ -56,7 +57,7 @@ class Stats(C.Structure):
                [(n, C.c_double) for n in ("ms_seed", "ms_chain", "ms_sw_score", "ms_sw_tb", "ms_post", "ms_h2d",
                                           "ms_d2h", "ms_total")] + \
                [(n, C.c_uint64) for n in ("launches", "warp_reads", "warp_minimizers", "warp_anchors",
-                                          "warp_bases", "long_reads", "graph_launches")]
+                                          "warp_bases", "long_reads", "graph_launches", "batch_retries")]
 
 
 class KernelTime(C.Structure):
@@ -65,7 +66,13 @@ class KernelTime(C.Structure):
 
 class SwTuning(C.Structure):
     _fields_ = [("W", C.c_int32), ("traceback", C.c_int32), ("len_bucket", C.c_int32), ("form", C.c_int32),
-                ("ms_inter", C.c_double), ("ms_intra", C.c_double), ("tasks", C.c_int64)]
+                ("ms_inter", C.c_double), ("ms_intra", C.c_double), ("tasks", C.c_int64), ("ms_narrow", C.c_double),
+                ("lanes_per_pair", C.c_int32), ("pad_", C.c_int32)]
+
+
+class SeedTuning(C.Structure):
+    _fields_ = [("tuned", C.c_int32), ("reads_per_block", C.c_int32), ("ms_64", C.c_double), ("ms_128", C.c_double),
+                ("reads", C.c_int64)]
 
 
 class ServeParams(C.Structure):
@@ -126,6 +133,7 @@ SIGNATURES = {
     "dnaln_gpu_set_sub_batch": (C.c_int, [P, i64]),
     "dnaln_gpu_set_option": (C.c_int, [P, C.c_char_p, i64]),
     "dnaln_gpu_sw_tuning": (C.c_int, [P, C.POINTER(SwTuning), i32, C.POINTER(i32)]),
+    "dnaln_gpu_seed_tuning": (C.c_int, [P, C.POINTER(SeedTuning)]),
     "dnaln_gpu_map_submit": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64, C.POINTER(i64),
                              C.POINTER(i64)]),
     "dnaln_gpu_map_wait": (C.c_int, [P, i64]),
@@ -144,6 +152,7 @@ SIGNATURES = {
     "dnaln_serve_submit": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64, C.POINTER(i64),
                                      C.POINTER(i64)]),
     "dnaln_serve_wait": (C.c_int, [P, i64, C.POINTER(dbl)]),
+    "dnaln_serve_cancel": (C.c_int, [P, i64]),
     "dnaln_serve_get_stats": (C.c_int, [P, C.POINTER(ServeStats)]),
     "dnaln_serve_reset_stats": (C.c_int, [P]),
     "dnaln_serve_last_error": (C.c_char_p, [P]),
@@ -153,6 +162,7 @@ SIGNATURES = {
     "dnaln_gpu_chain": (C.c_int, [P, P, P, P, P, i64, i32, C.POINTER(ChainParams), P, P, P, P, P, P, P]),
     "dnaln_gpu_align": (C.c_int, [P, P, P, P, P, P, P, i64, i32, C.POINTER(ScoreParams), P, P, i64,
                                   C.POINTER(i64)]),
+    "dnaln_gpu_int_peak": (C.c_int, [i32, i32, P, C.POINTER(dbl), C.POINTER(dbl)]),
     "dnaln_gpu_align_noalloc": (C.c_int, [P, P, P, P, P, P, i64, i32, i32, C.POINTER(ScoreParams), P, P, i64, P]),
     "dnaln_gpu_map_batch": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64, C.POINTER(i64)]),
     "dnaln_gpu_map_batch_device": (C.c_int, [P, i32, P, P, P, P, i64, C.POINTER(MapParams), P, P, i64,

@@ -163,13 +163,22 @@ struct dnaln_ctx {
   bool warp_seed_only = false;  // option: every read through the warp-per-read seeding kernels
   bool length_order = true;     // option: SW tasks of mixed-length batches run longest first
   bool long_thread = true;      // option: listed long reads one thread each before the warp kernels
+  bool stealing = true;         // option: the listed-read kernels take work by atomic claims
+  // reads per block of the thread-per-read seeding kernel: option "seed_block" (0 = tuned
+  // on the first batch of at least kSeedTuneReads reads, else 64 or 128) and the tuning
+  int seed_block = 0;
+  dnaln_seed_tuning seed_tune{};
   // SW kernel form per (band width, traceback, read-length bucket): option "sw_form" 0 =
   // tuned on the first batch that needs it, 1 = inter-sequence, 2 = intra-sequence
   int sw_mode = 0;
   std::map<int, dnaln_sw_tuning> sw_tune;
-  cudaEvent_t tune_ev[3] = {};
+  cudaEvent_t tune_ev[kSwForms + 1] = {};
   int* h_tune = nullptr;  // pinned read-back of a device task count
   int64_t pool_cap = 0;   // entries of the warp-path chaining pool (grown from the batches' use)
+  int64_t pool_min = int64_t(1) << 16;  // the pool's floor (option "chain_pool" lowers it)
+  // fault injection on the host (option "fail_alloc_after"): the device allocation after
+  // this many more succeed fails as if the device were out of memory; -1 = off
+  int64_t fail_alloc_after = -1;
   // CUDA graphs of batches (run_map): cache by launch key, keys seen once, and the buffer
   // epoch, bumped whenever a buffer a graph may reference is reallocated or rewritten
   bool graphs = true, capturing = false;
@@ -190,6 +199,8 @@ struct dnaln_ctx {
 };
 
 namespace {
+
+constexpr int64_t kSeedTuneReads = 32768;  // smallest batch the reads-per-block tuner times
 
 int fail(dnaln_ctx* c, int code, const char* fmt, ...) {
   char buf[512];
@@ -224,6 +235,10 @@ T* dbuf(dnaln_ctx* c, const char* name, size_t count) {
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
+    if (c->fail_alloc_after >= 0 && c->fail_alloc_after-- == 0) {
+      fail(c, DNALN_ERR_OOM, "out of device memory allocating %zu bytes for %s (injected)", need, name);
+      return nullptr;
+    }
     size_t cap = need + need / 4;
     if (cudaMalloc(&b.p, cap) != cudaSuccess) {
       cudaGetLastError();
@@ -464,20 +479,23 @@ int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks,
   if (!fb) return DNALN_ERR_OOM;
   const KernelTrace kt = tracer(c);
   // the kernel form: fixed by the option, or tuned once per (W, traceback, length bucket)
-  // by timing both forms on the first chunk (they give identical results, so the second
-  // run only rewrites the same outputs)
-  SwForm form = kSwInter;
+  // by timing every form the band width has on the first chunk (they give identical
+  // results, so each later run only rewrites the same outputs)
+  std::vector<SwForm> forms;
+  for (int f = 0; f < kSwForms; ++f)
+    if (sw_has_form(sp.W, bytes_ok, static_cast<SwForm>(f))) forms.push_back(static_cast<SwForm>(f));
+  SwForm form = forms.empty() ? kSwInter : forms.front();
   bool tune = false;
   const int bucket = rows_max <= 256 ? 0 : (rows_max <= 1024 ? 1 : 2);
   const int key = sp.W | (tb ? 1 : 0) << 10 | bucket << 11;
-  if (sw_has_both_forms(sp.W, bytes_ok)) {
-    if (c->sw_mode == 1) {
-      form = kSwInter;
-    } else if (c->sw_mode == 2) {
-      form = kSwIntra;
+  if (forms.size() > 1) {
+    const SwForm pinned = c->sw_mode == 1 ? kSwInter : (c->sw_mode == 2 ? kSwIntra : (c->sw_mode == 3 ? kSwIntraNarrow
+                                                                                                      : kSwInter));
+    if (c->sw_mode != 0 && std::find(forms.begin(), forms.end(), pinned) != forms.end()) {
+      form = pinned;
     } else {
       auto it = c->sw_tune.find(key);
-      if (it != c->sw_tune.end()) form = it->second.form ? kSwIntra : kSwInter;
+      if (it != c->sw_tune.end()) form = static_cast<SwForm>(it->second.form);
       else if (c->capturing) return fail(c, DNALN_ERR_CUDA, "capture stopped: a kernel form is still to be tuned");
       else tune = true;
     }
@@ -491,30 +509,41 @@ int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks,
       return ok;
     };
     if (b == 0 && tune) {
-      // both forms once untimed first: a kernel's first launch in a process also loads it
-      if (!run(kSwInter) || !run(kSwIntra)) return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
+      // every form once untimed first: a kernel's first launch in a process also loads it
+      for (SwForm f : forms)
+        if (!run(f)) return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
+      double ms[kSwForms] = {0, 0, 0};
       CK(cudaEventRecord(c->tune_ev[0], c->st));
-      if (!run(kSwInter)) return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
-      CK(cudaEventRecord(c->tune_ev[1], c->st));
-      if (!run(kSwIntra)) return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
-      CK(cudaEventRecord(c->tune_ev[2], c->st));
+      for (size_t x = 0; x < forms.size(); ++x) {
+        if (!run(forms[x])) return fail(c, DNALN_ERR_DEVICE, "SW launch without its scratch (W=%d)", sp.W);
+        CK(cudaEventRecord(c->tune_ev[1 + x], c->st));
+      }
       int64_t live = cnt;
       if (n_dev) {
         CK(cudaMemcpyAsync(c->h_tune, n_dev, sizeof(int), cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
         live = std::min<int64_t>(cnt, *c->h_tune);
       } else {
-        CK(cudaEventSynchronize(c->tune_ev[2]));
+        CK(cudaEventSynchronize(c->tune_ev[forms.size()]));
       }
       dnaln_sw_tuning t{};
       t.W = sp.W;
       t.traceback = tb ? 1 : 0;
       t.len_bucket = bucket;
-      t.ms_inter = ev_ms(c->tune_ev[0], c->tune_ev[1]);
-      t.ms_intra = ev_ms(c->tune_ev[1], c->tune_ev[2]);
-      t.form = t.ms_intra < t.ms_inter ? 1 : 0;
+      double best = 1e30;
+      for (size_t x = 0; x < forms.size(); ++x) {
+        ms[forms[x]] = ev_ms(c->tune_ev[x], c->tune_ev[1 + x]);
+        if (ms[forms[x]] < best) {
+          best = ms[forms[x]];
+          form = forms[x];
+        }
+      }
+      t.ms_inter = sw_has_form(sp.W, bytes_ok, kSwInter) ? ms[kSwInter] : -1.0;
+      t.ms_intra = sw_has_form(sp.W, bytes_ok, kSwIntra) ? ms[kSwIntra] : -1.0;
+      t.ms_narrow = sw_has_form(sp.W, bytes_ok, kSwIntraNarrow) ? ms[kSwIntraNarrow] : -1.0;
+      t.form = form;
+      t.lanes_per_pair = sw_lanes_per_pair(sp.W, form);
       t.tasks = live;
-      form = t.form ? kSwIntra : kSwInter;
       c->sw_tune[key] = t;
       continue;
     }
@@ -569,6 +598,9 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
   CK(cudaMemsetAsync(info, 0, 10 * sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
   CK(cudaMemsetAsync(c->d_count, 0, 4 * sizeof(int), st));
+  // work-stealing claim counters: [0] long-read kernel, [1] warp chaining kernel
+  DBUF(claims, int, "claims", 2);
+  CK(cudaMemsetAsync(claims, 0, 2 * sizeof(int), st));
   unsigned long long* ctr = info + 1;  // cells, mapped, candidates (map.cuh)
   kt.begin(st, "k_len64");
   k_len64<<<nblk(n + 1), 256, 0, st>>>(d_seq_len, n, len64, info);
@@ -624,14 +656,44 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
     launch_encode_reads(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, codes);
     kt.end(st);
     c->stats.launches += 1;
-    kt.begin(st, "k_seed_chain_t");
-    const bool ok = launch_seed_chain_thread(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, n, ix.dev, sp, cp, cand,
-                                             cb, n_min, n_anchor, n_anc_t, big_list, big_n, c->d_err);
-    kt.end(st);
-    if (!ok) return fail(c, DNALN_ERR_CUDA, "thread-per-read seeding kernel could not be configured");
+    const auto seed_t = [&](int rpb) {
+      return launch_seed_chain_thread(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, n, ix.dev, sp, cp, cand, cb,
+                                      n_min, n_anchor, n_anc_t, big_list, big_n, c->d_err, rpb);
+    };
+    int rpb = c->seed_block ? c->seed_block : (c->seed_tune.tuned ? c->seed_tune.reads_per_block : 0);
+    if (rpb == 0 && (n < kSeedTuneReads || c->capturing)) rpb = 128;  // too small to time, or no host waits now
+    if (rpb == 0) {
+      // the reads-per-block tuner: each block size once untimed (a kernel's first launch
+      // also loads it), then each timed; every run rewrites the same outputs (the list of
+      // reads handed on is cleared before each), so the last run's stand
+      const int sizes[2] = {64, 128};
+      for (int x = 0; x < 2; ++x) {
+        CK(cudaMemsetAsync(big_n, 0, sizeof(int), st));
+        if (!seed_t(sizes[x])) return fail(c, DNALN_ERR_CUDA, "thread-per-read seeding kernel could not be configured");
+      }
+      for (int x = 0; x < 2; ++x) {
+        CK(cudaMemsetAsync(big_n, 0, sizeof(int), st));
+        CK(cudaEventRecord(c->tune_ev[x], st));
+        if (!seed_t(sizes[x])) return fail(c, DNALN_ERR_CUDA, "thread-per-read seeding kernel could not be configured");
+        CK(cudaEventRecord(c->tune_ev[x + 2], st));
+      }
+      CK(cudaEventSynchronize(c->tune_ev[3]));
+      dnaln_seed_tuning& t = c->seed_tune;
+      t.ms_64 = ev_ms(c->tune_ev[0], c->tune_ev[2]);
+      t.ms_128 = ev_ms(c->tune_ev[1], c->tune_ev[3]);
+      t.reads_per_block = t.ms_64 < t.ms_128 ? 64 : 128;
+      t.reads = n;
+      t.tuned = 1;
+      c->stats.launches += 3;
+    } else {
+      kt.begin(st, "k_seed_chain_t");
+      const bool ok = seed_t(rpb);
+      kt.end(st);
+      if (!ok) return fail(c, DNALN_ERR_CUDA, "thread-per-read seeding kernel could not be configured");
+    }
     if (c->long_thread && seed_long_supported(sp, cp) && max_len > seed_thread_max_len()) {
       // long reads one thread each, in length order; what exceeds its bounds goes on
-      const int64_t lt = seed_long_threads(n);
+      const int64_t lt = seed_long_threads(n, c->stealing);
       DBUF(lscr, uint32_t, "long_scratch", seed_long_scratch_words(lt));
       DBUF(big2, int32_t, "big2_list", n);
       const int32_t* order = big_list;
@@ -654,7 +716,8 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
       }
       kt.begin(st, "k_seed_chain_tl");
       if (!launch_seed_chain_long(st, d_seq_len, pofs, codes, order, big_n, lt, ix.dev, sp, cp, cand, cb, n_min,
-                                  n_anchor, n_anc_t, lscr, big2, c->d_count + 3, seed_thread_max_len(), c->d_err))
+                                  n_anchor, n_anc_t, lscr, big2, c->d_count + 3, seed_thread_max_len(),
+                                  c->stealing ? claims : nullptr, c->d_err))
         return fail(c, DNALN_ERR_CUDA, "long-read seeding kernel could not be configured");
       kt.end(st);
       warp_list = big2;
@@ -698,7 +761,7 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
   // pass 2 of the warp path: anchors, chains, candidates; the scratch of reads with many
   // anchors comes from a pool (sized from the previous batches; a batch that outgrows it
   // is mapped again with the size it asked for)
-  const int64_t pool_cap = std::max<int64_t>(c->pool_cap, 1 << 16);
+  const int64_t pool_cap = std::max<int64_t>(c->pool_cap, c->pool_min);
   AnchorScratch as;
   as.keys = dbuf<uint64_t>(c, "a_keys", pool_cap);
   as.f = dbuf<int32_t>(c, "a_f", pool_cap);
@@ -717,7 +780,8 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
   CK(cudaEventRecord(c->ev[kEvChain0], st));
   kt.begin(st, thread_path ? "k_chain_map<list>" : "k_chain_map");
   launch_chain_map(st, pofs, d_seq_len, n, thread_path ? warp_list : nullptr, thread_path ? warp_n : nullptr, n_min,
-                   n_anchor, mb, ix.dev, cp, cand, as, pool_top, pool_cap, cb, c->d_err);
+                   n_anchor, mb, ix.dev, cp, cand, as, pool_top, pool_cap, cb, c->stealing ? claims + 1 : nullptr,
+                   c->d_err);
   kt.end(st);
   CK(cudaEventRecord(c->ev[kEvChain1], st));
   CK(cudaGetLastError());
@@ -830,6 +894,7 @@ int map_finish(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_s
     // and map the batch again (outputs are rewritten in full; counters are not yet added)
     c->pool_cap = std::max<int64_t>(c->pool_cap, pool_used + pool_used / 4 + 1024);
     if (hint.retry) return fail(c, DNALN_ERR_DEVICE, "chaining pool still too small after growing it");
+    c->stats.batch_retries += 1;
     BatchHints again = hint;
     again.retry = true;
     again.bases = B;
@@ -889,7 +954,8 @@ std::string graph_key(const dnaln_ctx* c, const IndexRes& ix, const char* d_seq,
   put(ptrs, sizeof ptrs);
   const int64_t nums[] = {n, hint.seq_base, hint.bases, hint.max_len, hint.cigar_base, cigar_cap, c->pool_cap,
                           static_cast<int64_t>(c->dir_cap_bytes), c->sw_mode, c->warp_seed_only, c->long_thread,
-                          c->length_order};
+                          c->length_order, c->stealing, c->seed_block,
+                          c->seed_tune.tuned ? c->seed_tune.reads_per_block : 0};
   put(nums, sizeof nums);
   put(&p, sizeof p);
   return k;
@@ -991,6 +1057,10 @@ IndexRes* find_index(dnaln_ctx* c, int32_t id) {
 }
 
 int dalloc(dnaln_ctx* c, DevBuf& b, size_t bytes) {
+  if (c->fail_alloc_after >= 0 && c->fail_alloc_after-- == 0) {
+    b.p = nullptr;
+    return fail(c, DNALN_ERR_OOM, "out of device memory allocating %zu bytes for the index (injected)", bytes);
+  }
   if (cudaMalloc(&b.p, bytes ? bytes : 1) != cudaSuccess) {
     cudaGetLastError();
     b.p = nullptr;
@@ -1417,7 +1487,7 @@ int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
     return DNALN_OK;
   }
   if (k == "sw_form") {
-    if (value < 0 || value > 2) return fail(c, DNALN_ERR_INVALID_ARG, "sw_form must be 0 (tuned), 1 or 2");
+    if (value < 0 || value > 3) return fail(c, DNALN_ERR_INVALID_ARG, "sw_form must be 0 (tuned), 1, 2 or 3");
     c->sw_mode = static_cast<int>(value);
     return DNALN_OK;
   }
@@ -1427,6 +1497,26 @@ int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
   }
   if (k == "length_order") {
     c->length_order = value != 0;
+    return DNALN_OK;
+  }
+  if (k == "seed_block") {
+    if (value != 0 && value != 64 && value != 128)
+      return fail(c, DNALN_ERR_INVALID_ARG, "seed_block must be 0 (tuned), 64 or 128");
+    c->seed_block = static_cast<int>(value);
+    return DNALN_OK;
+  }
+  if (k == "work_stealing") {
+    c->stealing = value != 0;
+    return DNALN_OK;
+  }
+  if (k == "chain_pool") {  // entries of the chaining pool from now on (a floor and a start)
+    if (value < 64) return fail(c, DNALN_ERR_INVALID_ARG, "chain_pool must be >= 64");
+    c->pool_min = value;
+    c->pool_cap = value;
+    return DNALN_OK;
+  }
+  if (k == "fail_alloc_after") {
+    c->fail_alloc_after = value < 0 ? -1 : value;
     return DNALN_OK;
   }
   if (k == "dir_cap_bytes") {
@@ -1446,6 +1536,13 @@ int dnaln_gpu_sw_tuning(const dnaln_ctx* cc, dnaln_sw_tuning* out, int32_t cap, 
     ++i;
   }
   *n_out = i;
+  return DNALN_OK;
+}
+
+int dnaln_gpu_seed_tuning(const dnaln_ctx* cc, dnaln_seed_tuning* out) {
+  if (!cc || !out) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> ctx_lock(cc->mu);
+  *out = cc->seed_tune;
   return DNALN_OK;
 }
 

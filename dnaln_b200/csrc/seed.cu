@@ -942,11 +942,22 @@ __global__ void __launch_bounds__(kChainWarps * 32, 8)
                 const int32_t* __restrict__ list, const int* __restrict__ list_n, const int32_t* __restrict__ n_min,
                 const int64_t* __restrict__ n_anchor, MinBuf mb, DevIndex ix, ChainParamsDev cp, CandParams cand,
                 AnchorScratch as, unsigned long long* __restrict__ pool_top, int64_t pool_cap, CandBuf cb,
-                uint32_t* __restrict__ err) {
+                int* __restrict__ claim, uint32_t* __restrict__ err) {
   __shared__ ChainSmem sm[kChainWarps];
-  const int wib = threadIdx.x >> 5;
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t gw = static_cast<int64_t>(blockIdx.x) * kChainWarps + wib;
   const int64_t m = list ? static_cast<int64_t>(*list_n) : n;
+  if (claim) {  // work stealing: the warp takes the next read when it is done with its last
+    for (;;) {
+      int x = 0;
+      if (lane == 0) x = atomicAdd(claim, 1);
+      x = __shfl_sync(0xffffffffu, x, 0);
+      if (x >= m) break;
+      chain_read(list ? list[x] : x, pofs, seq_len, n_min, n_anchor, mb, ix, cp, cand, as, pool_top, pool_cap, cb,
+                 err, sm[wib]);
+    }
+    return;
+  }
   for (int64_t x = gw; x < m; x += static_cast<int64_t>(gridDim.x) * kChainWarps)
     chain_read(list ? list[x] : x, pofs, seq_len, n_min, n_anchor, mb, ix, cp, cand, as, pool_top, pool_cap, cb, err,
                sm[wib]);
@@ -1031,12 +1042,26 @@ void launch_seed_list(cudaStream_t st, const char* seq, const int64_t* seq_off, 
 void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* list,
                       const int* list_n, const int32_t* n_min, const int64_t* n_anchor, MinBuf mb,
                       const DevIndex& ix, const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as,
-                      unsigned long long* pool_top, int64_t pool_cap, CandBuf cb, uint32_t* err) {
+                      unsigned long long* pool_top, int64_t pool_cap, CandBuf cb, int* claim, uint32_t* err) {
   if (n <= 0) return;
-  // grid-stride over a count that may be known on the device only: a few resident waves
-  const int64_t blocks = std::min<int64_t>((n + kChainWarps - 1) / kChainWarps, int64_t{16} * device_sm_count());
+  // a count that may be known on the device only: with work stealing the resident blocks,
+  // otherwise a grid-stride over a few resident waves
+  int64_t cap = int64_t{16} * device_sm_count();
+  if (claim) {
+    static std::atomic<int> resident[kMaxDevices];
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices) {
+      v = resident[dev].load(std::memory_order_relaxed);
+      if (v <= 0 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_chain_map, kChainWarps * 32, 0) == cudaSuccess &&
+          v > 0)
+        resident[dev].store(v, std::memory_order_relaxed);
+    }
+    cudaGetLastError();
+    cap = int64_t{v > 0 ? v : 8} * device_sm_count();
+  }
+  const int64_t blocks = std::min<int64_t>((n + kChainWarps - 1) / kChainWarps, cap);
   k_chain_map<<<static_cast<unsigned>(blocks), kChainWarps * 32, 0, st>>>(
-      pofs, seq_len, n, list, list_n, n_min, n_anchor, mb, ix, cp, cand, as, pool_top, pool_cap, cb, err);
+      pofs, seq_len, n, list, list_n, n_min, n_anchor, mb, ix, cp, cand, as, pool_top, pool_cap, cb, claim, err);
 }
 
 void launch_sketch_codes(cudaStream_t st, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,

@@ -137,10 +137,13 @@ void launch_seed_list(cudaStream_t st, const char* seq, const int64_t* seq_off, 
 // list[0, *list_n) (n = the list's size). n_anchor[r] = the read's anchor count (pass 1);
 // reads of more than 32 anchors take their scratch (as, pool_cap entries per array) from
 // the pool by an atomic add on *pool_top; past the capacity a read sets kErrChainPool.
+// With `claim` (an int zeroed by the caller) the grid is the resident warps only and each
+// warp takes its next read by an atomic add on *claim (work stealing); without, the warps
+// stride over the reads.
 void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_len, int64_t n, const int32_t* list,
                       const int* list_n, const int32_t* n_min, const int64_t* n_anchor, MinBuf mb,
                       const DevIndex& ix, const ChainParamsDev& cp, const CandParams& cand, AnchorScratch as,
-                      unsigned long long* pool_top, int64_t pool_cap, CandBuf cb, uint32_t* err);
+                      unsigned long long* pool_top, int64_t pool_cap, CandBuf cb, int* claim, uint32_t* err);
 
 // Codes of both strands of reads [0, n) (seed_thread.cu): forward at codes[2*pofs[r]],
 // reverse complement right after it (src/mapper.cpp:88-99), from the ASCII reads.
@@ -151,29 +154,33 @@ void launch_encode_reads(cudaStream_t st, const char* seq, const int64_t* seq_of
 // admit, from their ASCII bytes (the codes in HBM are launch_encode_reads' job), writing
 // candidates of the admitted reads, n_min, n_anc_t (their anchor counts, for statistics)
 // and n_anchor = 0 (no scratch); the others are appended to big_list (count in *big_n,
-// zeroed by the caller) for launch_seed_list / launch_chain_map. Returns false, launching
-// nothing, when the parameters are outside the path's range.
+// zeroed by the caller) for launch_seed_list / launch_chain_map. reads_per_block: 64 or
+// 128 (threads per block; same results). Returns false, launching nothing, when the
+// parameters are outside the path's range.
 bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp);
 int seed_thread_max_len();  // the longest read the short thread kernel stages
 bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
                               const int32_t* seq_len, int64_t n, const DevIndex& ix, const SeedParams& sp,
                               const ChainParamsDev& cp,
                               const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
-                              int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err);
+                              int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err,
+                              int reads_per_block = 128);
 
 // Long reads, one thread each (seed_long.cu): the reads of list[0, *list_n) longer than
 // min_len (typically those the short kernel listed) with their state in `scratch`
 // (seed_long_scratch_words(threads) words); the others, and reads past its bounds, go to
 // next_list (count *next_n) for the warp kernels.
-// threads = seed_long_threads(upper bound of the list length).
+// threads = seed_long_threads(upper bound of the list length, stealing). With `claim` (an
+// int zeroed by the caller; then threads must come from seed_long_threads(n, true)) the
+// warps take 32 list positions at a time by an atomic add on *claim (work stealing).
 bool seed_long_supported(const SeedParams& sp, const ChainParamsDev& cp);
-int64_t seed_long_threads(int64_t n_max);
+int64_t seed_long_threads(int64_t n_max, bool stealing);
 size_t seed_long_scratch_words(int64_t threads);
 bool launch_seed_chain_long(cudaStream_t st, const int32_t* seq_len, const int64_t* pofs, const uint8_t* codes,
                             const int32_t* list, const int* list_n, int64_t threads, const DevIndex& ix,
                             const SeedParams& sp, const ChainParamsDev& cp, const CandParams& cand, CandBuf cb,
                             int32_t* n_min, int64_t* n_anchor, int32_t* n_anc_t, uint32_t* scratch,
-                            int32_t* next_list, int* next_n, int min_len, uint32_t* err);
+                            int32_t* next_list, int* next_n, int min_len, int* claim, uint32_t* err);
 // Sort keys (longest first; slots at or past *list_n last) and values (read ids) of a list
 // whose length is only known on the device; n_max = the list buffer's size.
 void launch_long_order(cudaStream_t st, const int32_t* list, const int* list_n, int n_max, const int32_t* seq_len,

@@ -44,31 +44,35 @@ namespace dnb {
 
 namespace {
 
-constexpr int kTT = 128;                  // threads (= reads) per block
 constexpr int kTMaxLen = 256;             // longest read staged
 constexpr int kTWords = kTMaxLen / 4;     // staged code words per read
-constexpr int kTPitch = kTT + 1;          // word pitch of the staging layout (spreads banks)
 constexpr int kTMaxMin = 32;              // minimizers per read
 constexpr int kTMaxAnc = 32;              // anchors per read (one bit each in a 32-bit mask)
 constexpr int kTMaxChains = 8;            // chains per read passing the score / anchor filters
 constexpr int kTW = 10;                   // window length of the compiled sketch
 constexpr int kProbe = 8;                 // minimizers probed with independent loads at once
 
-// Dynamic shared memory of a block: two regions of 32-bit words, each thread owning one
-// column of each (word w of thread T at w * pitch + T), so that after the cooperative
-// staging no thread ever touches another thread's words. Region A (pitch kTPitch): the
-// staged ASCII words, later the anchor keys (two words each). Region B (pitch kTT): the
-// minimizers {hash, pos | strand << 31} (two words each), later f << 8 | (prev + 1) of
-// each anchor (words 0..31) and the chain table (words 32..63).
+// Dynamic shared memory of a block of TT threads (= reads): two regions of 32-bit words,
+// each thread owning one column of each (word w of thread T at w * pitch + T), so that
+// after the cooperative staging no thread ever touches another thread's words. Region A
+// (pitch TT + 1, which spreads the banks): the staged ASCII words, later the anchor keys
+// (two words each). Region B (pitch TT): the minimizers {hash, pos | strand << 31} (two
+// words each), later f << 8 | (prev + 1) of each anchor (words 0..31) and the chain table
+// (words 32..63). The block size is the tuner's reads-per-block choice (64 or 128); the
+// shared memory per read, and so the reads resident per SM, barely depend on it.
 constexpr int kWordsA = kTWords + 2;  // a read of kTMaxLen bytes at any offset within its first word
 constexpr int kWordsB = 64;
 static_assert(2 * kTMaxAnc <= kWordsA, "anchor keys must fit a staging column");
 static_assert((3 + kTMaxLen + 3) / 4 <= kWordsA, "a staged read must fit its column");
 static_assert(2 * kTMaxMin <= kWordsB && kTMaxAnc + 4 * kTMaxChains <= kWordsB, "region B column too small");
-constexpr int kRegionA = kWordsA * kTPitch * 4;
-constexpr int kRegionB = kWordsB * kTT * 4;
 constexpr int kTMaxBand = 256;  // chaining band the shared gap-cost table holds
-constexpr int kThreadSmem = kRegionA + kRegionB + (kTMaxBand + 1) * 4;
+template <int TT>
+struct TLayout {
+  static constexpr int kPitch = TT + 1;
+  static constexpr int kRegionA = kWordsA * kPitch * 4;
+  static constexpr int kRegionB = kWordsB * TT * 4;
+  static constexpr int kSmem = kRegionA + kRegionB + (kTMaxBand + 1) * 4;
+};
 
 __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return b < a ? b : a; }
 
@@ -101,39 +105,40 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-template <int W>
-__global__ void __launch_bounds__(kTT)
+template <int W, int TT>
+__global__ void __launch_bounds__(TT)
     k_seed_chain_t(const char* __restrict__ seq, const int64_t* __restrict__ seq_off, int64_t seq_base,
                    const int32_t* __restrict__ seq_len, int64_t n, DevIndex ix, SeedParams sp, ChainParamsDev cp,
                    CandParams cand,
                    CandBuf cb, int32_t* __restrict__ n_min, int64_t* __restrict__ n_anchor,
                    int32_t* __restrict__ n_anc_t, int32_t* __restrict__ big_list, int* __restrict__ big_n,
                    uint32_t* __restrict__ err) {
+  using L = TLayout<TT>;
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* const stg = reinterpret_cast<uint32_t*>(smem);  // region A (all columns, for the staging)
-  int32_t* const lut = reinterpret_cast<int32_t*>(smem + kRegionA + kRegionB);  // chaining gap costs
+  int32_t* const lut = reinterpret_cast<int32_t*>(smem + L::kRegionA + L::kRegionB);  // chaining gap costs
   const int T = threadIdx.x, lane = T & 31;
-  for (int d = T; d <= cp.band; d += kTT) lut[d] = cp.cost[d];
+  for (int d = T; d <= cp.band; d += TT) lut[d] = cp.cost[d];
   __syncthreads();
   uint32_t* const ca = stg + T;                                                   // this thread's A column
-  uint32_t* const cbw = reinterpret_cast<uint32_t*>(smem + kRegionA) + T;         // this thread's B column
+  uint32_t* const cbw = reinterpret_cast<uint32_t*>(smem + L::kRegionA) + T;         // this thread's B column
   // anchor a: word 2a = strand << 31 | rpos, word 2a+1 = qpos (>= 0 here); as one 64-bit
   // key (word 2a high) it orders like (strand, rpos, qpos), the reference's anchor order
-  const auto a_hi = [&](int a) -> uint32_t& { return ca[2 * a * kTPitch]; };
-  const auto a_lo = [&](int a) -> uint32_t& { return ca[(2 * a + 1) * kTPitch]; };
+  const auto a_hi = [&](int a) -> uint32_t& { return ca[2 * a * L::kPitch]; };
+  const auto a_lo = [&](int a) -> uint32_t& { return ca[(2 * a + 1) * L::kPitch]; };
   const auto key_ld = [&](int a) { return static_cast<uint64_t>(a_hi(a)) << 32 | a_lo(a); };
   const auto key_st = [&](int a, uint64_t v) {
     a_hi(a) = static_cast<uint32_t>(v >> 32);
     a_lo(a) = static_cast<uint32_t>(v);
   };
   // DP word of anchor i: (prev + 1) | f << 8 | max(f[0..i]) << 20 (f <= k * 32 < 4096)
-  const auto fp_at = [&](int i) -> uint32_t& { return cbw[i * kTT]; };
+  const auto fp_at = [&](int i) -> uint32_t& { return cbw[i * TT]; };
   const auto f_of = [](uint32_t w) { return static_cast<int>((w >> 8) & 0xFFFu); };
   const auto ch_at = [&](int field, int c) -> int32_t& {
-    return reinterpret_cast<int32_t&>(cbw[(kTMaxAnc + field * kTMaxChains + c) * kTT]);
+    return reinterpret_cast<int32_t&>(cbw[(kTMaxAnc + field * kTMaxChains + c) * TT]);
   };
 
-  const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kTT + (T & ~31);  // first read of this warp
+  const int64_t r0 = static_cast<int64_t>(blockIdx.x) * TT + (T & ~31);  // first read of this warp
   const int64_t r = r0 + lane;
   int len = 0;
   uint64_t a_word = 0;  // this read's first ASCII byte rounded down to a 4-byte boundary
@@ -154,7 +159,7 @@ __global__ void __launch_bounds__(kTT)
     const int nwj = __shfl_sync(0xffffffffu, nwords, j);
     const int tj = (T & ~31) + j;
     for (int w = lane; w < nwj; w += 32)
-      cp_async4(stg + w * kTPitch + tj, reinterpret_cast<const void*>(aj + 4u * static_cast<uint64_t>(w)));
+      cp_async4(stg + w * L::kPitch + tj, reinterpret_cast<const void*>(aj + 4u * static_cast<uint64_t>(w)));
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(kTT)
     int run = 0;
     auto roll = [&](int i) {  // consumes code i (called with i = 0, 1, 2, ...)
       const int jb = i + offb;  // byte of the staged words
-      if ((jb & 3) == 0 || i == 0) wcur = ca[(jb >> 2) * kTPitch];
+      if ((jb & 3) == 0 || i == 0) wcur = ca[(jb >> 2) * L::kPitch];
       const uint32_t c = nt4((wcur >> (8 * (jb & 3))) & 0xFFu);
       run = c < 4 ? run + 1 : 0;
       fwd = ((fwd << 2) | (c & 3u)) & mask2k;
@@ -208,8 +213,8 @@ __global__ void __launch_bounds__(kTT)
             arg = static_cast<int>(static_cast<uint32_t>(m) >> 1);
           if (arg >= 0 && arg != prev_arg) {
             if (nmin < kTMaxMin) {
-              cbw[2 * nmin * kTT] = static_cast<uint32_t>(m >> 32);
-              cbw[(2 * nmin + 1) * kTT] = static_cast<uint32_t>(arg) | (static_cast<uint32_t>(m) & 1u) << 31;
+              cbw[2 * nmin * TT] = static_cast<uint32_t>(m >> 32);
+              cbw[(2 * nmin + 1) * TT] = static_cast<uint32_t>(arg) | (static_cast<uint32_t>(m) & 1u) << 31;
             }
             ++nmin;
           }
@@ -241,7 +246,7 @@ __global__ void __launch_bounds__(kTT)
         bk[q] = make_ulonglong2(kInvalidHash, 0);
         slot[q] = 0;
         if (j0 + q < nmin) {
-          m[q] = make_uint2(cbw[2 * (j0 + q) * kTT], cbw[(2 * (j0 + q) + 1) * kTT]);
+          m[q] = make_uint2(cbw[2 * (j0 + q) * TT], cbw[(2 * (j0 + q) + 1) * TT]);
           slot[q] = static_cast<uint64_t>(m[q].x) & ix.mask;
           bk[q] = __ldg(ix.table + slot[q]);
           pending |= 1u << q;
@@ -437,6 +442,19 @@ __global__ void __launch_bounds__(kTT)
   cb.n_cand[r] = nd;
 }
 
+template <int TT>
+bool launch_thread_tt(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+                      const int32_t* seq_len, int64_t n, const DevIndex& ix, const SeedParams& sp,
+                      const ChainParamsDev& cp, const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
+                      int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err) {
+  static std::atomic<bool> attr_set[kMaxDevices];
+  if (!set_smem_limit_once(k_seed_chain_t<kTW, TT>, TLayout<TT>::kSmem, attr_set)) return false;
+  const int64_t blocks = (n + TT - 1) / TT;
+  k_seed_chain_t<kTW, TT><<<static_cast<unsigned>(blocks), TT, TLayout<TT>::kSmem, st>>>(
+      seq, seq_off, seq_base, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list, big_n, err);
+  return true;
+}
+
 }  // namespace
 
 int seed_thread_max_len() { return kTMaxLen; }
@@ -457,15 +475,16 @@ bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* s
                               const int32_t* seq_len, int64_t n, const DevIndex& ix, const SeedParams& sp,
                               const ChainParamsDev& cp,
                               const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
-                              int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err) {
+                              int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err, int reads_per_block) {
   if (!seed_thread_supported(sp, cp)) return false;
   if (n <= 0) return true;
-  static std::atomic<bool> attr_set[kMaxDevices];
-  if (!set_smem_limit_once(k_seed_chain_t<kTW>, kThreadSmem, attr_set)) return false;
-  const int64_t blocks = (n + kTT - 1) / kTT;
-  k_seed_chain_t<kTW><<<static_cast<unsigned>(blocks), kTT, kThreadSmem, st>>>(
-      seq, seq_off, seq_base, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list, big_n, err);
-  return true;
+  if (reads_per_block == 64)
+    return launch_thread_tt<64>(st, seq, seq_off, seq_base, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t,
+                                big_list, big_n, err);
+  if (reads_per_block == 128)
+    return launch_thread_tt<128>(st, seq, seq_off, seq_base, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor,
+                                 n_anc_t, big_list, big_n, err);
+  return false;
 }
 
 }  // namespace dnb

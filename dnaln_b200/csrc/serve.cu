@@ -75,7 +75,7 @@ struct Request {
   std::vector<std::vector<uint32_t>> part_cig;   // CIGAR ops of each part, read order
   std::vector<std::pair<int64_t, int64_t>> part_span;
   int status = DNALN_OK;
-  bool done = false;
+  bool done = false, cancelled = false;
   Clock::time_point t_submit;
   double latency_ms = 0.0;
 };
@@ -370,7 +370,7 @@ void lane_main(dnaln_server* s, Lane* L) {
       for (int64_t i = pt.a; i < pt.b; ++i) bases += r->seq_len[i];
       if (st != DNALN_OK && r->status == DNALN_OK) r->status = st;
       r->parts_done += 1;
-      if (r->next >= r->n && r->parts_done == r->parts) complete(s, r);
+      if (!r->done && r->next >= r->n && r->parts_done == r->parts) complete(s, r);
     }
     s->ms_complete += std::chrono::duration<double, std::milli>(Clock::now() - c0).count();
     s->n_batches += 1;
@@ -498,6 +498,29 @@ int dnaln_serve_submit(dnaln_server* s, int32_t index_id, const char* seq, const
     s->cv_done.notify_all();
   else
     s->cv_work.notify_one();
+  return DNALN_OK;
+}
+
+int dnaln_serve_cancel(dnaln_server* s, int64_t request) {
+  if (!s) return DNALN_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(s->mu);
+  auto it = s->requests.find(request);
+  if (it == s->requests.end()) {
+    s->err = "unknown request (or already waited for)";
+    return DNALN_ERR_INVALID_ARG;
+  }
+  Request* r = it->second.get();
+  if (r->done) return DNALN_OK;  // finished before the cancel: its result stands
+  // no further part of it goes into a batch; parts already in a batch finish first (their
+  // lanes write into the caller's buffers), then the request completes as cancelled
+  r->cancelled = true;
+  r->status = DNALN_ERR_CANCELLED;
+  r->next = r->n;
+  s->waiting.erase(std::remove(s->waiting.begin(), s->waiting.end(), r), s->waiting.end());
+  if (r->parts_done == r->parts) {
+    complete(s, r);
+    s->cv_done.notify_all();
+  }
   return DNALN_OK;
 }
 

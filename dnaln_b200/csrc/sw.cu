@@ -37,6 +37,8 @@
 // (h == e) is 1,0, and otherwise H came from F — so the walk (src/align.cpp:87-143)
 // takes the reference's steps. The best cell is the first strict maximum in row-major
 // order (per-row maximum with its first column, then strict across rows).
+#include <algorithm>
+#include <cstdlib>
 #include <type_traits>
 
 #include "common.cuh"
@@ -514,9 +516,169 @@ __global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1) k_sw_u2(c
   if (has_b) res[tb.slot] = stash(static_cast<int>(best_b) - static_cast<int>(kBias), TB ? bi_b : 0, bd_b);
 }
 
-// Wide bands, W = 32 * LANES + 1: LANES consecutive lanes of a warp share one pair of
+// k_sw_u2 with fewer instructions per cell (same results, same outputs):
+//  * E and F by the DPX add-max (max(a + b, c) in one instruction, signed 16x2: the biased
+//    values lie in [0, 32767], where signed and unsigned order agree), so the open-gap
+//    candidates hup - (O+E) and hleft - (O+E) are never materialised; the extension bits
+//    come from e - hup + (O+E) and f - hleft + (O+E), one 3-input add each (both halves
+//    non-negative, so no borrow crosses them);
+//  * the substitution profile of a query code from a 5-entry table in shared memory, the
+//    next row's read one row ahead;
+//  * target codes read without range or N checks: the pair reaches this point only when
+//    both windows [0, qlen + W - 1) are N-free and inside their contigs, and reads past a
+//    window are clamped to its last base (a row past a query's end is an N row for it,
+//    whose scores do not depend on the target), so a code is always 0..3 and the prmt
+//    selector of two codes is two multiply-adds.
+template <int W, bool TB>
+__global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1)
+    k_sw_u2v(const SwTask* __restrict__ tasks, int base, int n, const int* __restrict__ n_dev,
+             const uint8_t* __restrict__ qbase, const uint8_t* __restrict__ tbase, SwParams p,
+             SwResult* __restrict__ res, uint32_t* __restrict__ dir, int rows_max, int* __restrict__ fb) {
+  static_assert(W >= 3, "a window of at least two columns past an empty query");
+  constexpr int WQ = (W + 3) / 4;
+  __shared__ uint32_t s_prof[8];
+  if (threadIdx.x < 5) s_prof[threadIdx.x] = prof_biased(p, threadIdx.x);
+  __syncthreads();
+  const int lt = blockIdx.x * blockDim.x + threadIdx.x;  // pair index within this launch
+  const int nn = n_dev ? min(n, *n_dev) : n;
+  const int ia = base + 2 * lt, ib = ia + 1;
+  if (ia >= nn) return;
+  const bool has_b = ib < nn;
+  uint32_t* DP = TB ? pair_base(dir, 2 * lt, rows_max, WQ) : nullptr;
+  const SwTask ta = tasks[ia];
+  SwTask tb = ta;
+  if (has_b) tb = tasks[ib];
+  else tb.qlen = 0;
+  const int qmax = max(ta.qlen, tb.qlen);
+  const bool fits = qmax * p.match + 2 * (p.oe + p.ge + p.mismatch + p.ambig) < 16000 &&
+                    p.match + kScoreBias <= 127 && p.mismatch <= kScoreBias && p.ambig <= kScoreBias;
+  if (!fits || window_has_n(ta, W, tbase) || (has_b && window_has_n(tb, W, tbase))) {
+    const int k = atomicAdd(fb, has_b ? 2 : 1);
+    fb[1 + k] = 2 * lt;
+    if (has_b) fb[2 + k] = 2 * lt + 1;
+    return;
+  }
+  const uint8_t* __restrict__ qa = qbase + ta.q_off;
+  const uint8_t* __restrict__ qb = qbase + tb.q_off;
+  const int qla = ta.qlen, qlb = tb.qlen;
+  // both windows are N-free over [0, qlen + W - 1): column j of each reads its window at
+  // min(j, qlen + W - 2), a code in 0..3
+  const uint8_t* __restrict__ wa = tbase + ta.t_start;
+  const uint8_t* __restrict__ wb = tbase + tb.t_start;
+  const int ja = qla + W - 2, jb = qlb + W - 2;
+  auto tc2 = [&](int j) {
+    const uint32_t a = __ldg(wa + min(j, ja)), b = __ldg(wb + min(j, jb));
+    return a * 17u + b * 4352u + 50304u;  // sel2(a, b)
+  };
+  auto qcode = [&](const uint8_t* __restrict__ q, int ql, int i) {
+    return i < ql ? min(static_cast<uint32_t>(q[i]), 4u) : 4u;
+  };
+  uint32_t H[W + 1], E[W + 1], T[W];
+#pragma unroll
+  for (int d = 0; d <= W; ++d) {
+    H[d] = kBias2;
+    E[d] = kBias2;
+  }
+#pragma unroll
+  for (int d = 0; d < W; ++d) T[d] = tc2(d);
+  const uint32_t OE = pack2(p.oe), GE = pack2(p.ge), SB = pack2(kScoreBias);
+  const uint32_t NOE = pack2(static_cast<uint32_t>(-p.oe));  // -(O+E) in each signed half
+  uint32_t best2 = kBias2;
+  uint32_t best_a = kBias, best_b = kBias;
+  int bi_a = -1, bi_b = -1;
+  extern __shared__ uint32_t sw_rows[];
+  uint32_t* const row_a = sw_rows + threadIdx.x;
+  uint32_t* const row_b = sw_rows + W * kSwThreads + threadIdx.x;
+  int buf_a = 0, buf_b = 1;
+  uint32_t plo = s_prof[qcode(qa, qla, 0)], phi = s_prof[qcode(qb, qlb, 0)];
+  uint32_t ca = qcode(qa, qla, 1), cb = qcode(qb, qlb, 1);  // codes of the next row
+  uint32_t* rowp = DP;
+  for (int i = 0; i < qmax; ++i) {
+    // the next row's codes and profile words and the target column entering the band are
+    // loaded up front, so their latency hides behind this row
+    const uint32_t t_next = tc2(i + W);
+    const uint32_t plo_next = s_prof[ca], phi_next = s_prof[cb];
+    const uint32_t ca_next = qcode(qa, qla, i + 2), cb_next = qcode(qb, qlb, i + 2);
+    uint32_t f = kBias2, hleft = kBias2, hdiag = H[0], rmax = 0, dw = 0;
+#pragma unroll
+    for (int d = 0; d < W; ++d) {
+      const uint32_t hup = H[d + 1], eup = E[d + 1];
+      const uint32_t hd = hdiag + prmt(plo, phi, T[d]) - SB;
+      const uint32_t e = __viaddmax_s16x2(hup, NOE, eup - GE);
+      const uint32_t fn = __viaddmax_s16x2(hleft, NOE, f - GE);
+      const uint32_t m1 = __vmaxu2(hd, e);
+      const uint32_t h = __vimax3_u16x2(m1, fn, kBias2);
+      if constexpr (TB) {
+        // each term is >= 0 per half; saturated to 0/1 it is one code bit
+        const uint32_t b3 = __vminu2(m1 - hd, kOne2), b2 = __vminu2(h - m1, kOne2);
+        const uint32_t b1 = __vminu2(e - hup + OE, kOne2), b0 = __vminu2(fn - hleft + OE, kOne2);
+        dw = dw * 16u + ((b3 * 2u + b2) * 4u + (b1 * 2u + b0));
+        if ((d & 3) == 3 || d == W - 1) {
+          if ((d & 3) != 3) dw <<= 4 * (3 - (d & 3));
+          rowp[(d >> 2) * 32] = dw;
+          dw = 0;
+        }
+        rmax = d == 0 ? h : __vmaxu2(rmax, h);
+      } else {
+        best2 = __vmaxu2(best2, h);
+      }
+      H[d] = h;
+      E[d] = e;
+      f = fn;
+      hleft = h;
+      hdiag = hup;
+    }
+    if constexpr (TB) {  // a strictly better row (rows in order: the first strict maximum)
+      const bool up_a = (rmax & 0xFFFFu) > best_a, up_b = (rmax >> 16) > best_b;
+      if (up_a || up_b) {
+        const int dst = row_buffer(up_a, up_b, buf_a, buf_b);
+        uint32_t* const row = dst ? row_b : row_a;
+#pragma unroll
+        for (int d = 0; d < W; ++d) row[d * kSwThreads] = H[d];
+        if (up_a) {
+          best_a = rmax & 0xFFFFu;
+          bi_a = i;
+          buf_a = dst;
+        }
+        if (up_b) {
+          best_b = rmax >> 16;
+          bi_b = i;
+          buf_b = dst;
+        }
+      }
+      rowp += WQ * 32;
+    }
+#pragma unroll
+    for (int d = 0; d + 1 < W; ++d) T[d] = T[d + 1];
+    T[W - 1] = t_next;
+    plo = plo_next;
+    phi = phi_next;
+    ca = ca_next;
+    cb = cb_next;
+  }
+  int bd_a = 0, bd_b = 0;
+  if constexpr (!TB) {
+    best_a = best2 & 0xFFFFu;
+    best_b = best2 >> 16;
+  } else {  // first column of the best row holding the best value, per half
+    bd_a = bi_a >= 0 ? W : -1;
+    bd_b = bi_b >= 0 ? W : -1;
+    const uint32_t* const ra = buf_a ? row_b : row_a;
+    const uint32_t* const rb = buf_b ? row_b : row_a;
+#pragma unroll 1
+    for (int d = W - 1; d >= 0; --d) {
+      if (bi_a >= 0 && (ra[d * kSwThreads] & 0xFFFFu) == best_a) bd_a = d;
+      if (bi_b >= 0 && (rb[d * kSwThreads] >> 16) == best_b) bd_b = d;
+    }
+  }
+  res[ta.slot] = stash(static_cast<int>(best_a) - static_cast<int>(kBias), TB ? bi_a : 0, bd_a);
+  if (has_b) res[tb.slot] = stash(static_cast<int>(best_b) - static_cast<int>(kBias), TB ? bi_b : 0, bd_b);
+}
+
+// Wide bands, W = CH * LANES + 1: LANES consecutive lanes of a warp share one pair of
 // alignments (A and B in the 16-bit halves, as in k_sw_u2), lane c holding band cells
-// [32c, 32c + 32) of the row in registers (the last lane also cell W - 1). Lane c works on
+// [CH c, CH c + CH) of the row in registers (the last lane also cell W - 1); CH = 32, or 16
+// for twice the lanes per pair (fewer registers, more pairs in flight, a longer skew). Lane c works on
 // row t - c at step t, so its left neighbour finished the same row one step earlier: the
 // row's running F and H(left) arrive by one shuffle at the start of the step. The one value
 // a lane needs from its right neighbour — H and E of the previous row at the neighbour's
@@ -527,12 +689,13 @@ __global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1) k_sw_u2(c
 // lanes of a pair combine (value, then earliest row, then smallest column) at the end:
 // the first strict maximum of the whole band in row-major order. Pairs k_sw_u2 would
 // hand to the int32 kernel are listed in fb the same way.
-template <int LANES, bool TB>
-__global__ void __launch_bounds__(kSwThreads, TB ? 3 : 1)
+template <int LANES, int CH, bool TB>
+__global__ void __launch_bounds__(kSwThreads, TB ? (CH == 16 ? 4 : 3) : 1)
     k_sw_wide(const SwTask* __restrict__ tasks, int base, int n, const int* __restrict__ n_dev,
               const uint8_t* __restrict__ qbase, const uint8_t* __restrict__ tbase, SwParams p,
               SwResult* __restrict__ res, uint32_t* __restrict__ dir, int rows_max, int* __restrict__ fb) {
-  constexpr int W = 32 * LANES + 1, WQ = (W + 3) / 4, CH = 32;
+  static_assert(CH % 4 == 0 && CH >= 8, "a lane's cells fill whole direction words");
+  constexpr int W = CH * LANES + 1, WQ = (W + 3) / 4;
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int c = lane % LANES;  // chunk of this lane
@@ -743,11 +906,12 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_fb(const SwTask* __restrict__
                                                       SwResult* __restrict__ res, uint32_t* __restrict__ dir,
                                                       int rows_max, const int* __restrict__ fb) {
   constexpr int WQ = (W + 3) / 4;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= fb[0]) return;
-  const int lt = fb[1 + j];
-  const SwTask tk = tasks[base + lt];
-  res[tk.slot] = sw_one_reg<W, TB>(tk, qbase, tbase, p, TB ? pair_base(dir, lt, rows_max, WQ) : nullptr, lt & 1);
+  const int nfb = fb[0];
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nfb; j += gridDim.x * blockDim.x) {
+    const int lt = fb[1 + j];
+    const SwTask tk = tasks[base + lt];
+    res[tk.slot] = sw_one_reg<W, TB>(tk, qbase, tbase, p, TB ? pair_base(dir, lt, rows_max, WQ) : nullptr, lt & 1);
+  }
 }
 
 // The tasks k_sw_u2 / k_sw_wide listed (an N in the target window, or outside the biased
@@ -768,9 +932,12 @@ __global__ void __launch_bounds__(kSwThreads)
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int c = lane % LANES;
-  const int j = (blockIdx.x * blockDim.x + threadIdx.x) / LANES;  // entry of the fallback list
   const int nfb = fb[0];
-  if ((blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / LANES >= nfb) return;  // warp-uniform
+  const int stride = static_cast<int>(gridDim.x * blockDim.x / LANES);
+  // a warp takes 32 / LANES consecutive entries of the fallback list per round (jw, the
+  // first, is warp-uniform, so every lane takes the same rounds)
+  for (int jw = static_cast<int>((blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / LANES); jw < nfb; jw += stride) {
+  const int j = jw + lane / LANES;  // entry of the fallback list
   const bool live = j < nfb;
   const int lt = live ? fb[1 + j] : 0;
   SwTask tk{};
@@ -885,11 +1052,13 @@ __global__ void __launch_bounds__(kSwThreads)
     const uint64_t x = __shfl_xor_sync(FULL, key, o);
     key = x > key ? x : key;
   }
-  if (c != 0 || !live) return;
-  const int kb = static_cast<int>(key >> 40);
-  const int kbi = static_cast<int>(0xFFFFFu - static_cast<uint32_t>((key >> 12) & 0xFFFFFu)) - 1;
-  const int kbd = static_cast<int>(0xFFFu - static_cast<uint32_t>(key & 0xFFFu));
-  res[tk.slot] = TB ? stash(kb, kbi, kbd) : stash(kb, 0, 0);
+  if (c == 0 && live) {
+    const int kb = static_cast<int>(key >> 40);
+    const int kbi = static_cast<int>(0xFFFFFu - static_cast<uint32_t>((key >> 12) & 0xFFFFFu)) - 1;
+    const int kbd = static_cast<int>(0xFFFu - static_cast<uint32_t>(key & 0xFFFu));
+    res[tk.slot] = TB ? stash(kb, kbi, kbd) : stash(kb, 0, 0);
+  }
+  }
 }
 
 // Traceback of every task of the launch from the stashed best cell (one task per thread;
@@ -988,6 +1157,15 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_any(const SwTask* __restrict_
   res[tk.slot] = r;
 }
 
+// EXPERIMENT (to be removed): which k_sw_u2 form runs, from DNALN_SW_VARIANT (default 1).
+inline int sw_variant() {
+  static const int v = [] {
+    const char* e = std::getenv("DNALN_SW_VARIANT");
+    return e ? std::atoi(e) : 1;
+  }();
+  return v;
+}
+
 template <int W>
 void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int count, int n, const int* n_dev,
                const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res, uint32_t* dir,
@@ -998,7 +1176,12 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
   // W = 65: the fallback list runs two lanes per alignment (k_sw_fb_lanes<2>); narrower
   // bands keep the one-thread kernel, whose band fits in registers
   constexpr bool kLanesFb = W == 65;
-  const int blocks_fb = static_cast<int>((static_cast<int64_t>(count) * 2 + kSwThreads - 1) / kSwThreads);
+  // the fallback kernels stride over a list whose length only the device knows (usually
+  // short or empty): a few resident waves, not one block per possible entry
+  const int fb_cap = 8 * device_sm_count();
+  const int blocks_fb =
+      std::min(fb_cap, static_cast<int>((static_cast<int64_t>(count) * 2 + kSwThreads - 1) / kSwThreads));
+  const int blocks_fb1 = std::min(fb_cap, blocks_tasks);
   const KernelTrace none;
   const KernelTrace& t = kt ? *kt : none;
   cudaMemsetAsync(fb, 0, sizeof(int), st);
@@ -1009,14 +1192,23 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
       set_smem_limit_once(k_sw_u2<W, true>, kRowBytes, attr_set);
     }
     t.begin(st, "k_sw_u2<tb>");
-    k_sw_u2<W, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
-                                                                  rows_max, fb);
+    if (sw_variant()) {
+      if (kRowBytes > 48 * 1024) {
+        static std::atomic<bool> attr_set2[kMaxDevices];
+        set_smem_limit_once(k_sw_u2v<W, true>, kRowBytes, attr_set2);
+      }
+      k_sw_u2v<W, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
+                                                                     rows_max, fb);
+    } else {
+      k_sw_u2<W, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
+                                                                    rows_max, fb);
+    }
     t.end(st);
     t.begin(st, "k_sw_fb<tb>");
     if constexpr (kLanesFb)
       k_sw_fb_lanes<2, true><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     else
-      k_sw_fb<W, true><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+      k_sw_fb<W, true><<<blocks_fb1, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_walk");
     k_sw_walk<W><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, count, n, n_dev, qbase, tbase, p, res, dir,
@@ -1024,39 +1216,46 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
     t.end(st);
   } else {
     t.begin(st, "k_sw_u2<score>");
-    k_sw_u2<W, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max,
-                                                           fb);
+    if (sw_variant())
+      k_sw_u2v<W, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
+                                                              rows_max, fb);
+    else
+      k_sw_u2<W, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
+                                                             rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<score>");
     if constexpr (kLanesFb)
       k_sw_fb_lanes<2, false><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     else
-      k_sw_fb<W, false><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+      k_sw_fb<W, false><<<blocks_fb1, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     t.end(st);
   }
 }
 
-template <int LANES>
+template <int LANES, int CH = 32>
 void launch_wide(cudaStream_t st, bool tb, const SwTask* tasks, int base, int count, int n, const int* n_dev,
                  const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res, uint32_t* dir,
                  int rows_max, uint32_t* cig, const int64_t* cig_off, int* fb, uint32_t* err, const KernelTrace* kt) {
-  constexpr int W = 32 * LANES + 1;
+  constexpr int W = CH * LANES + 1;
+  constexpr int FBL = (W - 1) / 32;  // lanes per alignment of the int32 fallback kernel
   const int pairs = (count + 1) / 2;
   const int blocks_pairs = static_cast<int>((static_cast<int64_t>(pairs) * LANES + kSwThreads - 1) / kSwThreads);
   const int blocks_tasks = (count + kSwThreads - 1) / kSwThreads;
-  // the fallback list holds at most `count` tasks (its length is known on the device only)
-  const int blocks_fb = static_cast<int>((static_cast<int64_t>(count) * LANES + kSwThreads - 1) / kSwThreads);
+  // the fallback list holds at most `count` tasks (its length is known on the device only;
+  // the kernel strides over it, so a few resident waves suffice)
+  const int blocks_fb = std::min(8 * device_sm_count(),
+                                 static_cast<int>((static_cast<int64_t>(count) * FBL + kSwThreads - 1) / kSwThreads));
   const KernelTrace none;
   const KernelTrace& t = kt ? *kt : none;
   cudaMemsetAsync(fb, 0, sizeof(int), st);
   if (tb) {
-    constexpr int kRowBytes = 2 * 33 * kSwThreads * 4;  // the two saved best rows of each lane
+    constexpr int kRowBytes = 2 * (CH + 1) * kSwThreads * 4;  // the two saved best rows of each lane
     t.begin(st, "k_sw_wide<tb>");
-    k_sw_wide<LANES, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res,
-                                                                        dir, rows_max, fb);
+    k_sw_wide<LANES, CH, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p,
+                                                                            res, dir, rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<tb>");
-    k_sw_fb_lanes<LANES, true><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    k_sw_fb_lanes<FBL, true><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_walk");
     k_sw_walk<W><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, count, n, n_dev, qbase, tbase, p, res, dir,
@@ -1064,12 +1263,12 @@ void launch_wide(cudaStream_t st, bool tb, const SwTask* tasks, int base, int co
     t.end(st);
   } else {
     t.begin(st, "k_sw_wide<score>");
-    k_sw_wide<LANES, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
-                                                                 rows_max, fb);
+    k_sw_wide<LANES, CH, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
+                                                                     rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<score>");
-    k_sw_fb_lanes<LANES, false><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max,
-                                                                  fb);
+    k_sw_fb_lanes<FBL, false><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max,
+                                                                fb);
     t.end(st);
   }
 }
@@ -1108,7 +1307,21 @@ size_t sw_band_bytes_per_task(int W, bool bytes_ok) {
 
 int sw_launches(int W, bool bytes_ok, bool tb) { return sw_uses_generic(W, bytes_ok) ? 1 : (tb ? 3 : 2); }
 
-bool sw_has_both_forms(int W, bool bytes_ok) { return !sw_uses_generic(W, bytes_ok) && (W == 33 || W == 65); }
+bool sw_has_form(int W, bool bytes_ok, SwForm form) {
+  if (sw_uses_generic(W, bytes_ok)) return form == kSwInter;
+  switch (form) {
+    case kSwInter: return W != 129;
+    case kSwIntra: return W == 33 || W == 65 || W == 129;
+    case kSwIntraNarrow: return W == 33 || W == 65 || W == 129;
+    default: return false;
+  }
+}
+
+int sw_lanes_per_pair(int W, SwForm form) {
+  if (form == kSwIntra) return (W - 1) / 32;
+  if (form == kSwIntraNarrow) return (W - 1) / 16;
+  return 1;
+}
 
 bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int base, int count, int n,
                const int* n_dev, const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res,
@@ -1117,13 +1330,21 @@ bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int
   if (count <= 0) return true;
   const bool generic = sw_uses_generic(p.W, bytes_ok);
   if ((tb && !dir) || (generic && !band) || (!generic && !fb) || (base % kSwTaskGroup) != 0) return false;
-  if (!generic && form == kSwIntra && sw_has_both_forms(p.W, bytes_ok)) {
-    if (p.W == 33)
-      launch_wide<1>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, fb, err,
-                     kt);
-    else
-      launch_wide<2>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, fb, err,
-                     kt);
+  if (!generic && form != kSwInter && sw_has_form(p.W, bytes_ok, form)) {
+#define DNB_SW_WIDE(L, CHV) \
+  launch_wide<L, CHV>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, fb, err, kt)
+    const bool narrow = form == kSwIntraNarrow;
+    if (p.W == 33) {
+      if (narrow) DNB_SW_WIDE(2, 16);
+      else DNB_SW_WIDE(1, 32);
+    } else if (p.W == 65) {
+      if (narrow) DNB_SW_WIDE(4, 16);
+      else DNB_SW_WIDE(2, 32);
+    } else {
+      if (narrow) DNB_SW_WIDE(8, 16);
+      else DNB_SW_WIDE(4, 32);
+    }
+#undef DNB_SW_WIDE
     return true;
   }
   if (!generic) {
@@ -1138,9 +1359,9 @@ bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int
       DNB_SW_U2(33)
       DNB_SW_U2(43)
       DNB_SW_U2(65)
-      case 129:
-        launch_wide<4>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, fb,
-                       err, kt);
+      case 129:  // no inter-sequence form at this width
+        launch_wide<4, 32>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, fb,
+                           err, kt);
         return true;
       default: break;
     }

@@ -24,12 +24,15 @@ size_t sw_band_bytes_per_task(int W, bool bytes_ok);
 // Kernels one launch_sw call issues (for launch accounting).
 int sw_launches(int W, bool bytes_ok, bool tb);
 
-// Two kernel forms compute the same register-resident bands: inter-sequence (k_sw_u2, a
-// thread holds the whole band row of two alignments) and intra-sequence (k_sw_wide, the
-// row of a pair spread over (W - 1) / 32 lanes in a skewed wavefront). W = 33 and 65 have
-// both; W = 129 only the intra form; the others only the inter form.
-enum SwForm : int { kSwInter = 0, kSwIntra = 1 };
-bool sw_has_both_forms(int W, bool bytes_ok);
+// Kernel forms of the register-resident bands, all with the same results: inter-sequence
+// (k_sw_u2, a thread holds the whole band row of two alignments; W != 129) and intra-
+// sequence (k_sw_wide, the row of a pair spread over lanes in a skewed wavefront: (W - 1) /
+// 32 lanes of 32 cells, or, narrow, (W - 1) / 16 lanes of 16 cells; W = 33, 65, 129). The
+// generic kernel (other widths or scores) has the inter form only.
+enum SwForm : int { kSwInter = 0, kSwIntra = 1, kSwIntraNarrow = 2 };
+constexpr int kSwForms = 3;
+bool sw_has_form(int W, bool bytes_ok, SwForm form);
+int sw_lanes_per_pair(int W, SwForm form);
 
 // Aligns tasks[base, base + count) that are below the task count min(n, *n_dev) (n_dev
 // may be null; it lets a device-side producer size the batch without a host sync).

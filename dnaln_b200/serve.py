@@ -70,6 +70,11 @@ class Server:
         r.id = rid.value
         return r
 
+    def cancel(self, r: Request) -> None:
+        """dnaln_serve_cancel: the request's wait then raises DnalnError(ERR_CANCELLED),
+        unless it had already completed."""
+        self._check(self._lib.dnaln_serve_cancel(self._h, r.id))
+
     def wait(self, r: Request) -> MapResult:
         lat = C.c_double()
         self._check(self._lib.dnaln_serve_wait(self._h, r.id, C.byref(lat)))

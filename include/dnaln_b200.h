@@ -33,6 +33,7 @@ extern "C" {
 #define DNALN_ERR_DEVICE 6       /* a kernel reported an internal inconsistency (error flag) */
 #define DNALN_ERR_NOT_FOUND 7    /* unknown index id */
 #define DNALN_ERR_IO 8           /* an index image file could not be written, read or verified */
+#define DNALN_ERR_CANCELLED 9    /* a served request was cancelled (dnaln_serve_cancel) */
 
 typedef struct dnaln_ctx dnaln_ctx;
 
@@ -96,6 +97,7 @@ typedef struct {
   uint64_t warp_reads, warp_minimizers, warp_anchors, warp_bases;
   uint64_t long_reads; /* reads seeded and chained by the long-read thread kernel */
   uint64_t graph_launches; /* batches launched as a captured CUDA graph (running total) */
+  uint64_t batch_retries;  /* batches mapped again after the chaining pool grew */
 } dnaln_stats;
 
 /* ---- context ---------------------------------------------------------------------- */
@@ -134,29 +136,61 @@ int dnaln_gpu_set_sub_batch(dnaln_ctx* ctx, int64_t reads);
  *   "graphs"         1 = a batch whose size the host knows (the host-buffer calls) and
  *                    whose launches repeat is captured once as a CUDA graph and replayed
  *                    (default); 0 = launched kernel by kernel;
- *   "sw_form"        banded SW kernel form where a band width has two (W = 33, 65): 0 =
- *                    tuned per context (default), 1 = inter-sequence, 2 = intra-sequence;
+ *   "sw_form"        banded SW kernel form where a band width has several (W = 33, 65,
+ *                    129): 0 = tuned per context (default), 1 = inter-sequence, 2 = intra-
+ *                    sequence, 3 = intra-sequence narrow (a form the width lacks falls back
+ *                    to the width's first form);
  *   "long_thread"    1 = reads the short thread kernel lists go one thread each through
  *                    the long-read kernel first (default); 0 = straight to the warp kernels;
  *   "length_order"   1 = SW tasks of a batch whose reads differ in length run longest
  *                    first (default); 0 = in read order;
+ *   "seed_block"     reads per block of the thread-per-read seeding kernel: 0 = tuned
+ *                    (default, dnaln_gpu_seed_tuning), 64 or 128;
+ *   "work_stealing"  1 = the kernels of listed reads (long reads one thread each, the
+ *                    rest one warp each) run on the resident blocks only, each warp taking
+ *                    its next work by an atomic claim (default); 0 = fixed grids;
  *   "dir_cap_bytes"  traceback direction-code scratch per launch (default 1/32 of the
  *                    device's memory, at least 1 GiB and at most 8 GiB; a launch whose
- *                    tasks need more is split into chunks). */
+ *                    tasks need more is split into chunks);
+ *   "chain_pool"     entries of the chaining pool that reads seeded one warp each take
+ *                    their anchor scratch from (default 65,536, grown from the batches'
+ *                    use): a batch that outgrows the pool is mapped again after the pool
+ *                    grows to what it asked for (counted in dnaln_stats.batch_retries);
+ * Fault injection on the host (tests of the error paths; changes no result):
+ *   "fail_alloc_after" N >= 0: the device allocation after N more succeed fails as if the
+ *                    device were out of memory (DNALN_ERR_OOM; the context stays usable,
+ *                    and the next call allocates again); -1 = off (default). */
 int dnaln_gpu_set_option(dnaln_ctx* ctx, const char* name, int64_t value);
-/* The SW kernel-form tuner (no reference counterpart): band widths with two register-
- * resident kernel forms (W = 33, 65) — inter-sequence, a thread holding the band rows of
- * two alignments, and intra-sequence, a pair's row spread over (W - 1) / 32 lanes — are
- * timed against each other on the first batch of each (band width, traceback or score-
- * only, read-length bucket <= 256 / <= 1024 / longer) a context maps, and the faster form
- * runs from then on (`tasks` says how large the timed sample was). Both give identical
- * results. Writes min(cap, count) entries; *n_out = count. */
+/* The SW kernel-form tuner (no reference counterpart; the reference picks its SIMD lane
+ * grouping per task group, src/align_simd.cpp:50-70): band widths with more than one
+ * register-resident kernel form — inter-sequence (a thread holds the band rows of two
+ * alignments; W = 33, 65 and the other register widths) and intra-sequence (a pair's row
+ * spread over lanes in a skewed wavefront: (W - 1) / 32 lanes of 32 cells, or narrow,
+ * (W - 1) / 16 lanes of 16 cells; W = 33, 65, 129) — have every form timed on the first
+ * batch of each (band width, traceback or score-only, read-length bucket <= 256 / <= 1024
+ * / longer) a context maps, and the fastest runs from then on (`tasks` says how large the
+ * timed sample was). All forms give identical results. ms_* = -1 for a form the width
+ * lacks. Writes min(cap, count) entries; *n_out = count. */
 typedef struct {
-  int32_t W, traceback, len_bucket, form; /* form: 0 inter-sequence, 1 intra-sequence */
+  int32_t W, traceback, len_bucket, form; /* form: 0 inter-sequence, 1 intra-sequence, 2 intra narrow */
   double ms_inter, ms_intra;              /* the timed first chunk */
   int64_t tasks;
+  double ms_narrow;
+  int32_t lanes_per_pair;                 /* lanes of the chosen form per pair of alignments */
+  int32_t pad_;
 } dnaln_sw_tuning;
 int dnaln_gpu_sw_tuning(const dnaln_ctx* ctx, dnaln_sw_tuning* out, int32_t cap, int32_t* n_out);
+/* The reads-per-block tuner of the thread-per-read seeding kernel (no reference
+ * counterpart): on the first batch of at least 32,768 reads a context maps (option
+ * "seed_block" 0, the default), the kernel runs with 64 and with 128 reads per block, each
+ * timed, and the faster size is used from then on. Both give identical results. */
+typedef struct {
+  int32_t tuned;            /* 0 until a batch was timed */
+  int32_t reads_per_block;  /* the size chosen */
+  double ms_64, ms_128;     /* the timed runs */
+  int64_t reads;            /* the timed batch's reads */
+} dnaln_seed_tuning;
+int dnaln_gpu_seed_tuning(const dnaln_ctx* ctx, dnaln_seed_tuning* out);
 /* Page-locked host buffers for fast transfers (pass to the *_batch calls). */
 int dnaln_gpu_host_alloc(dnaln_ctx* ctx, size_t bytes, void** out);
 int dnaln_gpu_host_free(dnaln_ctx* ctx, void* p);
@@ -261,6 +295,14 @@ int dnaln_gpu_align_noalloc(const uint8_t* d_q, const int64_t* d_q_off, const in
                             int32_t traceback, const dnaln_score_params* sp, dnaln_align_result* d_out,
                             uint32_t* d_cigar, int64_t cigar_stride, void* stream);
 
+/* Measured issue rate of the integer instructions the banded SW recurrence is made of (no
+ * reference counterpart: the denominator of the SW kernels' integer roofline). Runs, on
+ * every SM of `device`, independent chains of 32-bit adds and 16x2 DPX three-way maxima:
+ * mode 0 one to one (the recurrence's mix), 1 adds only, 2 maxima only; the best of five
+ * timed launches on `stream` (a cudaStream_t, NULL = default stream). *thread_ops_per_s =
+ * thread instructions of the mode per second; *best_ms (may be NULL) = that launch's time. */
+int dnaln_gpu_int_peak(int32_t device, int32_t mode, void* stream, double* thread_ops_per_s, double* best_ms);
+
 /* ---- whole batch: Mapper::map (src/mapper.cpp:75-223) --------------------------------
  * n reads, ASCII, read r = seq[seq_off[r] .. + seq_len[r]); name_hash[r] = FNV-1a of the
  * read name (src/common.hpp:136-140, dnaln_fnv1a below), the tie-break between equal
@@ -334,6 +376,12 @@ int dnaln_serve_submit(dnaln_server* s, int32_t index_id, const char* seq, const
 /* Blocks until the request is complete; returns its status, *latency_ms (may be NULL) =
  * submit-to-completion time. Each request is waited for once. */
 int dnaln_serve_wait(dnaln_server* s, int64_t request, double* latency_ms);
+/* Cancels a request not yet waited for: none of its reads not yet in a batch is mapped, and
+ * once the parts already in a batch have finished, dnaln_serve_wait returns
+ * DNALN_ERR_CANCELLED for it (its records are then partial and its CIGAR count 0). Its
+ * buffers stay the library's until that wait returns. A request already complete keeps its
+ * result (the call returns DNALN_OK and changes nothing). Other requests are not affected. */
+int dnaln_serve_cancel(dnaln_server* s, int64_t request);
 int dnaln_serve_get_stats(dnaln_server* s, dnaln_serve_stats* out);
 int dnaln_serve_reset_stats(dnaln_server* s);
 const char* dnaln_serve_last_error(const dnaln_server* s);

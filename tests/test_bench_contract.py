@@ -45,3 +45,17 @@ def test_reference_arm_other_ranks_do_no_work():
     r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_reference_arm_loads_no_mapping_code():
+    # the reference arm's inputs come from the generator library alone: the process never
+    # maps libdnaln_b200.so, so what it times is the reference's code only
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--n-reads', '5000', '--steps', '1', "
+            "'--warmup', '0']; runpy.run_path('bench.py', run_name='__main__'); "
+            "m = open('/proc/self/maps').read(); "
+            "print('MAPS', 'libdnaln_b200.so' in m, 'libdnaln_synth.so' in m, 'libdnaln_ref.so' in m)")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("MAPS")][0]
+    product, generator, reference = line.split()[1:]
+    assert product == "False" and generator == "True"

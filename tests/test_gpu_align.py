@@ -137,20 +137,28 @@ def test_traceback_consistency(ctx):
             assert int(cig[0]) & 0xF == 0 and int(cig[-1]) & 0xF == 0
 
 
-@pytest.mark.parametrize("bw", [16, 32])
+@pytest.mark.parametrize("bw", [16, 32, 64])
 def test_sw_forms_identical_and_tuned(ctx, port, bw):
-    # W = 33 and 65 have an inter-sequence and an intra-sequence kernel; both must give the
-    # oracle's results, and the tuner (sw_form 0) times them on the first batch
+    # W = 33 and 65 have an inter-sequence kernel and two intra-sequence ones (32 or 16
+    # cells per lane), W = 129 the two intra-sequence ones; every form must give the
+    # oracle's results, and the tuner (sw_form 0) times them all on the first batch
     rng = np.random.default_rng(100 + bw)
-    qs, ts = random_tasks(rng, 9000, bw, max_len=300)
+    qs, ts = random_tasks(rng, 9000 if bw < 64 else 3000, bw, max_len=300)
     sc = (2, 4, 4, 2, 1, bw)
+    W = 2 * bw + 1
     try:
         for tb in (False, True):
             exp = port.align(qs, ts, tb, sc)
-            for form in (1, 2, 0):
+            for form in (1, 2, 3, 0):
                 ctx.set_option("sw_form", form)
                 check_same(ctx.align(qs, ts, tb, D.ScoreParams(*sc)), exp, tb)
     finally:
         ctx.set_option("sw_form", 0)
-    tuned = [t for t in ctx.sw_tuning() if t["W"] == 2 * bw + 1]
-    assert tuned and all(t["form"] in (0, 1) and t["ms_inter"] > 0 and t["ms_intra"] > 0 for t in tuned)
+    tuned = [t for t in ctx.sw_tuning() if t["W"] == W]
+    assert tuned
+    for t in tuned:
+        assert t["ms_intra"] > 0 and t["ms_narrow"] > 0
+        assert (t["ms_inter"] > 0) == (W != 129)
+        timed = {f: ms for f, ms in enumerate((t["ms_inter"], t["ms_intra"], t["ms_narrow"])) if ms > 0}
+        assert t["form"] == min(timed, key=timed.get)  # the fastest form was chosen
+        assert t["lanes_per_pair"] == {0: 1, 1: (W - 1) // 32, 2: (W - 1) // 16}[t["form"]]

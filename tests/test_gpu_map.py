@@ -96,7 +96,7 @@ def test_sw_forms_give_the_same_records(ctx, repeat, bw):
     iid = ctx.index_build(g)
     try:
         got = []
-        for form in (1, 2, 0):
+        for form in (1, 2, 3, 0):
             ctx.set_option("sw_form", form)
             got.append(ctx.map_batch(iid, reads, p))
     finally:
@@ -304,3 +304,45 @@ def test_repeat_120mbp_workload_against_reference(ctx, ref):
         assert multi > 10_000
     finally:
         ctx.index_free(iid)
+
+
+def test_seed_block_tuner_and_pinned_sizes_agree(ctx):
+    # the reads-per-block tuner times 64 and 128 reads per block on the first large batch;
+    # every size gives the same records
+    g, reads, _ = synth.workload("small-1Mbp-10k-150bp", seed=9, n_reads=40_000)
+    p = D.default_map_params()
+    got = []
+    for size in (0, 64, 128):
+        with D.Context(ctx.device) as c2:
+            c2.set_option("seed_block", size)
+            j = c2.index_build(g)
+            got.append(c2.map_batch(j, reads, p))
+            t = c2.seed_tuning()
+            if size == 0:
+                assert t["tuned"] == 1 and t["reads_per_block"] in (64, 128) and t["reads"] == len(reads)
+                assert t["ms_64"] > 0 and t["ms_128"] > 0
+                assert t["reads_per_block"] == (64 if t["ms_64"] < t["ms_128"] else 128)
+            else:
+                assert t["tuned"] == 0
+    for other in got[1:]:
+        assert np.array_equal(gpu_records(got[0]), gpu_records(other))
+        assert np.array_equal(got[0].cigar, other.cigar)
+
+
+@pytest.mark.parametrize("wl", ["repeat", "mixed"])
+def test_work_stealing_and_fixed_grids_agree(ctx, request, wl):
+    # the listed-read kernels (long reads one thread each, the rest one warp each) either
+    # take work by atomic claims on resident blocks or stride over fixed grids: same records
+    g, reads, _ = request.getfixturevalue(wl)
+    p = D.default_map_params()
+    iid = ctx.index_build(g)
+    try:
+        ctx.set_option("work_stealing", 1)
+        a = ctx.map_batch(iid, reads, p)
+        ctx.set_option("work_stealing", 0)
+        b = ctx.map_batch(iid, reads, p)
+    finally:
+        ctx.set_option("work_stealing", 1)
+        ctx.index_free(iid)
+    assert np.array_equal(gpu_records(a), gpu_records(b))
+    assert np.array_equal(a.cigar, b.cigar)
