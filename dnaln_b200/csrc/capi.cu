@@ -163,7 +163,9 @@ struct dnaln_ctx {
   bool warp_seed_only = false;  // option: every read through the warp-per-read seeding kernels
   bool length_order = true;     // option: SW tasks of mixed-length batches run longest first
   bool long_thread = true;      // option: listed long reads one thread each before the warp kernels
-  bool stealing = true;         // option: the listed-read kernels take work by atomic claims
+  // option "work_stealing": the warp chaining kernel takes reads by atomic claims on
+  // resident blocks (default) instead of striding over a fixed grid
+  bool stealing = true;
   // reads per block of the thread-per-read seeding kernel: option "seed_block" (0 = tuned
   // on the first batch of at least kSeedTuneReads reads, else 64 or 128) and the tuning
   int seed_block = 0;
@@ -598,7 +600,7 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
   CK(cudaMemsetAsync(info, 0, 10 * sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), st));
   CK(cudaMemsetAsync(c->d_count, 0, 4 * sizeof(int), st));
-  // work-stealing claim counters: [0] long-read kernel, [1] warp chaining kernel
+  // work-stealing claim counters: [1] warp chaining kernel ([0] spare)
   DBUF(claims, int, "claims", 2);
   CK(cudaMemsetAsync(claims, 0, 2 * sizeof(int), st));
   unsigned long long* ctr = info + 1;  // cells, mapped, candidates (map.cuh)
@@ -693,7 +695,7 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
     }
     if (c->long_thread && seed_long_supported(sp, cp) && max_len > seed_thread_max_len()) {
       // long reads one thread each, in length order; what exceeds its bounds goes on
-      const int64_t lt = seed_long_threads(n, c->stealing);
+      const int64_t lt = seed_long_threads(n);
       DBUF(lscr, uint32_t, "long_scratch", seed_long_scratch_words(lt));
       DBUF(big2, int32_t, "big2_list", n);
       const int32_t* order = big_list;
@@ -716,8 +718,7 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
       }
       kt.begin(st, "k_seed_chain_tl");
       if (!launch_seed_chain_long(st, d_seq_len, pofs, codes, order, big_n, lt, ix.dev, sp, cp, cand, cb, n_min,
-                                  n_anchor, n_anc_t, lscr, big2, c->d_count + 3, seed_thread_max_len(),
-                                  c->stealing ? claims : nullptr, c->d_err))
+                                  n_anchor, n_anc_t, lscr, big2, c->d_count + 3, seed_thread_max_len(), c->d_err))
         return fail(c, DNALN_ERR_CUDA, "long-read seeding kernel could not be configured");
       kt.end(st);
       warp_list = big2;

@@ -170,17 +170,15 @@ bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* s
 // min_len (typically those the short kernel listed) with their state in `scratch`
 // (seed_long_scratch_words(threads) words); the others, and reads past its bounds, go to
 // next_list (count *next_n) for the warp kernels.
-// threads = seed_long_threads(upper bound of the list length, stealing). With `claim` (an
-// int zeroed by the caller; then threads must come from seed_long_threads(n, true)) the
-// warps take 32 list positions at a time by an atomic add on *claim (work stealing).
+// threads = seed_long_threads(upper bound of the list length).
 bool seed_long_supported(const SeedParams& sp, const ChainParamsDev& cp);
-int64_t seed_long_threads(int64_t n_max, bool stealing);
+int64_t seed_long_threads(int64_t n_max);
 size_t seed_long_scratch_words(int64_t threads);
 bool launch_seed_chain_long(cudaStream_t st, const int32_t* seq_len, const int64_t* pofs, const uint8_t* codes,
                             const int32_t* list, const int* list_n, int64_t threads, const DevIndex& ix,
                             const SeedParams& sp, const ChainParamsDev& cp, const CandParams& cand, CandBuf cb,
                             int32_t* n_min, int64_t* n_anchor, int32_t* n_anc_t, uint32_t* scratch,
-                            int32_t* next_list, int* next_n, int min_len, int* claim, uint32_t* err);
+                            int32_t* next_list, int* next_n, int min_len, uint32_t* err);
 // Sort keys (longest first; slots at or past *list_n last) and values (read ids) of a list
 // whose length is only known on the device; n_max = the list buffer's size.
 void launch_long_order(cudaStream_t st, const int32_t* list, const int* list_n, int n_max, const int32_t* seq_len,

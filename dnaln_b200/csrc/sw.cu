@@ -14,8 +14,8 @@
 //    registers, the band row (H, E of W+1 cells, W target selectors) in registers.
 //    Values are kept biased by +16384, so every half stays positive and every add or
 //    subtract of the recurrence is one 32-bit integer add on both halves (no borrow can
-//    cross halves) — these run on the FMA pipe; maxima are unsigned 16x2 max
-//    (vmaxu2 / DPX vimax3_u16x2). The substitution scores of both alignments are one
+//    cross halves); E and F are DPX add-maxima (viaddmax), the other maxima unsigned 16x2
+//    max (vmaxu2 / DPX vimax3_u16x2). The substitution scores of both alignments are one
 //    prmt.b32 from an 8-byte per-row profile {s(qA, A..T) + 64, s(qB, A..T) + 64}.
 //    Direction bits come from non-negative differences (hd vs max(hd, E), ...)
 //    saturated to 0/1 with vminu2 and combined with integer multiply-adds.
@@ -38,7 +38,6 @@
 // takes the reference's steps. The best cell is the first strict maximum in row-major
 // order (per-row maximum with its first column, then strict across rows).
 #include <algorithm>
-#include <cstdlib>
 #include <type_traits>
 
 #include "common.cuh"
@@ -375,163 +374,28 @@ __device__ bool window_has_n(const SwTask& tk, int W, const uint8_t* __restrict_
 }
 
 // Two alignments per thread in biased 16-bit halves (A low, B high). Pairs it cannot take
-// (an N in a target window, or scores/lengths outside the 16-bit range) are listed in
-// fb (fb[0] = count, then local task indices) for k_sw_fb. With traceback at W <= 33 the
-// launch bound asks for three resident blocks (<= 170 registers, no spills), which gives
-// the latency-bound recurrence 12 warps per SM instead of 8.
-template <int W, bool TB>
-__global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1) k_sw_u2(const SwTask* __restrict__ tasks, int base, int n,
-                                                      const int* __restrict__ n_dev, const uint8_t* __restrict__ qbase,
-                                                      const uint8_t* __restrict__ tbase, SwParams p,
-                                                      SwResult* __restrict__ res, uint32_t* __restrict__ dir,
-                                                      int rows_max, int* __restrict__ fb) {
-  constexpr int WQ = (W + 3) / 4;
-  const int lt = blockIdx.x * blockDim.x + threadIdx.x;  // pair index within this launch
-  const int nn = n_dev ? min(n, *n_dev) : n;
-  const int ia = base + 2 * lt, ib = ia + 1;
-  if (ia >= nn) return;
-  const bool has_b = ib < nn;
-  uint32_t* DP = TB ? pair_base(dir, 2 * lt, rows_max, WQ) : nullptr;
-  const SwTask ta = tasks[ia];
-  SwTask tb = ta;
-  if (has_b) tb = tasks[ib];
-  else tb.qlen = 0;
-  const int qmax = max(ta.qlen, tb.qlen);
-  const bool fits = qmax * p.match + 2 * (p.oe + p.ge + p.mismatch + p.ambig) < 16000 &&
-                    p.match + kScoreBias <= 127 && p.mismatch <= kScoreBias && p.ambig <= kScoreBias;
-  if (!fits || window_has_n(ta, W, tbase) || (has_b && window_has_n(tb, W, tbase))) {
-    const int k = atomicAdd(fb, has_b ? 2 : 1);
-    fb[1 + k] = 2 * lt;
-    if (has_b) fb[2 + k] = 2 * lt + 1;
-    return;
-  }
-  const uint8_t* __restrict__ qa = qbase + ta.q_off;
-  const uint8_t* __restrict__ qb = qbase + tb.q_off;
-  const int qla = ta.qlen, qlb = tb.qlen;
-  // a target code of A or B past its own window only feeds rows that cannot matter to it
-  auto tc2 = [&](int64_t j) {
-    const uint32_t a = tcode(tbase, ta, j), b = has_b ? tcode(tbase, tb, j) : 0u;
-    return sel2(a > 3 ? 0u : a, b > 3 ? 0u : b);
-  };
-  auto qcode = [&](const uint8_t* __restrict__ q, int ql, int i) {
-    return i < ql ? min(static_cast<uint32_t>(q[i]), 4u) : 4u;
-  };
-  uint32_t H[W + 1], E[W + 1], T[W];
-#pragma unroll
-  for (int d = 0; d <= W; ++d) {
-    H[d] = kBias2;
-    E[d] = kBias2;
-  }
-#pragma unroll
-  for (int d = 0; d < W; ++d) T[d] = tc2(d);
-  const uint32_t OE = pack2(p.oe), GE = pack2(p.ge), SB = pack2(kScoreBias);
-  uint32_t best2 = kBias2;
-  uint32_t best_a = kBias, best_b = kBias;
-  int bi_a = -1, bi_b = -1;
-  // With traceback, each half's best row is kept in shared memory ([d][thread] words) the
-  // moment it improves the best score, and its first maximal column is found once, after
-  // the last row: one max per cell instead of tracking the argmax per cell.
-  extern __shared__ uint32_t sw_rows[];
-  uint32_t* const row_a = sw_rows + threadIdx.x;
-  uint32_t* const row_b = sw_rows + W * kSwThreads + threadIdx.x;
-  int buf_a = 0, buf_b = 1;  // which of the two row buffers holds each half's best row
-  uint32_t ca = qcode(qa, qla, 0), cb = qcode(qb, qlb, 0);
-  for (int i = 0; i < qmax; ++i) {
-    // rows past a query's end are N rows for it: they cannot raise its best (values only
-    // decrease) and its walk never reaches them. Next row's codes are loaded up front so
-    // their latency hides behind this row.
-    const uint32_t plo = prof_biased(p, ca), phi = prof_biased(p, cb);
-    const uint32_t t_next = tc2(static_cast<int64_t>(i) + W);
-    const uint32_t ca_next = qcode(qa, qla, i + 1), cb_next = qcode(qb, qlb, i + 1);
-    uint32_t f = kBias2, hleft = kBias2, hdiag = H[0], rmax = 0, dw = 0;
-#pragma unroll
-    for (int d = 0; d < W; ++d) {
-      const uint32_t hup = H[d + 1], eup = E[d + 1];
-      const uint32_t hd = hdiag + prmt(plo, phi, T[d]) - SB;
-      const uint32_t eo = hup - OE, ee = eup - GE, fo = hleft - OE, fe = f - GE;
-      const uint32_t e = __vmaxu2(eo, ee);
-      f = __vmaxu2(fo, fe);
-      const uint32_t m1 = __vmaxu2(hd, e);
-      const uint32_t h = __vimax3_u16x2(m1, f, kBias2);
-      H[d] = h;
-      E[d] = e;
-      if constexpr (TB) {
-        // each difference is >= 0 per half; saturated to 0/1 it is one code bit
-        const uint32_t c = ((__vminu2(m1 - hd, kOne2) * 2u + __vminu2(h - m1, kOne2)) * 2u +
-                            __vminu2(e - eo, kOne2)) * 2u + __vminu2(f - fo, kOne2);
-        dw = dw * 16u + c;
-        if ((d & 3) == 3 || d == W - 1) {
-          if ((d & 3) != 3) dw <<= 4 * (3 - (d & 3));
-          DP[(static_cast<size_t>(i) * WQ + (d >> 2)) * 32] = dw;
-          dw = 0;
-        }
-        rmax = d == 0 ? h : __vmaxu2(rmax, h);
-      } else {
-        best2 = __vmaxu2(best2, h);
-      }
-      hleft = h;
-      hdiag = hup;
-    }
-    if constexpr (TB) {  // a strictly better row (rows in order: the first strict maximum)
-      const bool up_a = (rmax & 0xFFFFu) > best_a, up_b = (rmax >> 16) > best_b;
-      if (up_a || up_b) {
-        const int dst = row_buffer(up_a, up_b, buf_a, buf_b);
-        uint32_t* const row = dst ? row_b : row_a;
-#pragma unroll
-        for (int d = 0; d < W; ++d) row[d * kSwThreads] = H[d];
-        if (up_a) {
-          best_a = rmax & 0xFFFFu;
-          bi_a = i;
-          buf_a = dst;
-        }
-        if (up_b) {
-          best_b = rmax >> 16;
-          bi_b = i;
-          buf_b = dst;
-        }
-      }
-    }
-#pragma unroll
-    for (int d = 0; d + 1 < W; ++d) T[d] = T[d + 1];
-    T[W - 1] = t_next;
-    ca = ca_next;
-    cb = cb_next;
-  }
-  int bd_a = 0, bd_b = 0;
-  if constexpr (!TB) {
-    best_a = best2 & 0xFFFFu;
-    best_b = best2 >> 16;
-  } else {  // first column of the best row holding the best value, per half
-    bd_a = bi_a >= 0 ? W : -1;
-    bd_b = bi_b >= 0 ? W : -1;
-    const uint32_t* const ra = buf_a ? row_b : row_a;
-    const uint32_t* const rb = buf_b ? row_b : row_a;
-#pragma unroll 1
-    for (int d = W - 1; d >= 0; --d) {
-      if (bi_a >= 0 && (ra[d * kSwThreads] & 0xFFFFu) == best_a) bd_a = d;
-      if (bi_b >= 0 && (rb[d * kSwThreads] >> 16) == best_b) bd_b = d;
-    }
-  }
-  res[ta.slot] = stash(static_cast<int>(best_a) - static_cast<int>(kBias), TB ? bi_a : 0, bd_a);
-  if (has_b) res[tb.slot] = stash(static_cast<int>(best_b) - static_cast<int>(kBias), TB ? bi_b : 0, bd_b);
-}
-
-// k_sw_u2 with fewer instructions per cell (same results, same outputs):
+// (an N in a target window, or scores/lengths outside the 16-bit range) are listed in fb
+// (fb[0] = count, then local task indices) for k_sw_fb. With traceback at W <= 33 the
+// launch bound asks for three resident blocks (<= 170 registers, no spills): 12 warps per
+// SM instead of 8. Per cell:
 //  * E and F by the DPX add-max (max(a + b, c) in one instruction, signed 16x2: the biased
 //    values lie in [0, 32767], where signed and unsigned order agree), so the open-gap
 //    candidates hup - (O+E) and hleft - (O+E) are never materialised; the extension bits
 //    come from e - hup + (O+E) and f - hleft + (O+E), one 3-input add each (both halves
 //    non-negative, so no borrow crosses them);
-//  * the substitution profile of a query code from a 5-entry table in shared memory, the
-//    next row's read one row ahead;
-//  * target codes read without range or N checks: the pair reaches this point only when
+//  * the substitution scores of both alignments are one prmt.b32 on the row's profile
+//    words, taken from a 5-entry table in shared memory one row ahead;
+//  * target codes are read without range or N checks: the pair reaches the DP only when
 //    both windows [0, qlen + W - 1) are N-free and inside their contigs, and reads past a
 //    window are clamped to its last base (a row past a query's end is an N row for it,
 //    whose scores do not depend on the target), so a code is always 0..3 and the prmt
 //    selector of two codes is two multiply-adds.
+// Against the former form (vmax of materialised open/extend candidates, profile words
+// rebuilt per row, range-checked target reads) this took the traceback kernel from 3.06 to
+// 2.56 ms per 1,000,000 x 150 bp reads.
 template <int W, bool TB>
 __global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1)
-    k_sw_u2v(const SwTask* __restrict__ tasks, int base, int n, const int* __restrict__ n_dev,
+    k_sw_u2(const SwTask* __restrict__ tasks, int base, int n, const int* __restrict__ n_dev,
              const uint8_t* __restrict__ qbase, const uint8_t* __restrict__ tbase, SwParams p,
              SwResult* __restrict__ res, uint32_t* __restrict__ dir, int rows_max, int* __restrict__ fb) {
   static_assert(W >= 3, "a window of at least two columns past an empty query");
@@ -1157,15 +1021,6 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_any(const SwTask* __restrict_
   res[tk.slot] = r;
 }
 
-// EXPERIMENT (to be removed): which k_sw_u2 form runs, from DNALN_SW_VARIANT (default 1).
-inline int sw_variant() {
-  static const int v = [] {
-    const char* e = std::getenv("DNALN_SW_VARIANT");
-    return e ? std::atoi(e) : 1;
-  }();
-  return v;
-}
-
 template <int W>
 void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int count, int n, const int* n_dev,
                const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res, uint32_t* dir,
@@ -1192,17 +1047,8 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
       set_smem_limit_once(k_sw_u2<W, true>, kRowBytes, attr_set);
     }
     t.begin(st, "k_sw_u2<tb>");
-    if (sw_variant()) {
-      if (kRowBytes > 48 * 1024) {
-        static std::atomic<bool> attr_set2[kMaxDevices];
-        set_smem_limit_once(k_sw_u2v<W, true>, kRowBytes, attr_set2);
-      }
-      k_sw_u2v<W, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
-                                                                     rows_max, fb);
-    } else {
-      k_sw_u2<W, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
-                                                                    rows_max, fb);
-    }
+    k_sw_u2<W, true><<<blocks_pairs, kSwThreads, kRowBytes, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
+                                                                  rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<tb>");
     if constexpr (kLanesFb)
@@ -1216,12 +1062,8 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
     t.end(st);
   } else {
     t.begin(st, "k_sw_u2<score>");
-    if (sw_variant())
-      k_sw_u2v<W, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
-                                                              rows_max, fb);
-    else
-      k_sw_u2<W, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir,
-                                                             rows_max, fb);
+    k_sw_u2<W, false><<<blocks_pairs, kSwThreads, 0, st>>>(tasks, base, n, n_dev, qbase, tbase, p, res, dir, rows_max,
+                                                           fb);
     t.end(st);
     t.begin(st, "k_sw_fb<score>");
     if constexpr (kLanesFb)
@@ -1330,6 +1172,10 @@ bool launch_sw(cudaStream_t st, bool tb, bool bytes_ok, const SwTask* tasks, int
   if (count <= 0) return true;
   const bool generic = sw_uses_generic(p.W, bytes_ok);
   if ((tb && !dir) || (generic && !band) || (!generic && !fb) || (base % kSwTaskGroup) != 0) return false;
+  // the kernels bound their tasks by n (and the device count): a launch covers tasks
+  // [base, base + count) only, so that no thread of a grid rounded up past `count` takes a
+  // task of the next chunk, whose scratch this launch does not hold
+  if (n > base + count) n = base + count;
   if (!generic && form != kSwInter && sw_has_form(p.W, bytes_ok, form)) {
 #define DNB_SW_WIDE(L, CHV) \
   launch_wide<L, CHV>(st, tb, tasks, base, count, n, n_dev, qbase, tbase, p, res, dir, rows_max, cig, cig_off, fb, err, kt)

@@ -146,9 +146,9 @@ int dnaln_gpu_set_sub_batch(dnaln_ctx* ctx, int64_t reads);
  *                    first (default); 0 = in read order;
  *   "seed_block"     reads per block of the thread-per-read seeding kernel: 0 = tuned
  *                    (default, dnaln_gpu_seed_tuning), 64 or 128;
- *   "work_stealing"  1 = the kernels of listed reads (long reads one thread each, the
- *                    rest one warp each) run on the resident blocks only, each warp taking
- *                    its next work by an atomic claim (default); 0 = fixed grids;
+ *   "work_stealing"  1 = the warp-per-read chaining kernel runs on the resident blocks
+ *                    only, each warp taking its next read by an atomic claim (default);
+ *                    0 = a fixed grid striding over the reads;
  *   "dir_cap_bytes"  traceback direction-code scratch per launch (default 1/32 of the
  *                    device's memory, at least 1 GiB and at most 8 GiB; a launch whose
  *                    tasks need more is split into chunks);

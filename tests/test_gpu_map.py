@@ -331,18 +331,19 @@ def test_seed_block_tuner_and_pinned_sizes_agree(ctx):
 
 @pytest.mark.parametrize("wl", ["repeat", "mixed"])
 def test_work_stealing_and_fixed_grids_agree(ctx, request, wl):
-    # the listed-read kernels (long reads one thread each, the rest one warp each) either
-    # take work by atomic claims on resident blocks or stride over fixed grids: same records
+    # the warp-per-read chaining kernel either takes reads by atomic claims on resident
+    # blocks or strides over a fixed grid: same records
     g, reads, _ = request.getfixturevalue(wl)
     p = D.default_map_params()
     iid = ctx.index_build(g)
     try:
-        ctx.set_option("work_stealing", 1)
-        a = ctx.map_batch(iid, reads, p)
-        ctx.set_option("work_stealing", 0)
-        b = ctx.map_batch(iid, reads, p)
+        got = []
+        for mode in (1, 0):
+            ctx.set_option("work_stealing", mode)
+            got.append(ctx.map_batch(iid, reads, p))
     finally:
         ctx.set_option("work_stealing", 1)
         ctx.index_free(iid)
-    assert np.array_equal(gpu_records(a), gpu_records(b))
-    assert np.array_equal(a.cigar, b.cigar)
+    for other in got[1:]:
+        assert np.array_equal(gpu_records(got[0]), gpu_records(other))
+        assert np.array_equal(got[0].cigar, other.cigar)
