@@ -203,6 +203,7 @@ struct dnaln_ctx {
 namespace {
 
 constexpr int64_t kSeedTuneReads = 32768;  // smallest batch the reads-per-block tuner times
+constexpr int64_t kSwTuneMinTasks = 4096;  // smallest SW sample whose timing picks a form
 
 int fail(dnaln_ctx* c, int code, const char* fmt, ...) {
   char buf[512];
@@ -540,6 +541,9 @@ int launch_sw_chunked(dnaln_ctx* c, bool tb, bool bytes_ok, const SwTask* tasks,
           form = forms[x];
         }
       }
+      // a sample of a few tasks times launch overheads, not the forms: keep the width's
+      // first form (inter-sequence where it has one)
+      if (live < kSwTuneMinTasks) form = forms.front();
       t.ms_inter = sw_has_form(sp.W, bytes_ok, kSwInter) ? ms[kSwInter] : -1.0;
       t.ms_intra = sw_has_form(sp.W, bytes_ok, kSwIntra) ? ms[kSwIntra] : -1.0;
       t.ms_narrow = sw_has_form(sp.W, bytes_ok, kSwIntraNarrow) ? ms[kSwIntraNarrow] : -1.0;

@@ -779,20 +779,23 @@ __global__ void __launch_bounds__(kSwThreads) k_sw_fb(const SwTask* __restrict__
 }
 
 // The tasks k_sw_u2 / k_sw_wide listed (an N in the target window, or outside the biased
-// 16-bit range) for bands of W = 32 * LANES + 1 columns, one alignment per LANES lanes in
-// int32: lane c holds band columns [32c, 32c + 32) (the last lane also column W - 1) and
+// 16-bit range) for bands of W = CH * LANES + 1 columns, one alignment per LANES lanes in
+// int32: lane c holds band columns [CH c, CH c + CH) (the last lane also column W - 1) and
 // computes row t - c at step t — k_sw_wide's skewed wavefront, exchanging the left lane's
 // last (H, F) and the right lane's first (H, E) by shuffles. Scores come from the 5-entry
 // profile (N scored as the reference scores it), direction codes go to the task's half of
 // the pair words, the best cell is the first strict maximum in row-major order: the same
 // results and codes as sw_one_reg, which runs one alignment per thread and, at W = 129,
-// spills its band to local memory.
-template <int LANES, bool TB>
+// spills its band to local memory. The list is short (windows that cross a contig end or
+// an N run), so the kernel's time is one task's serial latency: narrow chunks (8 or 16
+// cells per lane) spread a task over more lanes and shorten it.
+template <int LANES, int CH, bool TB>
 __global__ void __launch_bounds__(kSwThreads)
     k_sw_fb_lanes(const SwTask* __restrict__ tasks, int base, const uint8_t* __restrict__ qbase,
                   const uint8_t* __restrict__ tbase, SwParams p, SwResult* __restrict__ res,
                   uint32_t* __restrict__ dir, int rows_max, const int* __restrict__ fb) {
-  constexpr int W = 32 * LANES + 1, WQ = (W + 3) / 4, CH = 32;
+  static_assert(CH % 4 == 0 && CH >= 8, "a lane's cells fill whole direction words");
+  constexpr int W = CH * LANES + 1, WQ = (W + 3) / 4;
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int c = lane % LANES;
@@ -1028,14 +1031,15 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
   const int pairs = (count + 1) / 2;
   const int blocks_pairs = (pairs + kSwThreads - 1) / kSwThreads;
   const int blocks_tasks = (count + kSwThreads - 1) / kSwThreads;
-  // W = 65: the fallback list runs two lanes per alignment (k_sw_fb_lanes<2>); narrower
-  // bands keep the one-thread kernel, whose band fits in registers
-  constexpr bool kLanesFb = W == 65;
+  // W = 33 and 65: the fallback list runs four lanes per alignment (k_sw_fb_lanes), the
+  // other widths the one-thread kernel, whose band fits in registers
+  constexpr bool kLanesFb = W == 33 || W == 65;
+  constexpr int kFbCh = (W - 1) / 4;
   // the fallback kernels stride over a list whose length only the device knows (usually
   // short or empty): a few resident waves, not one block per possible entry
   const int fb_cap = 8 * device_sm_count();
   const int blocks_fb =
-      std::min(fb_cap, static_cast<int>((static_cast<int64_t>(count) * 2 + kSwThreads - 1) / kSwThreads));
+      std::min(fb_cap, static_cast<int>((static_cast<int64_t>(count) * 4 + kSwThreads - 1) / kSwThreads));
   const int blocks_fb1 = std::min(fb_cap, blocks_tasks);
   const KernelTrace none;
   const KernelTrace& t = kt ? *kt : none;
@@ -1052,7 +1056,8 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
     t.end(st);
     t.begin(st, "k_sw_fb<tb>");
     if constexpr (kLanesFb)
-      k_sw_fb_lanes<2, true><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+      k_sw_fb_lanes<4, kFbCh, true><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir,
+                                                                      rows_max, fb);
     else
       k_sw_fb<W, true><<<blocks_fb1, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     t.end(st);
@@ -1067,7 +1072,8 @@ void launch_u2(cudaStream_t st, bool tb, const SwTask* tasks, int base, int coun
     t.end(st);
     t.begin(st, "k_sw_fb<score>");
     if constexpr (kLanesFb)
-      k_sw_fb_lanes<2, false><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+      k_sw_fb_lanes<4, kFbCh, false><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir,
+                                                                       rows_max, fb);
     else
       k_sw_fb<W, false><<<blocks_fb1, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
     t.end(st);
@@ -1079,7 +1085,8 @@ void launch_wide(cudaStream_t st, bool tb, const SwTask* tasks, int base, int co
                  const uint8_t* qbase, const uint8_t* tbase, const SwParams& p, SwResult* res, uint32_t* dir,
                  int rows_max, uint32_t* cig, const int64_t* cig_off, int* fb, uint32_t* err, const KernelTrace* kt) {
   constexpr int W = CH * LANES + 1;
-  constexpr int FBL = (W - 1) / 32;  // lanes per alignment of the int32 fallback kernel
+  constexpr int FBCH = W == 33 ? 8 : 16;  // cells per lane of the int32 fallback kernel
+  constexpr int FBL = (W - 1) / FBCH;     // its lanes per alignment
   const int pairs = (count + 1) / 2;
   const int blocks_pairs = static_cast<int>((static_cast<int64_t>(pairs) * LANES + kSwThreads - 1) / kSwThreads);
   const int blocks_tasks = (count + kSwThreads - 1) / kSwThreads;
@@ -1097,7 +1104,8 @@ void launch_wide(cudaStream_t st, bool tb, const SwTask* tasks, int base, int co
                                                                             res, dir, rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<tb>");
-    k_sw_fb_lanes<FBL, true><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max, fb);
+    k_sw_fb_lanes<FBL, FBCH, true><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max,
+                                                                     fb);
     t.end(st);
     t.begin(st, "k_sw_walk");
     k_sw_walk<W><<<blocks_tasks, kSwThreads, 0, st>>>(tasks, base, count, n, n_dev, qbase, tbase, p, res, dir,
@@ -1109,8 +1117,8 @@ void launch_wide(cudaStream_t st, bool tb, const SwTask* tasks, int base, int co
                                                                      rows_max, fb);
     t.end(st);
     t.begin(st, "k_sw_fb<score>");
-    k_sw_fb_lanes<FBL, false><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir, rows_max,
-                                                                fb);
+    k_sw_fb_lanes<FBL, FBCH, false><<<blocks_fb, kSwThreads, 0, st>>>(tasks, base, qbase, tbase, p, res, dir,
+                                                                      rows_max, fb);
     t.end(st);
   }
 }

@@ -169,7 +169,8 @@ int dnaln_gpu_set_option(dnaln_ctx* ctx, const char* name, int64_t value);
  * (W - 1) / 16 lanes of 16 cells; W = 33, 65, 129) — have every form timed on the first
  * batch of each (band width, traceback or score-only, read-length bucket <= 256 / <= 1024
  * / longer) a context maps, and the fastest runs from then on (`tasks` says how large the
- * timed sample was). All forms give identical results. ms_* = -1 for a form the width
+ * timed sample was; a sample under 4,096 tasks keeps the width's first form, inter-sequence
+ * where it has one). All forms give identical results. ms_* = -1 for a form the width
  * lacks. Writes min(cap, count) entries; *n_out = count. */
 typedef struct {
   int32_t W, traceback, len_bucket, form; /* form: 0 inter-sequence, 1 intra-sequence, 2 intra narrow */

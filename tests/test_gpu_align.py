@@ -160,5 +160,8 @@ def test_sw_forms_identical_and_tuned(ctx, port, bw):
         assert t["ms_intra"] > 0 and t["ms_narrow"] > 0
         assert (t["ms_inter"] > 0) == (W != 129)
         timed = {f: ms for f, ms in enumerate((t["ms_inter"], t["ms_intra"], t["ms_narrow"])) if ms > 0}
-        assert t["form"] == min(timed, key=timed.get)  # the fastest form was chosen
+        if t["tasks"] >= 4096:
+            assert t["form"] == min(timed, key=timed.get)  # the fastest form was chosen
+        else:  # too small a sample to time: the width's first form
+            assert t["form"] == min(timed)
         assert t["lanes_per_pair"] == {0: 1, 1: (W - 1) // 32, 2: (W - 1) // 16}[t["form"]]
