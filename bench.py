@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--serve-lanes", type=int, default=3)
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.5, 0.8],
                     help="offered loads as fractions of the measured capacity (--workload serve)")
+    ap.add_argument("--dir-cap-bytes", type=int, default=0,
+                    help="traceback direction-code scratch per launch (0 = the library's default; smaller splits "
+                         "launches, e.g. to keep a profiled case small)")
     ap.add_argument("--no-legs", action="store_true",
                     help="skip the mixed-length (batched vs plain, bw 16 / 64) and serving legs of the default run")
     ap.add_argument("--leg-requests", type=int, default=600, help="requests per load point of the serving leg")
@@ -560,6 +563,8 @@ def run_ours(args) -> None:
     p = D.default_map_params(bw=args.bw)
     ctx = D.Context(local)
     ctx.set_option("sw_form", args.sw_form)
+    if args.dir_cap_bytes:
+        ctx.set_option("dir_cap_bytes", args.dir_cap_bytes)
     t_ix = time.perf_counter()
     iid = ctx.index_build(g)
     index_build_s = time.perf_counter() - t_ix
