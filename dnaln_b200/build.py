@@ -22,7 +22,7 @@ LIB = PKG / "libdnaln_b200.so"
 
 CUDA_SOURCES = ["csrc/sw.cu", "csrc/seed.cu", "csrc/seed_thread.cu", "csrc/map.cu", "csrc/capi.cu", "csrc/noalloc.cu",
                 "csrc/serve.cu", "csrc/index_build.cu",
-                "csrc/seed_long.cu", "csrc/peak.cu"]
+                "csrc/seed_long.cu", "csrc/peak.cu", "csrc/encode_bulk.cu"]
 HOST_SOURCES = ["host/sam.cpp", "host/reads.cpp", "host/eval.cpp"]
 # the seeded workload generator, a library of its own (no CUDA): programs that only need
 # workloads, such as the reference's CPU baseline, load it without the mapping path

@@ -166,6 +166,9 @@ struct dnaln_ctx {
   // option "work_stealing": the warp chaining kernel takes reads by atomic claims on
   // resident blocks (default) instead of striding over a fixed grid
   bool stealing = true;
+  // option "encode_bulk": the codes of both strands through shared memory by bulk (TMA)
+  // copies, or read by read from global memory (default: measured faster)
+  bool encode_bulk = false;
   // reads per block of the thread-per-read seeding kernel: option "seed_block" (0 = tuned
   // on the first batch of at least kSeedTuneReads reads, else 64 or 128) and the tuning
   int seed_block = 0;
@@ -415,9 +418,9 @@ inline unsigned nblk(int64_t n, int t = 256) { return static_cast<unsigned>((n +
 int check_device_errors(dnaln_ctx* c, uint32_t bits) {
   if (bits == 0) return DNALN_OK;
   return fail(c, DNALN_ERR_DEVICE, "kernel error flags 0x%x (traceback bounds %d, cigar overflow %d, chain scratch %d, "
-                                   "probe loop %d)",
+                                   "probe loop %d, bulk copy wait %d)",
               bits, !!(bits & kErrTracebackBounds), !!(bits & kErrCigarOverflow), !!(bits & kErrChainScratch),
-              !!(bits & kErrProbeLoop));
+              !!(bits & kErrProbeLoop), !!(bits & kErrAsyncCopy));
 }
 
 // SW tasks of a batch whose reads differ in length, longest first (a thread's two
@@ -659,7 +662,10 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
   CK(cudaEventRecord(c->ev[kEvSeed0], st));
   if (thread_path) {
     kt.begin(st, "k_encode_reads");
-    launch_encode_reads(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, codes);
+    if (c->encode_bulk)
+      launch_encode_reads_bulk(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, codes, c->d_err);
+    else
+      launch_encode_reads(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, pofs, n, codes);
     kt.end(st);
     c->stats.launches += 1;
     const auto seed_t = [&](int rpb) {
@@ -959,7 +965,7 @@ std::string graph_key(const dnaln_ctx* c, const IndexRes& ix, const char* d_seq,
   put(ptrs, sizeof ptrs);
   const int64_t nums[] = {n, hint.seq_base, hint.bases, hint.max_len, hint.cigar_base, cigar_cap, c->pool_cap,
                           static_cast<int64_t>(c->dir_cap_bytes), c->sw_mode, c->warp_seed_only, c->long_thread,
-                          c->length_order, c->stealing, c->seed_block,
+                          c->length_order, c->stealing, c->encode_bulk, c->seed_block,
                           c->seed_tune.tuned ? c->seed_tune.reads_per_block : 0};
   put(nums, sizeof nums);
   put(&p, sizeof p);
@@ -1508,6 +1514,10 @@ int dnaln_gpu_set_option(dnaln_ctx* c, const char* name, int64_t value) {
     if (value != 0 && value != 64 && value != 128)
       return fail(c, DNALN_ERR_INVALID_ARG, "seed_block must be 0 (tuned), 64 or 128");
     c->seed_block = static_cast<int>(value);
+    return DNALN_OK;
+  }
+  if (k == "encode_bulk") {
+    c->encode_bulk = value != 0;
     return DNALN_OK;
   }
   if (k == "work_stealing") {

@@ -68,6 +68,8 @@ enum : uint32_t {
   // query longer than the stated maximum, a negative length or offset); the call fails
   // with DNALN_ERR_INVALID_ARG and the other tasks' results stand
   kErrBadTask = 1u << 6,
+  // a bulk (TMA) copy into shared memory did not complete within its wait's bound
+  kErrAsyncCopy = 1u << 7,
 };
 
 // Thomas Wang's 64-bit mix restricted to `mask` bits, step for step as the index keys are

@@ -149,6 +149,11 @@ void launch_chain_map(cudaStream_t st, const int64_t* pofs, const int32_t* seq_l
 // reverse complement right after it (src/mapper.cpp:88-99), from the ASCII reads.
 void launch_encode_reads(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
                          const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes);
+// The same codes through shared memory by bulk (TMA) copies, tiles of back-to-back reads
+// (encode_bulk.cu); a tile that is not back to back is encoded read by read. err gets
+// kErrAsyncCopy if a bulk load's bounded wait runs out.
+void launch_encode_reads_bulk(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+                              const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes, uint32_t* err);
 
 // One thread per read (seed_thread.cu): passes 1 and 2 of the reads the per-thread budgets
 // admit, from their ASCII bytes (the codes in HBM are launch_encode_reads' job), writing

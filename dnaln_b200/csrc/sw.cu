@@ -561,6 +561,9 @@ __global__ void __launch_bounds__(kSwThreads, TB ? (CH == 16 ? 4 : 3) : 1)
   static_assert(CH % 4 == 0 && CH >= 8, "a lane's cells fill whole direction words");
   constexpr int W = CH * LANES + 1, WQ = (W + 3) / 4;
   constexpr unsigned FULL = 0xffffffffu;
+  __shared__ uint32_t s_prof[8];  // profile words of the five query codes
+  if (threadIdx.x < 5) s_prof[threadIdx.x] = prof_biased(p, threadIdx.x);
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int c = lane % LANES;  // chunk of this lane
   const int lt = (blockIdx.x * blockDim.x + threadIdx.x) / LANES;  // pair index within this launch
@@ -590,9 +593,16 @@ __global__ void __launch_bounds__(kSwThreads, TB ? (CH == 16 ? 4 : 3) : 1)
   const uint8_t* __restrict__ qa = qbase + ta.q_off;
   const uint8_t* __restrict__ qb = qbase + tb.q_off;
   const int qla = ta.qlen, qlb = tb.qlen;
-  auto tc2 = [&](int64_t j) {
-    const uint32_t a = tcode(tbase, ta, j), b = has_b ? tcode(tbase, tb, j) : 0u;
-    return sel2(a > 3 ? 0u : a, b > 3 ? 0u : b);
+  // called for pairs that run here only: both windows [0, qlen + W - 1) N-free and inside
+  // their contigs, so column j reads its window at min(j, qlen + W - 2), a code in 0..3
+  // (past a window's end it feeds N rows only), and the prmt selector of two codes is two
+  // multiply-adds (as k_sw_u2)
+  const uint8_t* __restrict__ wa = tbase + ta.t_start;
+  const uint8_t* __restrict__ wb = tbase + tb.t_start;
+  const int ja = ta.qlen + W - 2, jb = tb.qlen + W - 2;
+  auto tc2 = [&](int j) {
+    const uint32_t a = __ldg(wa + min(j, ja)), b = __ldg(wb + min(j, jb));
+    return a * 17u + b * 4352u + 50304u;  // sel2(a, b)
   };
   auto qcode = [&](const uint8_t* __restrict__ q, int ql, int i) {
     return i >= 0 && i < ql ? min(static_cast<uint32_t>(q[i]), 4u) : 4u;
@@ -614,6 +624,10 @@ __global__ void __launch_bounds__(kSwThreads, TB ? (CH == 16 ? 4 : 3) : 1)
   uint32_t* const row_b = sw_rows + (CH + 1) * kSwThreads + threadIdx.x;
   int buf_a = 0, buf_b = 1;  // which of the two row buffers holds each half's best row
   uint32_t hout = kBias2, fout = kBias2;  // this lane's last cell of its previous row
+  // the row's profile words, and the codes of the next step's row: loaded a step ahead so
+  // their latency hides behind the step (row -c of a lane that has not reached row 0 is N)
+  uint32_t plo = s_prof[qcode(qa, qla, -c)], phi = s_prof[qcode(qb, qlb, -c)];
+  uint32_t cna = qcode(qa, qla, 1 - c), cnb = qcode(qb, qlb, 1 - c);
   const auto step = [&](const int t, auto steady) {
     constexpr bool kSteady = decltype(steady)::value;
     const int i = t - c;
@@ -625,11 +639,11 @@ __global__ void __launch_bounds__(kSwThreads, TB ? (CH == 16 ? 4 : 3) : 1)
     // row i's F and H(left) at column d0 - 1, from the left lane (its step t - 1)
     uint32_t hleft = __shfl_up_sync(FULL, hout, 1), f = __shfl_up_sync(FULL, fout, 1);
     if (c == 0) hleft = f = kBias2;
-    const uint32_t ca = qcode(qa, qla, i), cb = qcode(qb, qlb, i);
-    const uint32_t plo = prof_biased(p, ca), phi = prof_biased(p, cb);
+    const uint32_t plo_next = s_prof[cna], phi_next = s_prof[cnb];
+    const uint32_t cna_next = qcode(qa, qla, i + 2), cnb_next = qcode(qb, qlb, i + 2);
     // past the pair's end the window shifts in a valid selector (code A for both): the
     // profile of an N row scores every target alike
-    const uint32_t t_next = act ? tc2(static_cast<int64_t>(i) + 1 + d0 + CH) : sel2(0u, 0u);
+    const uint32_t t_next = act ? tc2(i + 1 + d0 + CH) : sel2(0u, 0u);
     uint32_t hdiag = H[0], rmax = 0, dw = 0;
     // local cell 0, then hand (H, E) of it to the left lane: the E input of its last cell
     uint32_t h0, e0;
@@ -721,6 +735,10 @@ __global__ void __launch_bounds__(kSwThreads, TB ? (CH == 16 ? 4 : 3) : 1)
       for (int k = 0; k < CH; ++k) T[k] = T[k + 1];
       T[CH] = t_next;
     }
+    plo = plo_next;
+    phi = phi_next;
+    cna = cna_next;
+    cnb = cnb_next;
   };
   const int ramp = steps < LANES - 1 ? steps : LANES - 1;
   for (int t = 0; t < ramp; ++t) step(t, std::false_type{});

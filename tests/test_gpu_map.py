@@ -347,3 +347,42 @@ def test_work_stealing_and_fixed_grids_agree(ctx, request, wl):
     for other in got[1:]:
         assert np.array_equal(gpu_records(got[0]), gpu_records(other))
         assert np.array_equal(got[0].cigar, other.cigar)
+
+
+def test_bulk_encode_and_per_read_encode_agree(ctx, mixed, small):
+    # the codes of both strands come from shared-memory tiles moved by bulk copies when a
+    # tile's reads are back to back, read by read otherwise; records must not depend on it,
+    # for packed reads and for reads stored out of order (every tile not back to back)
+    from dnaln_b200 import _native as N
+    for g, reads in ((mixed[0], mixed[1]), (small[0], small[1].slice(0, 4000))):
+        p = D.default_map_params()
+        iid = ctx.index_build(g)
+        try:
+            got = []
+            for bulk in (1, 0):
+                ctx.set_option("encode_bulk", bulk)
+                got.append(ctx.map_batch(iid, reads, p))
+            # reads stored in a permuted order in the buffer (offsets still per read)
+            n = len(reads)
+            order = np.random.default_rng(3).permutation(n)
+            chunks = [reads.read(int(i)) for i in order]
+            buf = np.frombuffer(b"".join(chunks), np.uint8).copy()
+            pos = np.zeros(n, np.int64)
+            pos[order] = np.concatenate([[0], np.cumsum([len(x) for x in chunks])[:-1]])
+            lens = np.ascontiguousarray(reads.seq_len)
+            nh = reads.name_hash()
+            rec = np.zeros(n, dtype=D.MAP_RECORD_DTYPE)
+            cap = int(np.sum(2 * lens.astype(np.int64) + 3))
+            cig = np.zeros(cap, np.uint32)
+            used = D.C.c_int64()
+            ctx.set_option("encode_bulk", 1)
+            rc = N.lib().dnaln_gpu_map_batch(ctx.handle, iid, N.ptr(buf), N.ptr(pos), N.ptr(lens), N.ptr(nh), n,
+                                             D.C.byref(p), N.ptr(rec), N.ptr(cig), cap, D.C.byref(used))
+            assert rc == 0, N.lib().dnaln_gpu_last_error(ctx.handle).decode()
+            got.append(D.MapResult(rec, cig[:used.value]))
+        finally:
+            ctx.set_option("encode_bulk", 0)
+            ctx.index_free(iid)
+        for other in got[1:]:
+            assert np.array_equal(gpu_records(got[0]), gpu_records(other))
+            assert np.array_equal(got[0].cigar, other.cigar)
