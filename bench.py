@@ -63,6 +63,10 @@ def parse():
     ap.add_argument("--serve-lanes", type=int, default=3)
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.5, 0.8],
                     help="offered loads as fractions of the measured capacity (--workload serve)")
+    ap.add_argument("--lanes", type=int, default=2, choices=[1, 2, 3, 4],
+                    help="mapping lanes: contexts sharing the resident index, each with its own stream and host "
+                         "thread; the step's batches alternate between them so one batch's kernels overlap "
+                         "another's (1 = one context, batches in sequence)")
     ap.add_argument("--dir-cap-bytes", type=int, default=0,
                     help="traceback direction-code scratch per launch (0 = the library's default; smaller splits "
                          "launches, e.g. to keep a profiled case small)")
@@ -562,24 +566,61 @@ def run_ours(args) -> None:
     n_reads = len(reads)
     p = D.default_map_params(bw=args.bw)
     ctx = D.Context(local)
-    ctx.set_option("sw_form", args.sw_form)
-    if args.dir_cap_bytes:
-        ctx.set_option("dir_cap_bytes", args.dir_cap_bytes)
     t_ix = time.perf_counter()
     iid = ctx.index_build(g)
     index_build_s = time.perf_counter() - t_ix
     L = N.lib()
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
+    # mapping lanes: further contexts share the one resident index (dnaln_gpu_index_attach),
+    # each with its own stream and buffers; batch k of a step goes to lane k % lanes
+    n_lanes = max(1, args.lanes)
+    lanes = [(ctx, iid, stream)]
+    for _ in range(1, n_lanes):
+        c2 = D.Context(local)
+        s2 = torch.cuda.Stream()
+        c2.set_stream(s2.cuda_stream)
+        lanes.append((c2, c2.index_attach(ctx, iid), s2))
+    for c, _, _ in lanes:
+        c.set_option("sw_form", args.sw_form)
+        if args.dir_cap_bytes:
+            c.set_option("dir_cap_bytes", args.dir_cap_bytes)
 
     spans = [(a, min(n_reads, a + BATCH)) for a in range(0, n_reads, BATCH)]
     parts = [reads.slice(a, b) for a, b in spans]
 
     # ---- device-resident inputs (value) --------------------------------------------
     dev = device_parts(reads, args.cigar_per_read)
+    lane_parts = [dev[k::n_lanes] for k in range(n_lanes)]
+    import concurrent.futures as cf
+    pool = cf.ThreadPoolExecutor(max_workers=n_lanes) if n_lanes > 1 else None
 
     def step_device():
-        map_device_step(ctx, iid, dev, p)
+        if pool is None:
+            map_device_step(ctx, iid, dev, p)
+            return
+        futs = [pool.submit(map_device_step, c, ix, lane_parts[k], p) for k, (c, ix, _) in enumerate(lanes)]
+        for f in futs:
+            f.result()
+
+    def all_lanes(fn):
+        for c, _, _ in lanes:
+            fn(c)
+
+    def merged_kernel_times():
+        out = {}
+        for c, _, _ in lanes:
+            for k, (n, t) in c.kernel_times().items():
+                a = out.get(k, (0, 0.0))
+                out[k] = (a[0] + n, a[1] + t)
+        return out
+
+    def merged_stats():
+        out = {}
+        for c, _, _ in lanes:
+            for k, v in c.stats().items():
+                out[k] = out.get(k, 0) + v
+        return out
 
     def barrier():
         if dist is not None:
@@ -593,45 +634,62 @@ def run_ours(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    # each lane's first batches alone: its tuners (SW kernel form, reads per block) time the
+    # kernels without another lane's work on the GPU
+    for c, ix, _ in lanes:
+        map_device_step(c, ix, dev[:2], p)
+        torch.cuda.synchronize()
     for _ in range(max(args.warmup, 3)):
         step_device()
     # kernel breakdown: every launch of PROFILE_STEPS untimed steps bracketed by event pairs
+    # (one lane, batches in sequence, so each launch's span is its own)
     barrier()
     ctx.reset_stats()
     ctx.set_kernel_trace(True)
     for _ in range(PROFILE_STEPS):
-        step_device()
+        map_device_step(ctx, iid, dev, p)
     barrier()
     breakdown = ctx.kernel_times()
+    ctx.set_kernel_trace(False)
     dom = max(breakdown, key=lambda k: breakdown[k][1])
-    # timed region: only the dominant kernel's launches carry event pairs (one per batch)
-    ctx.reset_stats()
-    ctx.set_kernel_trace(True, only=dom)
+    # timed region: only the dominant kernel's launches carry event pairs (one per batch).
+    # The start event is on the first lane's stream and every other lane's stream waits for
+    # it; the end event follows every lane's work (max over the lanes)
+    all_lanes(lambda c: c.reset_stats())
+    all_lanes(lambda c: c.set_kernel_trace(True, only=dom))
     clocks = ClockSampler(local)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    for _, _, sk in lanes[1:]:
+        sk.wait_event(e0)
     for _ in range(args.steps):
         step_device()
+    for _, _, sk in lanes[1:]:
+        stream.wait_stream(sk)
     e1.record(stream)
     barrier()
     clk = clocks.result()
     ms = max_over_ranks(e0.elapsed_time(e1))
-    st = ctx.stats()
-    ktimes = ctx.kernel_times()
-    ctx.set_kernel_trace(False)
+    st = merged_stats()
+    ktimes = merged_kernel_times()
+    # traceback SW tasks of the lanes whose dominant kernel is the traced one (a lane whose
+    # tuner chose another SW form ran its tasks there)
+    dom_tb_tasks = sum(c.stats()["sw_tasks_tb"] for c, _, _ in lanes if dom in c.kernel_times())
+    all_lanes(lambda c: c.set_kernel_trace(False))
     value = world * n_reads * args.steps / (ms / 1e3)
 
     # ---- the plain per-batch form of the same step: every read through the warp-per-read
     # seeding and chaining kernels (no length buckets), SW tasks in read order ----------
+    # (one lane, batches in sequence: the per-batch GPU path)
     ctx.set_option("warp_seed_only", 1)
     ctx.set_option("length_order", 0)
-    step_device()
+    map_device_step(ctx, iid, dev, p)
     barrier()
     g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     g0.record(stream)
     for _ in range(args.steps):
-        step_device()
+        map_device_step(ctx, iid, dev, p)
     g1.record(stream)
     barrier()
     ms_plain = max_over_ranks(g0.elapsed_time(g1))
@@ -648,38 +706,49 @@ def run_ours(args) -> None:
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
         host.append(dict(n=n, cap=cap, seq=pin(part.seq), off=pin(part.seq_off[:-1]), len=pin(lens),
                          hash=pin(part.name_hash().view(np.int32)),
-                         out=torch.empty(n * 40, dtype=torch.uint8).pin_memory(),
-                         cig=torch.empty(cap, dtype=torch.int32).pin_memory(),
-                         h2d=int(part.seq.nbytes) + 16 * n))
-    # each batch is submitted (dnaln_gpu_map_submit) once its previous use has been waited
-    # for, so the copies of one batch overlap the kernels of the others
-    for h in host:
-        h["used"], h["ticket"] = C.c_int64(), None
+                         h2d=int(part.seq.nbytes) + 16 * n,
+                         # two sets of result buffers: a step's batches are submitted while the
+                         # previous step's are still in flight (each lane's queue stays full)
+                         slots=[dict(out=torch.empty(n * 40, dtype=torch.uint8).pin_memory(),
+                                     cig=torch.empty(cap, dtype=torch.int32).pin_memory(),
+                                     used=C.c_int64(), ticket=None) for _ in range(2)]))
+    # batch i goes to lane i % lanes (its worker and streams are its context's own); a batch
+    # is resubmitted once its result set of two steps before has been waited for, so the
+    # copies of one batch overlap the kernels of the others and no lane waits for the host
+    for i, h in enumerate(host):
+        h["lane"] = lanes[i % n_lanes]
     e2e_used = {}
+    e2e_step = [0]
 
-    def wait_batch(i, h):
-        if h["ticket"] is not None:
-            rc = L.dnaln_gpu_map_wait(ctx.handle, h["ticket"])
-            h["ticket"] = None
+    def wait_slot(i, h, sl):
+        if sl["ticket"] is not None:
+            c = h["lane"][0]
+            rc = L.dnaln_gpu_map_wait(c.handle, sl["ticket"])
+            sl["ticket"] = None
             if rc:
-                raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
-            e2e_used[i] = h["used"].value
+                raise RuntimeError(L.dnaln_gpu_last_error(c.handle).decode())
+            e2e_used[i] = sl["used"].value
 
     def step_e2e():
+        k = e2e_step[0] & 1
         for i, h in enumerate(host):
-            wait_batch(i, h)
+            sl = h["slots"][k]
+            wait_slot(i, h, sl)
             t = C.c_int64()
-            rc = L.dnaln_gpu_map_submit(ctx.handle, iid, h["seq"].data_ptr(), h["off"].data_ptr(),
+            c, ix, _ = h["lane"]
+            rc = L.dnaln_gpu_map_submit(c.handle, ix, h["seq"].data_ptr(), h["off"].data_ptr(),
                                         h["len"].data_ptr(), h["hash"].data_ptr(), h["n"], C.byref(p),
-                                        h["out"].data_ptr(), h["cig"].data_ptr(), h["cap"], C.byref(h["used"]),
+                                        sl["out"].data_ptr(), sl["cig"].data_ptr(), h["cap"], C.byref(sl["used"]),
                                         C.byref(t))
             if rc:
-                raise RuntimeError(L.dnaln_gpu_last_error(ctx.handle).decode())
-            h["ticket"] = t.value
+                raise RuntimeError(L.dnaln_gpu_last_error(c.handle).decode())
+            sl["ticket"] = t.value
+        e2e_step[0] += 1
 
     def drain_e2e():
-        for i, h in enumerate(host):
-            wait_batch(i, h)
+        for k in (e2e_step[0] & 1, 1 - (e2e_step[0] & 1)):  # the older step first
+            for i, h in enumerate(host):
+                wait_slot(i, h, h["slots"][k])
 
     e2e_steps = args.e2e_steps or args.steps
     for _ in range(2):
@@ -716,9 +785,11 @@ def run_ours(args) -> None:
 
     # accuracy gate on the end-to-end results (Evaluator::add against the simulator's truth)
     acc = {"records": 0, "correct": 0, "mapq60_mapped": 0, "mapq60_wrong": 0}
+    last = (e2e_step[0] - 1) & 1  # the result set the last timed step wrote
     for (a, b), h in zip(spans, host):
-        recs = h["out"].numpy().view(D.MAP_RECORD_DTYPE)[:b - a]
-        ev = D.evaluate(D.MapResult(recs, h["cig"].numpy().view(np.uint32)), truth.contig[a:b], truth.start[a:b],
+        sl = h["slots"][last]
+        recs = sl["out"].numpy().view(D.MAP_RECORD_DTYPE)[:b - a]
+        ev = D.evaluate(D.MapResult(recs, sl["cig"].numpy().view(np.uint32)), truth.contig[a:b], truth.start[a:b],
                         truth.rev[a:b])
         for k in acc:
             acc[k] += int(ev[k])
@@ -736,7 +807,7 @@ def run_ours(args) -> None:
     mean_len = float(np.mean(reads.seq_len))
     launches, dom_ms = ktimes[dom]
     avg_launch_ms = dom_ms / launches
-    algo = kernel_bytes(dom, st, mean_len, args.bw)
+    algo = kernel_bytes(dom, dict(st, sw_tasks_tb=dom_tb_tasks), mean_len, args.bw)
     peak, peak_kind = measured_peaks()
     achieved = (algo / launches) / (avg_launch_ms / 1e3) / 1e9 if algo is not None else None
     traffic = None  # DRAM bytes per launch of this kernel from the committed ncu summary
@@ -769,13 +840,18 @@ def run_ours(args) -> None:
     roof_int = None
     if dom.startswith("k_sw_u2<tb>") or dom.startswith("k_sw_wide<tb>"):
         W = 2 * args.bw + 1
-        cells_per_launch = st["sw_tasks_tb"] * mean_len * W / launches
+        cells_per_launch = dom_tb_tasks * mean_len * W / launches
         roof_int = int_roofline(local, stream, dom, cells_per_launch, avg_launch_ms, inst_per_cell)
+        one = breakdown[dom][1] / breakdown[dom][0]
+        if "peak_cells_per_s" in roof_int:
+            roof_int["achieved_cells_per_s_one_lane"] = cells_per_launch / (one / 1e3)
+            roof_int["frac_int_one_lane"] = roof_int["achieved_cells_per_s_one_lane"] / roof_int["peak_cells_per_s"]
 
     out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, no dataset)",
-           "config": workload_config(n_reads, world, args.workload, args.bw, len(g.codes), mean_len),
+           "config": dict(workload_config(n_reads, world, args.workload, args.bw, len(g.codes), mean_len),
+                          lanes=n_lanes),
            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                    "ms_per_step": ms_e2e / e2e_steps, "wall_s": wall_e2e},
            "gpu_launches": int(st["launches"]),
@@ -790,8 +866,14 @@ def run_ours(args) -> None:
                         "avg_launch_ms": avg_launch_ms, "launches_timed": launches,
                         "issue_active": issue_active,
                         "issue_note": "fraction of the kernel's issue slots used, from the committed ncu capture "
-                                      "(profiles/): HBM is not what bounds these integer kernels"},
-           "kernels": kernels, "kernels_note": f"untimed breakdown over {PROFILE_STEPS} steps, every launch traced",
+                                      "(profiles/): HBM is not what bounds these integer kernels",
+                        "avg_launch_ms_one_lane": breakdown[dom][1] / breakdown[dom][0],
+                        "lanes_note": "avg_launch_ms is each launch's event span in the timed region, where the "
+                                      "lanes' batches overlap on the GPU; avg_launch_ms_one_lane is the same kernel "
+                                      "in the untimed one-lane traced steps"},
+           "kernels": kernels, "kernels_note": f"untimed breakdown over {PROFILE_STEPS} one-lane steps, every launch "
+                                               "traced; stages_ms_per_step and sw_gcups sum the lanes' event spans, "
+                                               "which overlap",
            "stages_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
            "sw_gcups": cells / (sw_ms / 1e3) / 1e9 if sw_ms > 0 else None,
            "sw_cells_per_step": cells / args.steps,
@@ -821,6 +903,10 @@ def run_ours(args) -> None:
         out["cpu_baseline"] = cpu_baseline(g, reads, p)
     if rank == 0:
         print(json.dumps(out), flush=True)
+    if pool is not None:
+        pool.shutdown()
+    for c, _, _ in lanes[1:]:
+        c.close()
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()
