@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--cigar-per-read", type=int, default=0,
                     help="CIGAR capacity per read of the output buffers (0 = the 2*len+3 bound)")
     ap.add_argument("--serve-requests", type=int, default=1500, help="requests per rate point (--workload serve)")
-    ap.add_argument("--serve-lanes", type=int, default=3)
+    ap.add_argument("--serve-lanes", type=int, default=4, help="lanes of the batching server (4 measured best of 3, 4, 6)")
     ap.add_argument("--serve-loads", type=float, nargs="*", default=[0.5, 0.8],
                     help="offered loads as fractions of the measured capacity (--workload serve)")
     ap.add_argument("--lanes", type=int, default=2, choices=[1, 2, 3, 4],
