@@ -1048,7 +1048,7 @@ def serve_points(ctx, pools: ServePools, iids, p, n_req: int, loads: list[float]
 def run_serve(args) -> None:
     """The serving workload: both indexes resident, Poisson arrivals at a swept rate,
     requests of log-uniform 1..50,000 reads (length uniform in [100, 300]) to either genome.
-    The continuously batching server (3 lanes, requests coalesced) is measured against
+    The continuously batching server (`--serve-lanes` lanes, default 4, requests coalesced) is measured against
     serving the same stream with the plain per-batch kernels (one lane, one request per batch)."""
     import torch
     import dnaln_b200 as D
