@@ -134,10 +134,9 @@ struct CigarWriter {
 struct PairCodes {
   const uint32_t* D;  // this pair's first word
   int WQ, half;
-  __device__ uint32_t operator()(int i, int d) const {
-    const uint32_t w = D[(static_cast<size_t>(i) * WQ + (d >> 2)) * 32];
-    return (w >> (16 * half + 4 * (3 - (d & 3)))) & 0xFu;
-  }
+  __device__ uint32_t word(int i, int d) const { return D[(static_cast<size_t>(i) * WQ + (d >> 2)) * 32]; }
+  __device__ int shift(int d) const { return 16 * half + 4 * (3 - (d & 3)); }
+  __device__ uint32_t operator()(int i, int d) const { return (word(i, d) >> shift(d)) & 0xFu; }
 };
 
 // Direction codes of the generic kernel: word (i, w), w < WW = ceil(W/8), holds cells
@@ -145,10 +144,16 @@ struct PairCodes {
 struct NibbleCodes {
   const uint32_t* D;
   int WW;
-  __device__ uint32_t operator()(int i, int d) const {
-    return (D[(static_cast<size_t>(i) * WW + (d >> 3)) * 32] >> (4 * (d & 7))) & 0xFu;
-  }
+  __device__ uint32_t word(int i, int d) const { return D[(static_cast<size_t>(i) * WW + (d >> 3)) * 32]; }
+  __device__ int shift(int d) const { return 4 * (d & 7); }
+  __device__ uint32_t operator()(int i, int d) const { return (word(i, d) >> shift(d)) & 0xFu; }
 };
+
+// High bit of each byte of x set where that byte is zero, every other bit clear.
+__device__ __forceinline__ uint64_t zero_bytes(uint64_t x) {
+  constexpr uint64_t kLow7 = 0x7F7F7F7F7F7F7F7Full;
+  return ~(((x & kLow7) + kLow7) | x | kLow7);
+}
 
 // The bytes p[0..7] as one little-endian word, from the aligned 8-byte word holding p[0]
 // and, unless p is aligned, the next one. Each of the two holds at least one of the eight
@@ -172,6 +177,7 @@ __device__ void traceback(const Codes& code, int W, int bi, int bd, int best, co
                           uint32_t* __restrict__ cig, int cap, uint32_t* __restrict__ err) {
   CigarWriter cw{cig, cap, 0, 0xFu, 0};
   int i = bi, d = bd, v = best, nm = 0;
+  const int smax = max(p.match, max(-p.mismatch, -p.ambig));  // the most one step can lower v
   if (d < 0 || d >= W) {
     atomicOr(err, kErrTracebackBounds);
     i = -1;
@@ -196,9 +202,31 @@ __device__ void traceback(const Codes& code, int W, int bi, int bd, int best, co
         // the block's 8 query and 8 target bytes are contiguous: two 8-byte words each
         // instead of 16 byte loads (the walk is bound by its L1 requests)
         const uint64_t qw = load8u(q + i - (kAhead - 1)), tw = load8u(tbase + x0);
+        uint32_t wk[kAhead], any = 0;
 #pragma unroll
         for (int k = 0; k < kAhead; ++k) {
-          cx[k] = code(i - k, d);
+          wk[k] = code.word(i - k, d);
+          any |= wk[k];
+        }
+        const int sh = code.shift(d);
+        // A block that is diagonal throughout, with v > 0 before each of its steps (each
+        // step lowers v by at most smax), is taken whole: its score and mismatches from the
+        // two byte words (bytes equal and both below 4: match; either above 3: ambiguous;
+        // else mismatch), exactly the sums of the steps below.
+        if (((any >> sh) & (kNotDiagE | kFromF)) == 0 && v > (kAhead - 1) * smax) {
+          const uint64_t amb = (qw | tw) & 0xFCFCFCFCFCFCFCFCull;
+          const uint64_t ok_amb = zero_bytes(amb);
+          const int n_match = __popcll(zero_bytes(qw ^ tw) & ok_amb);
+          const int n_amb = kAhead - __popcll(ok_amb);
+          v -= n_match * p.match - (kAhead - n_match - n_amb) * p.mismatch - n_amb * p.ambig;
+          nm += kAhead - n_match;
+          run += kAhead;
+          i -= kAhead;
+          continue;
+        }
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k) {
+          cx[k] = (wk[k] >> sh) & 0xFu;
           qa[k] = static_cast<int>((qw >> (8 * (kAhead - 1 - k))) & 0xFFu);
           const int t8 = static_cast<int>((tw >> (8 * (kAhead - 1 - k))) & 0xFFu);
           ta[k] = t8 > 3 ? 4 : t8;
