@@ -105,6 +105,17 @@ __device__ __forceinline__ uint32_t dir_code32(bool hd_ge_e, bool m1_ge_f, bool 
   return (hd_ge_e ? 0u : kNotDiagE) | (m1_ge_f ? 0u : kFromF) | (e_not_ext ? 0u : kExtE) | (f_not_ext ? 0u : kExtF);
 }
 
+// Global store with an L2 evict-first policy: streaming data (the direction codes, read
+// once by the walk) should not push the resident index out of L2.
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void st_evict_first(uint32_t* p, uint32_t v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
+}
+
 struct CigarWriter {
   uint32_t* out;
   int cap, n;
@@ -485,6 +496,7 @@ __global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1)
   uint32_t plo = s_prof[qcode(qa, qla, 0)], phi = s_prof[qcode(qb, qlb, 0)];
   uint32_t ca = qcode(qa, qla, 1), cb = qcode(qb, qlb, 1);  // codes of the next row
   uint32_t* rowp = DP;
+  const uint64_t pol = l2_evict_first_policy();
   for (int i = 0; i < qmax; ++i) {
     // the next row's codes and profile words and the target column entering the band are
     // loaded up front, so their latency hides behind this row
@@ -507,7 +519,7 @@ __global__ void __launch_bounds__(kSwThreads, (TB && W <= 33) ? 3 : 1)
         dw = dw * 16u + ((b3 * 2u + b2) * 4u + (b1 * 2u + b0));
         if ((d & 3) == 3 || d == W - 1) {
           if ((d & 3) != 3) dw <<= 4 * (3 - (d & 3));
-          rowp[(d >> 2) * 32] = dw;
+          st_evict_first(rowp + (d >> 2) * 32, dw, pol);
           dw = 0;
         }
         rmax = d == 0 ? h : __vmaxu2(rmax, h);
