@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import dnaln_b200 as D
-from helpers import SCHEMES, random_codes, random_tasks
+from helpers import SCHEMES, mutate, random_codes, random_tasks
 
 pytestmark = pytest.mark.gpu
 
@@ -29,6 +29,28 @@ def test_random_tasks_match_port(ctx, port, scheme, traceback):
     qs, ts = random_tasks(rng, 600, scheme[5])
     sp = D.ScoreParams(*scheme)
     check_same(ctx.align(qs, ts, traceback, sp), port.align(qs, ts, traceback, scheme), traceback)
+
+
+@pytest.mark.parametrize("scheme", SCHEMES + [(2, 0, 4, 2, 0, 16), (1, 3, 5, 2, 2, 12)])
+def test_walk_diagonal_blocks_against_reference(ctx, ref, scheme):
+    """Long diagonal runs, the case the walk takes eight steps at a time: queries with
+    scattered Ns and sparse substitutions against N-free targets (so the 16-bit DP kernels
+    take them), local starts and ends at every offset within a block (random junk on
+    either end of the query), and a scheme where mismatches and Ns cost nothing."""
+    rng = np.random.default_rng(31 + scheme[1] + 7 * scheme[4])
+    bw = scheme[5]
+    qs, ts = [], []
+    for i in range(400):
+        core = random_codes(rng, 40 + int(rng.integers(600)), 0.01)
+        head, tail = random_codes(rng, i % 9), random_codes(rng, (i // 9) % 9)
+        q = np.concatenate([head, core, tail])
+        m = mutate(rng, np.where(core > 3, rng.integers(0, 4, core.shape), core).astype(np.uint8), 0.005, 0.0)
+        shift = int(rng.integers(2 * bw + 1))
+        t = np.concatenate([random_codes(rng, shift + len(head)), m, random_codes(rng, 2 * bw + len(tail))])
+        qs.append(q)
+        ts.append(t.astype(np.uint8))
+    sp = D.ScoreParams(*scheme)
+    check_same(ctx.align(qs, ts, True, sp), ref.align(qs, ts, True, scheme), True)
 
 
 @pytest.mark.parametrize("n", [1, 5, 32, 33, 1003])
