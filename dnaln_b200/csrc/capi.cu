@@ -715,13 +715,14 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
         DBUF(lv_in, int32_t, "long_vin", n);
         DBUF(lv_out, int32_t, "long_vout", n);
         kt.begin(st, "k_long_keys");
-        launch_long_order(st, big_list, big_n, static_cast<int>(n), d_seq_len, lk_in, lv_in);
+        const int key_bits = launch_long_order(st, big_list, big_n, static_cast<int>(n), d_seq_len, max_len, lk_in, lv_in);
         kt.end(st);
         size_t tmp = 0;
-        CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, lk_in, lk_out, lv_in, lv_out, static_cast<int>(n), 0, 32, st));
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, lk_in, lk_out, lv_in, lv_out, static_cast<int>(n), 0, key_bits,
+                                           st));
         DBUF(tb, uint8_t, "cub_tmp_lsort", tmp);
         kt.begin(st, "cub_sort");
-        CK(cub::DeviceRadixSort::SortPairs(tb, tmp, lk_in, lk_out, lv_in, lv_out, static_cast<int>(n), 0, 32, st));
+        CK(cub::DeviceRadixSort::SortPairs(tb, tmp, lk_in, lk_out, lv_in, lv_out, static_cast<int>(n), 0, key_bits, st));
         kt.end(st);
         order = lv_out;
         c->stats.launches += 1;

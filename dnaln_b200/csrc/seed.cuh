@@ -185,9 +185,10 @@ bool launch_seed_chain_long(cudaStream_t st, const int32_t* seq_len, const int64
                             int32_t* n_min, int64_t* n_anchor, int32_t* n_anc_t, uint32_t* scratch,
                             int32_t* next_list, int* next_n, int min_len, uint32_t* err);
 // Sort keys (longest first; slots at or past *list_n last) and values (read ids) of a list
-// whose length is only known on the device; n_max = the list buffer's size.
-void launch_long_order(cudaStream_t st, const int32_t* list, const int* list_n, int n_max, const int32_t* seq_len,
-                       uint32_t* keys, int32_t* vals);
+// whose length is only known on the device; n_max = the list buffer's size, max_len at
+// least the longest read. Returns the number of low key bits the sort must cover.
+int launch_long_order(cudaStream_t st, const int32_t* list, const int* list_n, int n_max, const int32_t* seq_len,
+                      int64_t max_len, uint32_t* keys, int32_t* vals);
 
 // Stage entry points: sketch of code sequences, lookups, chaining of given anchor sets.
 void launch_sketch_codes(cudaStream_t st, const uint8_t* codes, const int64_t* seq_off, const int32_t* seq_len,

@@ -46,18 +46,21 @@ constexpr int kLWords = kLWordsA + kLWordsB + kLWordsU;
 __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return b < a ? b : a; }
 
 // Sort keys of the listed reads, longest first; slots at or past the device count last.
+// Keys are top - length with top = 2^bits - 1 (every length of the batch at most top), the
+// empty slots 2^bits: a sort over bits + 1 key bits.
 __global__ void k_long_keys(const int32_t* __restrict__ list, const int* __restrict__ list_n, int n_max,
-                            const int32_t* __restrict__ seq_len, uint32_t* __restrict__ keys,
+                            const int32_t* __restrict__ seq_len, uint32_t top, uint32_t* __restrict__ keys,
                             int32_t* __restrict__ vals) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= n_max) return;
   const int m = *list_n;
   if (x < m) {
     const int32_t r = list[x];
-    keys[x] = 0x7FFFFFFFu - static_cast<uint32_t>(seq_len[r]);
+    const uint32_t len = static_cast<uint32_t>(seq_len[r]);
+    keys[x] = len < top ? top - len : 0u;  // a length past top (not expected) still sorts first
     vals[x] = r;
   } else {
-    keys[x] = 0xFFFFFFFFu;
+    keys[x] = top + 1u;
     vals[x] = -1;
   }
 }
@@ -461,10 +464,13 @@ int64_t seed_long_threads(int64_t n_max) {
 
 size_t seed_long_scratch_words(int64_t threads) { return static_cast<size_t>(threads) * kLWords; }
 
-void launch_long_order(cudaStream_t st, const int32_t* list, const int* list_n, int n_max, const int32_t* seq_len,
-                       uint32_t* keys, int32_t* vals) {
-  if (n_max <= 0) return;
-  k_long_keys<<<(n_max + 255) / 256, 256, 0, st>>>(list, list_n, n_max, seq_len, keys, vals);
+int launch_long_order(cudaStream_t st, const int32_t* list, const int* list_n, int n_max, const int32_t* seq_len,
+                      int64_t max_len, uint32_t* keys, int32_t* vals) {
+  int bits = 16;  // 16 bits cover reads up to 65,535 bp: two radix passes instead of four
+  while (bits < 31 && max_len > (int64_t{1} << bits) - 1) ++bits;
+  if (n_max > 0)
+    k_long_keys<<<(n_max + 255) / 256, 256, 0, st>>>(list, list_n, n_max, seq_len, (1u << bits) - 1u, keys, vals);
+  return bits + 1;
 }
 
 bool launch_seed_chain_long(cudaStream_t st, const int32_t* seq_len, const int64_t* pofs, const uint8_t* codes,
