@@ -669,7 +669,7 @@ int map_enqueue(dnaln_ctx* c, IndexRes& ix, const char* d_seq, const int64_t* d_
     kt.end(st);
     c->stats.launches += 1;
     const auto seed_t = [&](int rpb) {
-      return launch_seed_chain_thread(st, d_seq, d_seq_off, hint.seq_base, d_seq_len, n, ix.dev, sp, cp, cand, cb,
+      return launch_seed_chain_thread(st, codes, pofs, d_seq_len, n, ix.dev, sp, cp, cand, cb,
                                       n_min, n_anchor, n_anc_t, big_list, big_n, c->d_err, rpb);
     };
     int rpb = c->seed_block ? c->seed_block : (c->seed_tune.tuned ? c->seed_tune.reads_per_block : 0);

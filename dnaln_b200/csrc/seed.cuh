@@ -156,7 +156,8 @@ void launch_encode_reads_bulk(cudaStream_t st, const char* seq, const int64_t* s
                               const int32_t* seq_len, const int64_t* pofs, int64_t n, uint8_t* codes, uint32_t* err);
 
 // One thread per read (seed_thread.cu): passes 1 and 2 of the reads the per-thread budgets
-// admit, from their ASCII bytes (the codes in HBM are launch_encode_reads' job), writing
+// admit, from their forward codes (codes + 2 * pofs[r], written by launch_encode_reads on
+// the same stream before), writing
 // candidates of the admitted reads, n_min, n_anc_t (their anchor counts, for statistics)
 // and n_anchor = 0 (no scratch); the others are appended to big_list (count in *big_n,
 // zeroed by the caller) for launch_seed_list / launch_chain_map. reads_per_block: 64 or
@@ -164,7 +165,7 @@ void launch_encode_reads_bulk(cudaStream_t st, const char* seq, const int64_t* s
 // parameters are outside the path's range.
 bool seed_thread_supported(const SeedParams& sp, const ChainParamsDev& cp);
 int seed_thread_max_len();  // the longest read the short thread kernel stages
-bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+bool launch_seed_chain_thread(cudaStream_t st, const uint8_t* codes, const int64_t* pofs,
                               const int32_t* seq_len, int64_t n, const DevIndex& ix, const SeedParams& sp,
                               const ChainParamsDev& cp,
                               const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,

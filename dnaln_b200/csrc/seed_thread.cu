@@ -8,12 +8,11 @@
 // algorithms directly; the 32 reads of a warp advance in lockstep (same k-mer index, same
 // DP row), so the shared-memory layouts [slot][thread] are bank-conflict free.
 //
-//  * Staging: the warp copies the ASCII bytes of its 32 reads into shared memory, each
+//  * Staging: the codes of both strands in HBM (src/mapper.cpp:88-99), which this kernel,
+//    SW and the warp kernels read, are written by k_encode_reads, launched before this
+//    one. The warp copies the forward codes of its 32 reads into shared memory, each
 //    read's aligned words into its thread's column, with one batch of cp.async for all
-//    of them and one wait (one memory latency per warp, not one per group of reads); the
-//    sketch converts the bytes to codes as it reads them. The codes of both strands in
-//    HBM (src/mapper.cpp:88-99), which SW and the warp kernels read, are written by
-//    k_encode_reads, a bandwidth-bound kernel launched before this one.
+//    of them and one wait (one memory latency per warp, not one per group of reads).
 //  * Sketch (src/minimizer.cpp:5-68): rolling 2-bit forward / reverse-complement words,
 //    canonical strand, 32-bit hash (hash32); the window minimum of w keys (hash, position,
 //    strand) by van Herk / Gil-Werman blocks of w: a running prefix minimum of the current
@@ -55,7 +54,7 @@ constexpr int kProbe = 8;                 // minimizers probed with independent 
 // Dynamic shared memory of a block of TT threads (= reads): two regions of 32-bit words,
 // each thread owning one column of each (word w of thread T at w * pitch + T), so that
 // after the cooperative staging no thread ever touches another thread's words. Region A
-// (pitch TT + 1, which spreads the banks): the staged ASCII words, later the anchor keys
+// (pitch TT + 1, which spreads the banks): the staged code words, later the anchor keys
 // (two words each). Region B (pitch TT): the minimizers {hash, pos | strand << 31} (two
 // words each), later f << 8 | (prev + 1) of each anchor (words 0..31) and the chain table
 // (words 32..63). The block size is the tuner's reads-per-block choice (64 or 128); the
@@ -107,7 +106,7 @@ __global__ void __launch_bounds__(256)
 
 template <int W, int TT>
 __global__ void __launch_bounds__(TT)
-    k_seed_chain_t(const char* __restrict__ seq, const int64_t* __restrict__ seq_off, int64_t seq_base,
+    k_seed_chain_t(const uint8_t* __restrict__ codes, const int64_t* __restrict__ pofs,
                    const int32_t* __restrict__ seq_len, int64_t n, DevIndex ix, SeedParams sp, ChainParamsDev cp,
                    CandParams cand,
                    CandBuf cb, int32_t* __restrict__ n_min, int64_t* __restrict__ n_anchor,
@@ -141,17 +140,17 @@ __global__ void __launch_bounds__(TT)
   const int64_t r0 = static_cast<int64_t>(blockIdx.x) * TT + (T & ~31);  // first read of this warp
   const int64_t r = r0 + lane;
   int len = 0;
-  uint64_t a_word = 0;  // this read's first ASCII byte rounded down to a 4-byte boundary
+  uint64_t a_word = 0;  // this read's first code byte rounded down to a 4-byte boundary
   int offb = 0, nwords = 0;
   if (r < n) {
     len = seq_len[r];
-    const uint64_t a = reinterpret_cast<uint64_t>(seq) + static_cast<uint64_t>(seq_off[r] - seq_base);
+    const uint64_t a = reinterpret_cast<uint64_t>(codes) + 2 * static_cast<uint64_t>(pofs[r]);  // forward codes
     offb = static_cast<int>(a & 3u);
     a_word = a - static_cast<uint64_t>(offb);
     if (len > 0 && len <= kTMaxLen) nwords = (offb + len + 3) >> 2;
   }
 
-  // ---- staging: word w of read j's ASCII (from its aligned start) into word w of column j.
+  // ---- staging: word w of read j's codes (from its aligned start) into word w of column j.
   // Every copied word holds at least one byte of its read, so it lies in the pages the
   // read is in. All copies of the warp are in flight before the one wait.
   for (int j = 0; j < 32; ++j) {
@@ -178,7 +177,7 @@ __global__ void __launch_bounds__(TT)
     auto roll = [&](int i) {  // consumes code i (called with i = 0, 1, 2, ...)
       const int jb = i + offb;  // byte of the staged words
       if ((jb & 3) == 0 || i == 0) wcur = ca[(jb >> 2) * L::kPitch];
-      const uint32_t c = nt4((wcur >> (8 * (jb & 3))) & 0xFFu);
+      const uint32_t c = (wcur >> (8 * (jb & 3))) & 0xFFu;  // 0..3, 4 for N
       run = c < 4 ? run + 1 : 0;
       fwd = ((fwd << 2) | (c & 3u)) & mask2k;
       rev = (rev >> 2) | ((3u - (c & 3u)) << (2 * k - 2));
@@ -443,7 +442,7 @@ __global__ void __launch_bounds__(TT)
 }
 
 template <int TT>
-bool launch_thread_tt(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+bool launch_thread_tt(cudaStream_t st, const uint8_t* codes, const int64_t* pofs,
                       const int32_t* seq_len, int64_t n, const DevIndex& ix, const SeedParams& sp,
                       const ChainParamsDev& cp, const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
                       int32_t* n_anc_t, int32_t* big_list, int* big_n, uint32_t* err) {
@@ -451,7 +450,7 @@ bool launch_thread_tt(cudaStream_t st, const char* seq, const int64_t* seq_off, 
   if (!set_smem_limit_once(k_seed_chain_t<kTW, TT>, TLayout<TT>::kSmem, attr_set)) return false;
   const int64_t blocks = (n + TT - 1) / TT;
   k_seed_chain_t<kTW, TT><<<static_cast<unsigned>(blocks), TT, TLayout<TT>::kSmem, st>>>(
-      seq, seq_off, seq_base, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list, big_n, err);
+      codes, pofs, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t, big_list, big_n, err);
   return true;
 }
 
@@ -471,7 +470,7 @@ void launch_encode_reads(cudaStream_t st, const char* seq, const int64_t* seq_of
   k_encode_reads<<<static_cast<unsigned>(blocks), 256, 0, st>>>(seq, seq_off, seq_base, seq_len, pofs, n, codes);
 }
 
-bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* seq_off, int64_t seq_base,
+bool launch_seed_chain_thread(cudaStream_t st, const uint8_t* codes, const int64_t* pofs,
                               const int32_t* seq_len, int64_t n, const DevIndex& ix, const SeedParams& sp,
                               const ChainParamsDev& cp,
                               const CandParams& cand, CandBuf cb, int32_t* n_min, int64_t* n_anchor,
@@ -479,10 +478,10 @@ bool launch_seed_chain_thread(cudaStream_t st, const char* seq, const int64_t* s
   if (!seed_thread_supported(sp, cp)) return false;
   if (n <= 0) return true;
   if (reads_per_block == 64)
-    return launch_thread_tt<64>(st, seq, seq_off, seq_base, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t,
+    return launch_thread_tt<64>(st, codes, pofs, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor, n_anc_t,
                                 big_list, big_n, err);
   if (reads_per_block == 128)
-    return launch_thread_tt<128>(st, seq, seq_off, seq_base, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor,
+    return launch_thread_tt<128>(st, codes, pofs, seq_len, n, ix, sp, cp, cand, cb, n_min, n_anchor,
                                  n_anc_t, big_list, big_n, err);
   return false;
 }
