@@ -88,6 +88,14 @@ __global__ void __launch_bounds__(256)
     k_encode_reads(const char* __restrict__ seq, const int64_t* __restrict__ seq_off, int64_t seq_base,
                    const int32_t* __restrict__ seq_len, const int64_t* __restrict__ pofs, int64_t n,
                    uint8_t* __restrict__ codes) {
+  // both codes of every byte value from a table in shared memory (forward code in the low
+  // byte, its complement in the high byte): one lookup per base instead of the arithmetic
+  __shared__ uint16_t s_code[256];
+  for (int b = threadIdx.x; b < 256; b += blockDim.x) {
+    const uint32_t c = nt4(static_cast<uint32_t>(b));
+    s_code[b] = static_cast<uint16_t>(c | (c < 4 ? 3 - c : 4u) << 8);
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int64_t nw = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
   for (int64_t r = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
@@ -97,9 +105,9 @@ __global__ void __launch_bounds__(256)
     uint8_t* rc = fw + len;
 #pragma unroll 4
     for (int i = lane; i < len; i += 32) {
-      const uint8_t c = static_cast<uint8_t>(nt4(s[i]));
-      fw[i] = c;
-      rc[len - 1 - i] = c < 4 ? static_cast<uint8_t>(3 - c) : 4;
+      const uint32_t cc = s_code[s[i]];
+      fw[i] = static_cast<uint8_t>(cc);
+      rc[len - 1 - i] = static_cast<uint8_t>(cc >> 8);
     }
   }
 }
