@@ -43,8 +43,6 @@ constexpr int kLWordsU = kLMaxAnc / 32;
 static_assert(2 * kLMaxMin <= kLWordsB, "minimizer slots must fit region B");
 constexpr int kLWords = kLWordsA + kLWordsB + kLWordsU;
 
-__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return b < a ? b : a; }
-
 // Sort keys of the listed reads, longest first; slots at or past the device count last.
 // Keys are top - length with top = 2^bits - 1 (every length of the batch at most top), the
 // empty slots 2^bits: a sort over bits + 1 key bits.
@@ -137,45 +135,63 @@ __global__ void __launch_bounds__(kLT, 6)
         rev = (rev >> 2) | ((3u - (c & 3u)) << (2 * k - 2));
       };
       for (int i = 0; i < k - 1; ++i) roll(i);
-      uint64_t cur[W], suf[W];
+      // window minimum over (hash, pos << 1 | strand) pairs by 32-bit hash compares, ties to
+      // the left operand, the earlier position (hashes < 2^(2k), invalid ones ~0)
+      uint32_t cur_h[W], cur_p[W], suf_h[W], suf_p[W];
 #pragma unroll
-      for (int u = 0; u < W; ++u) suf[u] = ~0ULL;
-      uint64_t pre = ~0ULL;
+      for (int u = 0; u < W; ++u) {
+        suf_h[u] = 0xFFFFFFFFu;
+        suf_p[u] = 0;
+      }
+      uint32_t pre_h = 0xFFFFFFFFu, pre_p = 0;
       int lastbad = -1, prev_arg = -1;
       for (int s0 = 0; s0 < nk && !big; s0 += W) {
 #pragma unroll
         for (int u = 0; u < W; ++u) {
           const int s = s0 + u;
-          cur[u] = ~0ULL;
+          cur_h[u] = 0xFFFFFFFFu;
+          cur_p[u] = 0;
           if (s < nk) {
             roll(s + k - 1);
-            uint64_t key = ~0ULL;
+            uint32_t h = 0xFFFFFFFFu, pw = 0;
             if (run >= k) {
               const uint32_t st = rev < fwd;
-              const uint32_t h = fwd != rev ? hash32(st ? rev : fwd, mask2k) : 0xFFFFFFFFu;
-              key = static_cast<uint64_t>(h) << 32 | static_cast<uint32_t>(s) << 1 | st;
+              h = fwd != rev ? hash32(st ? rev : fwd, mask2k) : 0xFFFFFFFFu;
+              pw = static_cast<uint32_t>(s) << 1 | st;
             } else {
               lastbad = s;
             }
-            cur[u] = key;
-            pre = u == 0 ? key : umin64(pre, key);
-            const uint64_t m = u + 1 < W ? umin64(suf[u + 1 < W ? u + 1 : 0], pre) : pre;
+            cur_h[u] = h;
+            cur_p[u] = pw;
+            if (u == 0 || h < pre_h) {
+              pre_h = h;
+              pre_p = pw;
+            }
+            uint32_t m_h = pre_h, m_p = pre_p;
+            if (u + 1 < W && !(pre_h < suf_h[u + 1 < W ? u + 1 : 0])) {
+              m_h = suf_h[u + 1 < W ? u + 1 : 0];
+              m_p = suf_p[u + 1 < W ? u + 1 : 0];
+            }
             int arg = -1;
-            if (s >= W - 1 && lastbad < s - W + 1 && static_cast<uint32_t>(m >> 32) != 0xFFFFFFFFu)
-              arg = static_cast<int>(static_cast<uint32_t>(m) >> 1);
+            if (s >= W - 1 && lastbad < s - W + 1 && m_h != 0xFFFFFFFFu) arg = static_cast<int>(m_p >> 1);
             if (arg >= 0 && arg != prev_arg) {
               if (nmin < kLMaxMin) {
-                B(2 * nmin) = static_cast<uint32_t>(m >> 32);
-                B(2 * nmin + 1) = static_cast<uint32_t>(arg) | (static_cast<uint32_t>(m) & 1u) << 31;
+                B(2 * nmin) = m_h;
+                B(2 * nmin + 1) = static_cast<uint32_t>(arg) | (m_p & 1u) << 31;
               }
               ++nmin;
             }
             prev_arg = arg;
           }
         }
-        suf[W - 1] = cur[W - 1];
+        suf_h[W - 1] = cur_h[W - 1];
+        suf_p[W - 1] = cur_p[W - 1];
 #pragma unroll
-        for (int u = W - 2; u >= 0; --u) suf[u] = umin64(cur[u], suf[u + 1]);
+        for (int u = W - 2; u >= 0; --u) {
+          const bool left = cur_h[u] <= suf_h[u + 1];
+          suf_h[u] = left ? cur_h[u] : suf_h[u + 1];
+          suf_p[u] = left ? cur_p[u] : suf_p[u + 1];
+        }
         if (nmin > kLMaxMin) big = true;
       }
     }
