@@ -178,12 +178,20 @@ __global__ void __launch_bounds__(TT)
   if (!big && len >= k) {
     const uint32_t mask2k = (1u << (2 * k)) - 1u;
     const int nk = len - k + 1;
-    uint32_t fwd = 0, rev = 0, wcur = 0;
+    uint32_t fwd = 0, rev = 0, wcur = ca[0], wsh = 8u * static_cast<uint32_t>(offb);
+    const uint32_t* wnext = ca + L::kPitch;
     int run = 0;
-    auto roll = [&](int i) {  // consumes code i (called with i = 0, 1, 2, ...)
-      const int jb = i + offb;  // byte of the staged words
-      if ((jb & 3) == 0 || i == 0) wcur = ca[(jb >> 2) * L::kPitch];
-      const uint32_t c = (wcur >> (8 * (jb & 3))) & 0xFFu;  // 0..3, 4 for N
+    // consumes the next code; a staged word is loaded as soon as the one before is used up,
+    // a whole position's work ahead of its first byte (the column holds one word past the
+    // read's last, so the load after the read's last word stays inside it)
+    auto roll = [&](int) {
+      const uint32_t c = (wcur >> wsh) & 0xFFu;  // 0..3, 4 for N
+      wsh += 8u;
+      if (wsh == 32u) {
+        wsh = 0u;
+        wcur = *wnext;
+        wnext += L::kPitch;
+      }
       run = c < 4 ? run + 1 : 0;
       fwd = ((fwd << 2) | (c & 3u)) & mask2k;
       rev = (rev >> 2) | ((3u - (c & 3u)) << (2 * k - 2));
