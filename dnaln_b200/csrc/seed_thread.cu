@@ -240,13 +240,14 @@ __global__ void __launch_bounds__(TT)
           }
           int arg = -1;
           if (s >= W - 1 && lastbad < s - W + 1 && m_h != 0xFFFFFFFFu) arg = static_cast<int>(m_p >> 1);
-          if (arg >= 0 && arg != prev_arg) {
-            if (nmin < kTMaxMin) {
-              cbw[2 * nmin * TT] = m_h;
-              cbw[(2 * nmin + 1) * TT] = static_cast<uint32_t>(arg) | (m_p & 1u) << 31;
-            }
-            ++nmin;
+          // emission as predicated stores and an add, not a branch per position
+          const bool emit = arg >= 0 && arg != prev_arg;
+          uint32_t* const slot = cbw + 2 * min(nmin, kTMaxMin - 1) * TT;
+          if (emit && nmin < kTMaxMin) {
+            slot[0] = m_h;
+            slot[TT] = static_cast<uint32_t>(arg) | (m_p & 1u) << 31;
           }
+          nmin += emit ? 1 : 0;
           prev_arg = arg;
         }
       }
