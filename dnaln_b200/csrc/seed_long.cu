@@ -174,13 +174,12 @@ __global__ void __launch_bounds__(kLT, 6)
             }
             int arg = -1;
             if (s >= W - 1 && lastbad < s - W + 1 && m_h != 0xFFFFFFFFu) arg = static_cast<int>(m_p >> 1);
-            if (arg >= 0 && arg != prev_arg) {
-              if (nmin < kLMaxMin) {
-                B(2 * nmin) = m_h;
-                B(2 * nmin + 1) = static_cast<uint32_t>(arg) | (m_p & 1u) << 31;
-              }
-              ++nmin;
+            const bool emit = arg >= 0 && arg != prev_arg;  // predicated, not a branch
+            if (emit && nmin < kLMaxMin) {
+              B(2 * nmin) = m_h;
+              B(2 * nmin + 1) = static_cast<uint32_t>(arg) | (m_p & 1u) << 31;
             }
+            nmin += emit ? 1 : 0;
             prev_arg = arg;
           }
         }
