@@ -321,19 +321,23 @@ __global__ void __launch_bounds__(TT)
 #pragma unroll
       for (int q = 0; q < kProbe; ++q) {
         if (j0 + q >= nmin || big) break;
-        if (cnt[q] == 0) continue;
         if (na + static_cast<int>(cnt[q]) > kTMaxAnc) {
           big = true;
           break;
         }
         const int32_t pos = static_cast<int32_t>(m[q].y & 0x7FFFFFFFu);
         const uint32_t mst = m[q].y >> 31;
-        for (uint32_t t = 0; t < cnt[q]; ++t) {
-          const uint32_t v = t == 0 ? v0[q] : __ldg(ix.positions + off[q] + t);
+        const auto anchor = [&](uint32_t v) {
           const uint32_t rv = (v & 1u) ^ mst;
           const int32_t qpos = rv ? len - pos - k : pos;
           a_hi(na) = rv << 31 | v >> 1;
           a_lo(na) = static_cast<uint32_t>(qpos);
+        };
+        // the first occurrence (most keys have one) with predicated stores, the rest in a loop
+        if (cnt[q] > 0) anchor(v0[q]);
+        na += cnt[q] > 0 ? 1 : 0;
+        for (uint32_t t = 1; t < cnt[q]; ++t) {
+          anchor(__ldg(ix.positions + off[q] + t));
           ++na;
         }
       }
