@@ -241,23 +241,33 @@ __global__ void __launch_bounds__(kLT, 6)
           if ((next >> q) & 1u) bk[q] = __ldg(ix.table + slot[q]);
         pending = next;
       }
+      // first occurrences of the group's keys as independent loads; each key's first anchor
+      // through predicated stores, the further ones in a loop
+      uint32_t v0[kP];
+#pragma unroll
+      for (int q = 0; q < kP; ++q) {
+        if (cnt[q] > sp.max_occ) cnt[q] = 0;
+        v0[q] = j0 + q < nmin && cnt[q] ? __ldg(ix.positions + off[q]) : 0u;
+      }
       for (int q = 0; q < kP && !big; ++q) {
         if (j0 + q >= nmin) break;
-        uint32_t c = cnt[q];
-        if (c > sp.max_occ) c = 0;
-        if (c == 0) continue;
+        const uint32_t c = cnt[q];
         if (na + static_cast<int>(c) > kLMaxAnc) {
           big = true;
           break;
         }
         const int32_t pos = static_cast<int32_t>(mp[q] & 0x7FFFFFFFu);
         const uint32_t mst = mp[q] >> 31;
-        for (uint32_t t = 0; t < c; ++t) {
-          const uint32_t v = __ldg(ix.positions + off[q] + t);
+        const auto anchor = [&](uint32_t v) {
           const uint32_t rv = (v & 1u) ^ mst;
           const int32_t qpos = rv ? len - pos - k : pos;
           A(2 * na) = rv << 31 | v >> 1;
           A(2 * na + 1) = static_cast<uint32_t>(qpos);
+        };
+        if (c > 0) anchor(v0[q]);
+        na += c > 0 ? 1 : 0;
+        for (uint32_t t = 1; t < c; ++t) {
+          anchor(__ldg(ix.positions + off[q] + t));
           ++na;
         }
       }
