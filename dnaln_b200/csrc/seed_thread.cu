@@ -384,17 +384,17 @@ __global__ void __launch_bounds__(TT)
         const uint32_t dr = hi_i - hi_j;  // same strand, sorted: rpos_i - rpos_j >= 0
         if (dr > max_gap) break;
         const int32_t dq = qi - static_cast<int32_t>(a_lo(j));
-        if (dr == 0 || dq <= 0) continue;
+        // the rest as selects (the pairs a warp's reads skip differ): a skipped pair still
+        // reads the gap table, at an index clamped to the band
         const int32_t dri = static_cast<int32_t>(dr);  // <= max_gap < 2^29
         const int32_t dd = dri > dq ? dri - dq : dq - dri;
-        if (dd > cp.band) continue;
+        const bool ok = dr != 0 && dq > 0 && dd <= cp.band;
         int g = dq < dri ? dq : dri;
         if (g > k) g = k;
-        const int sc = f_of(wj) + g - lut[dd];
-        if (sc > best) {
-          best = sc;
-          bj = j;
-        }
+        const int sc = f_of(wj) + g - lut[dd < cp.band ? dd : cp.band];
+        const bool up = ok && sc > best;
+        best = up ? sc : best;
+        bj = up ? j : bj;
       }
       pm = best > pm ? best : pm;
       fp_at(i) = static_cast<uint32_t>(bj + 1) | static_cast<uint32_t>(best) << 8 | static_cast<uint32_t>(pm) << 20;
