@@ -345,17 +345,17 @@ __global__ void __launch_bounds__(kLT, 6)
           const uint32_t dr = hi_i - hi_j;
           if (dr > max_gap) break;
           const int32_t dq = qi - static_cast<int32_t>(r1 ? q1 : (r2 ? q2 : A(2 * j + 1)));
-          if (dr == 0 || dq <= 0) continue;
+          // the rest as selects (a skipped pair reads the gap table at an index clamped to
+          // the band)
           const int32_t dri = static_cast<int32_t>(dr);
           const int32_t dd = dri > dq ? dri - dq : dq - dri;
-          if (dd > cp.band) continue;
+          const bool ok = dr != 0 && dq > 0 && dd <= cp.band;
           int g = dq < dri ? dq : dri;
           if (g > k) g = k;
-          const int sc = static_cast<int>(wj & 0xFFFFu) + g - lut[dd];
-          if (sc > best) {
-            best = sc;
-            bj = j;
-          }
+          const int sc = static_cast<int>(wj & 0xFFFFu) + g - lut[dd < cp.band ? dd : cp.band];
+          const bool up = ok && sc > best;
+          best = up ? sc : best;
+          bj = up ? j : bj;
         }
         pm = best > pm ? best : pm;
         const uint32_t wi = static_cast<uint32_t>(best) | static_cast<uint32_t>(pm) << 16;
